@@ -1,0 +1,198 @@
+"""Seeded synthetic RGBA8 textures for the encode/decode workloads.
+
+No public corpus exists for this path, so every workload is generated from
+numpy's PCG64 with a fixed seed (``0xB2000000 + workload id``), in the shapes,
+sizes and value distributions of the reference benchmark plan:
+
+* ``gradient_noise``   smooth per-channel 2-D gradients + uniform noise in
+                       [-8, 8], with 10% of the 4x4 blocks overwritten by one
+                       solid colour (512x512 BC1 encode+decode workload).
+* ``block_mix``        per-block classes: 40% gradient (random endpoints and
+                       direction, +-8 noise), 30% uniform random RGB, 20%
+                       two-colour edge (random line), 10% solid (4096x4096 BC1
+                       workload; also the colour part of the BC3 workload).
+* ``alpha_mix``        per-block alpha classes in equal thirds: binary 0/255
+                       half-plane cutout, linear ramp, uniform noise.
+* ``normal_map``       tangent-space normals of a sum of 8 Gaussian bumps,
+                       x/y mapped to [0, 255], packed (x, y, 0, 255).
+* ``mixed_batch``      many textures with log-uniform sizes in [4, 2048],
+                       25% forced to a non-multiple of 4, formats
+                       BC1:BC3:BC4:BC5 = 4:3:2:1, levels uniform in {0,5,10,18}.
+
+All arrays are ``uint8`` of shape ``(h, w, 4)``, row-major RGBA.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+SEED_BASE = 0xB2000000
+
+_YY, _XX = np.mgrid[0:4, 0:4]
+_XS = (_XX.reshape(16) - 1.5).astype(np.float32)
+_YS = (_YY.reshape(16) - 1.5).astype(np.float32)
+
+
+def rng_for(workload: int, stream: int = 0) -> np.random.Generator:
+    # identical to SeedSequence(SEED_BASE + workload).spawn(stream + 1)[stream], without building the siblings
+    ss = np.random.SeedSequence(SEED_BASE + workload, spawn_key=(stream,))
+    return np.random.Generator(np.random.PCG64(ss))
+
+
+def _blocks_to_image(blocks: np.ndarray, bw: int, bh: int, w: int, h: int) -> np.ndarray:
+    img = blocks.reshape(bh, bw, 4, 4, 4).transpose(0, 2, 1, 3, 4).reshape(bh * 4, bw * 4, 4)
+    return np.ascontiguousarray(img[:h, :w])
+
+
+def _mix_blocks(rng: np.random.Generator, n: int) -> np.ndarray:
+    """(n, 16, 3) uint8 colour blocks drawn from the 40/30/20/10 class mix."""
+    cls = rng.choice(4, size=n, p=[0.4, 0.3, 0.2, 0.1])
+    c0 = rng.integers(0, 256, size=(n, 3)).astype(np.float32)
+    c1 = rng.integers(0, 256, size=(n, 3)).astype(np.float32)
+    theta = rng.uniform(0, 2 * np.pi, size=n).astype(np.float32)
+    offs = rng.uniform(-1.5, 1.5, size=n).astype(np.float32)
+    noise = rng.integers(-8, 9, size=(n, 16, 3)).astype(np.float32)
+    rand = rng.integers(0, 256, size=(n, 16, 3)).astype(np.float32)
+
+    proj = np.cos(theta)[:, None] * _XS[None] + np.sin(theta)[:, None] * _YS[None]  # (n,16) in ~[-2.1, 2.1]
+    t = np.clip(proj / 4.24 + 0.5, 0.0, 1.0)
+    grad = c0[:, None, :] + (c1 - c0)[:, None, :] * t[:, :, None] + noise
+    edge = np.where((proj > offs[:, None])[:, :, None], c1[:, None, :], c0[:, None, :])
+    solid = np.broadcast_to(c0[:, None, :], (n, 16, 3))
+
+    out = np.empty((n, 16, 3), np.float32)
+    for k, src in enumerate((grad, rand, edge, solid)):
+        m = cls == k
+        out[m] = src[m]
+    return np.clip(np.rint(out), 0, 255).astype(np.uint8)
+
+
+def _alpha_blocks(rng: np.random.Generator, n: int) -> np.ndarray:
+    """(n, 16) uint8 alpha blocks: cutout / ramp / noise in equal thirds."""
+    cls = rng.integers(0, 3, size=n)
+    theta = rng.uniform(0, 2 * np.pi, size=n).astype(np.float32)
+    offs = rng.uniform(-1.5, 1.5, size=n).astype(np.float32)
+    a0 = rng.integers(0, 256, size=n).astype(np.float32)
+    a1 = rng.integers(0, 256, size=n).astype(np.float32)
+    noise = rng.integers(0, 256, size=(n, 16)).astype(np.float32)
+    proj = np.cos(theta)[:, None] * _XS[None] + np.sin(theta)[:, None] * _YS[None]
+    cut = np.where(proj > offs[:, None], 255.0, 0.0)
+    t = np.clip(proj / 4.24 + 0.5, 0.0, 1.0)
+    ramp = a0[:, None] + (a1 - a0)[:, None] * t
+    out = np.where((cls == 0)[:, None], cut, np.where((cls == 1)[:, None], ramp, noise))
+    return np.clip(np.rint(out), 0, 255).astype(np.uint8)
+
+
+def block_mix(w: int, h: int, workload: int = 2, stream: int = 0, with_alpha: bool = False) -> np.ndarray:
+    rng = rng_for(workload, stream)
+    bw, bh = (w + 3) // 4, (h + 3) // 4
+    n = bw * bh
+    blocks = np.empty((n, 16, 4), np.uint8)
+    step = 1 << 18
+    for s in range(0, n, step):
+        e = min(n, s + step)
+        blocks[s:e, :, :3] = _mix_blocks(rng, e - s)
+        blocks[s:e, :, 3] = _alpha_blocks(rng, e - s) if with_alpha else 255
+    return _blocks_to_image(blocks, bw, bh, w, h)
+
+
+def alpha_mix(w: int, h: int, workload: int = 3, stream: int = 0) -> np.ndarray:
+    return block_mix(w, h, workload, stream, with_alpha=True)
+
+
+def gradient_noise(w: int = 512, h: int = 512, workload: int = 1, stream: int = 0) -> np.ndarray:
+    rng = rng_for(workload, stream)
+    y, x = np.mgrid[0:h, 0:w].astype(np.float32)
+    base = np.stack([255 * x / max(w - 1, 1), 255 * y / max(h - 1, 1), 255 * (x + y) / max(w + h - 2, 1)], -1)
+    noise = rng.integers(-8, 9, size=(h, w, 3)).astype(np.float32)
+    img = np.empty((h, w, 4), np.uint8)
+    img[..., :3] = np.clip(np.rint(base + noise), 0, 255).astype(np.uint8)
+    img[..., 3] = 255
+    bw, bh = (w + 3) // 4, (h + 3) // 4
+    nsolid = int(round(0.1 * bw * bh))
+    pick = rng.choice(bw * bh, size=nsolid, replace=False)
+    cols = rng.integers(0, 256, size=(nsolid, 3)).astype(np.uint8)
+    for b, c in zip(pick, cols):
+        by, bx = divmod(int(b), bw)
+        img[by * 4:by * 4 + 4, bx * 4:bx * 4 + 4, :3] = c
+    return img
+
+
+def normal_map(w: int, h: int, workload: int = 3, stream: int = 1) -> np.ndarray:
+    rng = rng_for(workload, stream)
+    cx = rng.uniform(0, w, 8)
+    cy = rng.uniform(0, h, 8)
+    sig = rng.uniform(w / 32, w / 4, 8)
+    amp = rng.uniform(-1, 1, 8) * sig  # slopes of order one
+    ys = np.arange(h, dtype=np.float32)
+    xs = np.arange(w, dtype=np.float32)
+    img = np.empty((h, w, 4), np.uint8)
+    img[..., 2] = 0
+    img[..., 3] = 255
+    step = max(1, (1 << 24) // max(w, 1))
+    for r0 in range(0, h, step):
+        # central differences need one extra row above and below
+        yy = np.arange(max(r0 - 1, 0), min(r0 + step + 1, h), dtype=np.float32)
+        hf = np.zeros((len(yy), w), np.float32)
+        for k in range(8):
+            gx = np.exp(-((xs - cx[k]) ** 2) / (2 * sig[k] ** 2)).astype(np.float32)
+            gy = np.exp(-((yy - cy[k]) ** 2) / (2 * sig[k] ** 2)).astype(np.float32)
+            hf += np.float32(amp[k]) * gy[:, None] * gx[None, :]
+        dx = np.gradient(hf, axis=1)
+        dy = np.gradient(hf, axis=0) if len(yy) > 1 else np.zeros_like(hf)
+        nz = np.ones_like(hf)
+        norm = np.sqrt(dx * dx + dy * dy + nz)
+        nx, ny = -dx / norm, -dy / norm
+        lo = r0 - int(yy[0])
+        rows = min(step, h - r0)
+        img[r0:r0 + rows, :, 0] = np.clip(np.rint((nx[lo:lo + rows] + 1) * 127.5), 0, 255).astype(np.uint8)
+        img[r0:r0 + rows, :, 1] = np.clip(np.rint((ny[lo:lo + rows] + 1) * 127.5), 0, 255).astype(np.uint8)
+    del ys
+    return img
+
+
+FORMATS = ("bc1", "bc3", "bc4", "bc5")
+LEVELS = (0, 5, 10, 18)
+
+
+@dataclasses.dataclass
+class BatchItem:
+    fmt: str
+    level: int
+    width: int
+    height: int
+    seed_stream: int
+
+    def texture(self) -> np.ndarray:
+        if self.fmt == "bc3":
+            return alpha_mix(self.width, self.height, workload=4, stream=self.seed_stream)
+        return block_mix(self.width, self.height, workload=4, stream=self.seed_stream)
+
+
+def mixed_batch(count: int = 10000, workload: int = 4, max_side: int = 2048) -> list[BatchItem]:
+    """Descriptors of the mixed-size batch; textures are generated lazily per item."""
+    rng = rng_for(workload, 10**6)
+    lo, hi = math.log(4), math.log(max_side)
+    # log-uniform sides snapped to the 4-texel grid; a quarter are then pushed off it
+    ws = np.clip(4 * np.rint(np.exp(rng.uniform(lo, hi, count)) / 4), 4, max_side).astype(int)
+    hs = np.clip(4 * np.rint(np.exp(rng.uniform(lo, hi, count)) / 4), 4, max_side).astype(int)
+    ragged = rng.random(count) < 0.25
+    bump = rng.integers(1, 4, count)
+    which = rng.integers(0, 2, count)
+    fmts = rng.choice(4, size=count, p=[0.4, 0.3, 0.2, 0.1])
+    levels = rng.choice(4, size=count)
+    items = []
+    for i in range(count):
+        w, h = int(ws[i]), int(hs[i])
+        if ragged[i]:  # force one side off the 4-texel grid
+            if which[i] == 0:
+                w = (w // 4) * 4 + int(bump[i])
+                w = w - 4 if w > max_side else w
+            else:
+                h = (h // 4) * 4 + int(bump[i])
+                h = h - 4 if h > max_side else h
+        items.append(BatchItem(FORMATS[int(fmts[i])], LEVELS[int(levels[i])], w, h, i))
+    return items
