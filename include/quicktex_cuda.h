@@ -1,0 +1,146 @@
+/*
+ * quicktex_cuda.h — C-ABI of the B200 (sm_100a) S3TC encode/decode path.
+ *
+ * This is the drop-in boundary under the `_quicktex` Python module: every
+ * entry point replaces one call of the reference codec (drewcassidy/quicktex
+ * v0.3.1), cited beside it as `file:line` relative to the reference project
+ * root. Plain pointers and sizes only: no C++ or torch types cross it.
+ *
+ * Conventions
+ *  - Return value: QT_OK (0) or a QT_ERR_* status; qt_last_error() gives a
+ *    thread-local message for the last failing call on the calling thread.
+ *  - Textures are RGBA8, row-major, width*height*4 bytes (RawTexture,
+ *    quicktex/Texture.h:64-141). Block textures are row-major arrays of
+ *    ceil(w/4)*ceil(h/4) blocks of 8 (BC1, BC4) or 16 (BC3, BC5) bytes
+ *    (BlockTexture, quicktex/Texture.h:143-184), in the reference's wire
+ *    layout (BC1Block.h:30-125, BC4Block.h:28-105, BC3Block.h:28-58,
+ *    BC5Block.h:27-57).
+ *  - Encoders read edge blocks with modulo wrap (Texture.h:89-112); decoders
+ *    reproduce the reference's wrapped overwrite of edge texels
+ *    (Texture.h:114-134 in Decoder.h:45-51 loop order).
+ *  - `*_host` calls take HOST buffers and return when the result is in host
+ *    memory. `*_device` calls take DEVICE buffers and only enqueue work on
+ *    `stream` (a cudaStream_t, NULL = legacy default stream).
+ *  - All calls are thread-safe. Each device's constant tables are uploaded
+ *    on first use (or by qt_init).
+ */
+#ifndef QUICKTEX_CUDA_H
+#define QUICKTEX_CUDA_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the pybind layer maps them to the reference's Python exceptions) ---- */
+#define QT_OK 0
+#define QT_ERR_ARG 1     /* std::invalid_argument -> ValueError (e.g. BC1Encoder.cpp:48-50, 75) */
+#define QT_ERR_OOM 2     /* device allocation failed -> MemoryError */
+#define QT_ERR_CUDA 3    /* CUDA runtime error -> RuntimeError */
+#define QT_ERR_TIMEOUT 4 /* a bounded wait expired -> RuntimeError */
+#define QT_ERR_RANGE 5   /* std::out_of_range -> IndexError */
+#define QT_ERR_STATE 6   /* object used in the wrong state -> RuntimeError */
+
+/* ---- enum values: identical to the reference's (BC1Encoder.h:57-100, Interpolator.h:30) ---- */
+#define QT_COLOR_THREE 0x03
+#define QT_COLOR_FOUR 0x04
+#define QT_COLOR_THREE_BLACK 0x13
+#define QT_ERROR_NONE 0
+#define QT_ERROR_FASTER 1
+#define QT_ERROR_CHECK2 2
+#define QT_ERROR_FULL 3
+#define QT_ENDPOINT_LEAST_SQUARES 0
+#define QT_ENDPOINT_BOUNDING_BOX 1
+#define QT_ENDPOINT_BOUNDING_BOX_INT 2
+#define QT_ENDPOINT_PCA 3
+#define QT_INTERP_IDEAL 0
+#define QT_INTERP_IDEAL_ROUND 1
+#define QT_INTERP_NVIDIA 2
+#define QT_INTERP_AMD 3
+
+/* Resolved BC1 encoder settings: the state a BC1Encoder holds after its
+ * constructor and setters (BC1Encoder.h:102-170). */
+typedef struct qt_bc1_params {
+    int32_t color_mode;       /* QT_COLOR_* */
+    int32_t interpolator;     /* QT_INTERP_* */
+    int32_t error_mode;       /* QT_ERROR_* */
+    int32_t endpoint_mode;    /* QT_ENDPOINT_* */
+    int32_t two_ls_passes;    /* bool */
+    int32_t two_ep_passes;    /* bool */
+    int32_t two_cf_passes;    /* bool */
+    int32_t exhaustive;       /* bool */
+    uint32_t search_rounds;   /* any value */
+    uint32_t orderings4;      /* clamped to [1, 128] */
+    uint32_t orderings3;      /* clamped to [1, 32] */
+    uint32_t power_iterations;/* clamped to [4, 10] */
+} qt_bc1_params;
+
+/* Fills `out` with the settings of a preset level; replaces the
+ * BC1Encoder(level, color_mode, interpolator) constructor and
+ * BC1Encoder::SetLevel (BC1Encoder.cpp:47-71, 74-249). level > 19 or an
+ * invalid colour mode / interpolator -> QT_ERR_ARG. */
+int qt_bc1_params_for_level(unsigned level, int color_mode, int interpolator, qt_bc1_params *out);
+
+/* Clamps and checks a params block the way the reference's setters do
+ * (BC1Encoder.cpp:251-258). */
+int qt_bc1_params_validate(qt_bc1_params *p);
+
+/* Uploads the constant tables (ordering tables, factor matrices, single-colour
+ * match tables: OrderTable.h:57-89, SingleColorTable.h:46-90) to `device`.
+ * Optional: every entry point does it on first use of a device. */
+int qt_init(int device);
+
+const char *qt_last_error(void);
+
+/* Library version string. */
+const char *qt_version(void);
+
+/* ---- encoders: BlockEncoder<T>::Encode (Encoder.h:36-56) ---- */
+
+/* BC1Encoder::Encode -> EncodeBlock (BC1Encoder.cpp:261-342) per block. */
+int qt_bc1_encode_host(const uint8_t *rgba, int width, int height, const qt_bc1_params *params, uint8_t *blocks);
+int qt_bc1_encode_device(const uint8_t *rgba, int width, int height, const qt_bc1_params *params, uint8_t *blocks,
+                         void *stream);
+
+/* BC3Encoder::Encode -> EncodeBlock (BC3Encoder.cpp:27-32): BC1 in four-colour
+ * mode on RGB (params->color_mode is ignored) + BC4 on channel 3. */
+int qt_bc3_encode_host(const uint8_t *rgba, int width, int height, const qt_bc1_params *params, uint8_t *blocks);
+int qt_bc3_encode_device(const uint8_t *rgba, int width, int height, const qt_bc1_params *params, uint8_t *blocks,
+                         void *stream);
+
+/* BC4Encoder(channel)::Encode -> EncodeBlock (BC4Encoder.cpp:30-71). */
+int qt_bc4_encode_host(const uint8_t *rgba, int width, int height, int channel, uint8_t *blocks);
+int qt_bc4_encode_device(const uint8_t *rgba, int width, int height, int channel, uint8_t *blocks, void *stream);
+
+/* BC5Encoder(chan0, chan1)::Encode -> EncodeBlock (BC5Encoder.cpp:25-30). */
+int qt_bc5_encode_host(const uint8_t *rgba, int width, int height, int chan0, int chan1, uint8_t *blocks);
+int qt_bc5_encode_device(const uint8_t *rgba, int width, int height, int chan0, int chan1, uint8_t *blocks,
+                         void *stream);
+
+/* ---- decoders: BlockDecoder<T>::Decode (Decoder.h:36-54) ---- */
+
+/* BC1Decoder(write_alpha, interpolator)::Decode (BC1Decoder.cpp:31-52). */
+int qt_bc1_decode_host(const uint8_t *blocks, int width, int height, int interpolator, int write_alpha, uint8_t *rgba);
+int qt_bc1_decode_device(const uint8_t *blocks, int width, int height, int interpolator, int write_alpha,
+                         uint8_t *rgba, void *stream);
+
+/* BC3Decoder(interpolator)::Decode (BC3Decoder.cpp:26-32). */
+int qt_bc3_decode_host(const uint8_t *blocks, int width, int height, int interpolator, uint8_t *rgba);
+int qt_bc3_decode_device(const uint8_t *blocks, int width, int height, int interpolator, uint8_t *rgba, void *stream);
+
+/* BC4Decoder(channel)::Decode (BC4Decoder.cpp:29-50); other channels become (0,0,0,255). */
+int qt_bc4_decode_host(const uint8_t *blocks, int width, int height, int channel, uint8_t *rgba);
+int qt_bc4_decode_device(const uint8_t *blocks, int width, int height, int channel, uint8_t *rgba, void *stream);
+
+/* BC5Decoder(chan0, chan1)::Decode (BC5Decoder.cpp:25-30). */
+int qt_bc5_decode_host(const uint8_t *blocks, int width, int height, int chan0, int chan1, uint8_t *rgba);
+int qt_bc5_decode_device(const uint8_t *blocks, int width, int height, int chan0, int chan1, uint8_t *rgba,
+                         void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* QUICKTEX_CUDA_H */

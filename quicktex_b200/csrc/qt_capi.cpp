@@ -1,0 +1,513 @@
+// qt_capi.cpp — host side of the C-ABI declared in include/quicktex_cuda.h.
+//
+// Owns the constant tables (built once per process, uploaded once per
+// device), a pooled device allocator for the host-buffer entry points, the
+// thread-local error message, and argument checking with the reference's
+// error semantics.
+//
+// Compiled as plain C++ on x86-64 with -ffp-contract=off: the factor matrices
+// of the cluster-fit orderings are computed here with the reference's
+// operation order (OrderTable.h:65-83) and must match it bit for bit.
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "qt_internal.h"
+
+namespace {
+#include "qt_order_blob.inc"  // kOrderBlob[], kOrderBlobSize: quicktex_b200/data/bc1_order_tables.bin
+}
+
+namespace {
+
+thread_local std::string g_err;
+
+int set_err(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+int cuda_err(cudaError_t e, const char *what) {
+    if (e == cudaErrorMemoryAllocation) return set_err(QT_ERR_OOM, "%s: out of device memory", what);
+    return set_err(QT_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// ---------------------------------------------------------------------------
+// constant tables
+// ---------------------------------------------------------------------------
+constexpr size_t kBlobOrders4 = 8, kBlobOrders3 = 8 + 969 * 4, kBlobBest4 = 4352, kBlobBest3 = 4352 + 969 * 128 * 2;
+
+// Interpolators (Interpolator.cpp:47-138)
+int interp8(int t, int a, int b) {
+    if (t == QT_INTERP_IDEAL_ROUND) return (a * 2 + b + 1) / 3;
+    if (t == QT_INTERP_AMD) return (a * 43 + b * 21 + 32) >> 6;
+    return (a * 2 + b) / 3;
+}
+int s5to8(int v) { return (v << 3) | (v >> 2); }
+int s6to8(int v) { return (v << 2) | (v >> 4); }
+int nv5(int a, int b) { return ((2 * a + b) * 22) / 8; }
+int nv6(int a, int b) { int gd = b - a; return (256 * a + (gd / 4) + 128 + gd * 80) >> 8; }
+
+// SingleColorTable<B, N> (SingleColorTable.h:46-90); N does not enter the result.
+void build_match(int t, int bits, uint32_t out[256]) {
+    const int size = 1 << bits;
+    const bool ideal = t == QT_INTERP_IDEAL || t == QT_INTERP_IDEAL_ROUND;
+    const bool use8 = t != QT_INTERP_NVIDIA;
+    for (int i = 0; i < 256; i++) {
+        unsigned error = 256, lo_b = 0, hi_b = 0, err_b = 0;
+        for (int lo = 0; lo < size; lo++) {
+            const int lo8 = bits == 5 ? s5to8(lo) : s6to8(lo);
+            for (int hi = 0; hi < size; hi++) {
+                const int hi8 = bits == 5 ? s5to8(hi) : s6to8(hi);
+                int value = use8 ? interp8(t, hi8, lo8) : (bits == 5 ? nv5(hi, lo) : nv6(hi, lo));
+                value &= 0xFF;
+                unsigned e = (unsigned)std::abs(value - i);
+                if (ideal) e += (unsigned)(std::abs(hi8 - lo8) * 3) / 100;
+                if (e < error || (e == error && lo == hi)) {
+                    lo_b = (unsigned)lo;
+                    hi_b = (unsigned)hi;
+                    err_b = e;
+                    error = e;
+                }
+            }
+        }
+        out[i] = hi_b | (lo_b << 8) | (err_b << 16);
+    }
+}
+
+// OrderTable<N>::Generate (OrderTable.h:57-89)
+void build_factors(int n, int count, const uint8_t *hist, float (*fac)[4], uint16_t *hashes, uint32_t *orders) {
+    // OrderTable<N>::Weights (OrderTable.cpp:40-41): {s^2, s(n-1-s), s(n-1-s), (n-1-s)^2}
+    const float w4[4][4] = {{0, 0, 0, 9}, {1, 2, 2, 4}, {4, 2, 2, 1}, {9, 0, 0, 0}};
+    const float w3[3][4] = {{0, 0, 0, 4}, {1, 1, 1, 1}, {4, 0, 0, 0}};
+    const float denom = n == 4 ? 3.0f : 2.0f;
+    for (int i = 0; i < count; i++) {
+        const uint8_t *h = hist + (size_t)i * n;
+        bool any16 = false;
+        unsigned packed = 0;
+        uint32_t ord = 0;
+        for (int s = 0; s < n; s++) {
+            any16 |= h[s] == 16;
+            ord |= (uint32_t)h[s] << (8 * s);
+        }
+        for (int s = 0; s < n - 1; s++) packed |= (unsigned)h[s] << (4 * s);
+        if (!any16) hashes[packed] = (uint16_t)i;
+        orders[i] = ord;
+        float m[4] = {0, 0, 0, 0};
+        for (int s = 0; s < n; s++) {
+            const float *w = n == 4 ? w4[s] : w3[s];
+            for (int k = 0; k < 4; k++) m[k] = m[k] + w[k] * (float)h[s];
+        }
+        const float det = (m[0] * m[3]) - (m[1] * m[2]);
+        if (std::fabs(det) < 1e-8f) {
+            fac[i][0] = fac[i][1] = fac[i][2] = fac[i][3] = 0.0f;
+        } else {
+            const float t = m[0];
+            m[0] = m[3];
+            m[3] = t;
+            m[1] = m[1] * -1.0f;
+            m[2] = m[2] * -1.0f;
+            const float sc = (denom / 255.0f) / det;
+            for (int k = 0; k < 4; k++) fac[i][k] = m[k] * sc;
+        }
+    }
+}
+
+qtk::HostTables *make_tables() {
+    auto *t = new qtk::HostTables();
+    std::memset(t, 0, sizeof *t);
+    if (kOrderBlobSize != 262208 || std::memcmp(kOrderBlob, "QTOT", 4) != 0) {
+        std::fprintf(stderr, "quicktex_cuda: embedded ordering tables are corrupt\n");
+        std::abort();
+    }
+    const uint8_t *o4 = kOrderBlob + kBlobOrders4, *o3 = kOrderBlob + kBlobOrders3;
+    for (int i = 0; i < 969 * 128; i++) t->best4[i] = (uint16_t)(kOrderBlob[kBlobBest4 + 2 * i] | (kOrderBlob[kBlobBest4 + 2 * i + 1] << 8));
+    for (int i = 0; i < 153 * 32; i++) t->best3[i] = (uint16_t)(kOrderBlob[kBlobBest3 + 2 * i] | (kOrderBlob[kBlobBest3 + 2 * i + 1] << 8));
+    build_factors(4, 969, o4, t->factors4, t->hash4, t->orders4);
+    build_factors(3, 153, o3, t->factors3, t->hash3, t->orders3);
+    for (int it = 0; it < 4; it++) {
+        build_match(it, 5, t->match5[it]);
+        build_match(it, 6, t->match6[it]);
+    }
+    return t;
+}
+
+// ---------------------------------------------------------------------------
+// per-device state and pooled device buffers
+// ---------------------------------------------------------------------------
+constexpr int kMaxDevices = 64;
+std::mutex g_init_mu;
+bool g_inited[kMaxDevices];
+
+int ensure_device(int *dev_out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_err(e, "cudaGetDevice");
+    if (dev < 0 || dev >= kMaxDevices) return set_err(QT_ERR_ARG, "device %d out of range", dev);
+    if (dev_out) *dev_out = dev;
+    std::lock_guard<std::mutex> lk(g_init_mu);
+    if (g_inited[dev]) return QT_OK;
+    int rc = qtk::upload_tables(dev);
+    if (rc != 0) return cuda_err((cudaError_t)rc, "uploading tables");
+    g_inited[dev] = true;
+    return QT_OK;
+}
+
+// Size-class free lists of device buffers, per device. Buffers are kept for
+// reuse (resident across calls) and handed out exclusively.
+struct Pool {
+    std::mutex mu;
+    std::multimap<size_t, void *> free_[kMaxDevices];
+};
+Pool &pool() {
+    static Pool *p = new Pool();
+    return *p;
+}
+
+size_t size_class(size_t n) {
+    size_t c = 4096;
+    while (c < n) c <<= 1;
+    return c;
+}
+
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t cls = 0;
+    int dev = 0;
+    ~DevBuf() {
+        if (ptr) {
+            std::lock_guard<std::mutex> lk(pool().mu);
+            pool().free_[dev].emplace(cls, ptr);
+        }
+    }
+};
+
+int acquire(DevBuf &b, int dev, size_t n) {
+    b.dev = dev;
+    b.cls = size_class(n);
+    {
+        std::lock_guard<std::mutex> lk(pool().mu);
+        auto &fl = pool().free_[dev];
+        auto it = fl.find(b.cls);
+        if (it != fl.end()) {
+            b.ptr = it->second;
+            fl.erase(it);
+            return QT_OK;
+        }
+    }
+    cudaError_t e = cudaMalloc(&b.ptr, b.cls);
+    if (e != cudaSuccess) {
+        b.ptr = nullptr;
+        cudaGetLastError();
+        return cuda_err(e, "cudaMalloc");
+    }
+    return QT_OK;
+}
+
+// one non-blocking stream per host thread and device for the host-buffer calls
+cudaStream_t thread_stream(int dev) {
+    thread_local cudaStream_t streams[kMaxDevices] = {};
+    if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+    return streams[dev];
+}
+
+// ---------------------------------------------------------------------------
+// argument checks (reference error texts where it has them)
+// ---------------------------------------------------------------------------
+int check_dims(int w, int h) {
+    if (w <= 0) return set_err(QT_ERR_ARG, "Texture width must be greater than 0");
+    if (h <= 0) return set_err(QT_ERR_ARG, "Texture height must be greater than 0");
+    if ((long long)w * h > (1LL << 32)) return set_err(QT_ERR_ARG, "Texture too large");
+    return QT_OK;
+}
+int check_channel(int c) {
+    return (c < 0 || c > 3) ? set_err(QT_ERR_ARG, "Channel out of range") : QT_OK;
+}
+int check_interp(int t) {
+    return (t < 0 || t > 3) ? set_err(QT_ERR_ARG, "Invalid interpolator type") : QT_OK;
+}
+size_t nblocks(int w, int h) { return (size_t)((w + 3) / 4) * (size_t)((h + 3) / 4); }
+
+int check_ptr(const void *p, size_t align, const char *what) {
+    if (!p) return set_err(QT_ERR_ARG, "%s is NULL", what);
+    if (reinterpret_cast<uintptr_t>(p) % align) return set_err(QT_ERR_ARG, "%s must be %zu-byte aligned", what, align);
+    return QT_OK;
+}
+
+int finish_launch(int rc, const char *what) {
+    return rc ? cuda_err((cudaError_t)rc, what) : QT_OK;
+}
+
+// host path: H2D, kernel, D2H on this thread's stream; returns when done
+template <typename Launch>
+int run_host(const void *src, size_t src_bytes, void *dst, size_t dst_bytes, bool dst_needs_zero, Launch &&launch,
+             const char *what) {
+    int dev = 0;
+    int rc = ensure_device(&dev);
+    if (rc) return rc;
+    DevBuf din, dout;
+    if ((rc = acquire(din, dev, src_bytes)) || (rc = acquire(dout, dev, dst_bytes))) return rc;
+    cudaStream_t s = thread_stream(dev);
+    cudaError_t e = cudaMemcpyAsync(din.ptr, src, src_bytes, cudaMemcpyHostToDevice, s);
+    if (e != cudaSuccess) return cuda_err(e, "host-to-device copy");
+    if (dst_needs_zero && (e = cudaMemsetAsync(dout.ptr, 0, dst_bytes, s)) != cudaSuccess) return cuda_err(e, "memset");
+    rc = launch(din.ptr, dout.ptr, (void *)s);
+    if (rc) return cuda_err((cudaError_t)rc, what);
+    e = cudaMemcpyAsync(dst, dout.ptr, dst_bytes, cudaMemcpyDeviceToHost, s);
+    if (e != cudaSuccess) return cuda_err(e, "device-to-host copy");
+    e = cudaStreamSynchronize(s);
+    if (e != cudaSuccess) return cuda_err(e, what);
+    return QT_OK;
+}
+
+int set_level(qt_bc1_params *p, unsigned level) {
+    // BC1Encoder::SetLevel (BC1Encoder.cpp:74-249)
+    if (level > 19) return set_err(QT_ERR_ARG, "Level out of range, bust be between 0 and 18 inclusive");
+    p->two_ls_passes = p->two_ep_passes = p->two_cf_passes = p->exhaustive = 0;
+    p->power_iterations = 4;
+    p->error_mode = QT_ERROR_CHECK2;
+    p->endpoint_mode = QT_ENDPOINT_PCA;
+    p->search_rounds = 0;
+    p->orderings3 = p->orderings4 = 0;
+    struct Row { int ls, ep, cf, ex, em, epm, o4, o3, sr, pi; };
+    // -1 in epm keeps PCA; rows follow the switch in SetLevel
+    static const Row rows[20] = {
+        {0, 0, 0, 0, QT_ERROR_CHECK2, QT_ENDPOINT_BOUNDING_BOX_INT, 0, 0, 0, 4},  // 0
+        {0, 0, 0, 0, QT_ERROR_CHECK2, QT_ENDPOINT_LEAST_SQUARES, 0, 0, 0, 4},     // 1
+        {0, 0, 0, 0, QT_ERROR_CHECK2, QT_ENDPOINT_PCA, 0, 0, 0, 4},               // 2
+        {1, 0, 0, 0, QT_ERROR_CHECK2, QT_ENDPOINT_PCA, 0, 0, 0, 4},               // 3
+        {1, 0, 0, 0, QT_ERROR_FULL, QT_ENDPOINT_PCA, 0, 0, 0, 6},                 // 4
+        {1, 0, 0, 0, QT_ERROR_FASTER, QT_ENDPOINT_PCA, 0, 0, 0, 4},               // 5
+        {1, 0, 0, 0, QT_ERROR_FASTER, QT_ENDPOINT_PCA, 1, 1, 0, 4},               // 6
+        {1, 0, 0, 0, QT_ERROR_FASTER, QT_ENDPOINT_PCA, 4, 1, 0, 4},               // 7
+        {1, 0, 0, 0, QT_ERROR_FASTER, QT_ENDPOINT_PCA, 8, 1, 0, 4},               // 8
+        {1, 0, 0, 0, QT_ERROR_CHECK2, QT_ENDPOINT_PCA, 11, 3, 0, 4},              // 9
+        {1, 0, 0, 0, QT_ERROR_CHECK2, QT_ENDPOINT_PCA, 20, 8, 0, 4},              // 10
+        {1, 0, 0, 0, QT_ERROR_CHECK2, QT_ENDPOINT_PCA, 28, 16, 0, 4},             // 11
+        {1, 0, 0, 0, QT_ERROR_CHECK2, QT_ENDPOINT_PCA, 32, 32, 0, 4},             // 12
+        {1, 1, 0, 0, QT_ERROR_FULL, QT_ENDPOINT_PCA, 32, 32, 20, 6},              // 13
+        {1, 1, 0, 0, QT_ERROR_FULL, QT_ENDPOINT_PCA, 32, 32, 32, 6},              // 14
+        {1, 1, 0, 0, QT_ERROR_FULL, QT_ENDPOINT_PCA, 56, 32, 32, 6},              // 15
+        {1, 1, 0, 0, QT_ERROR_FULL, QT_ENDPOINT_PCA, 80, 32, 256, 6},             // 16
+        {1, 1, 0, 0, QT_ERROR_FULL, QT_ENDPOINT_PCA, 128, 32, 256, 4},            // 17
+        {1, 1, 1, 0, QT_ERROR_FULL, QT_ENDPOINT_PCA, 128, 32, 256, 6},            // 18
+        {1, 1, 1, 1, QT_ERROR_FULL, QT_ENDPOINT_PCA, 128, 32, 256, 6},            // 19
+    };
+    const Row &r = rows[level];
+    p->two_ls_passes = r.ls;
+    p->two_ep_passes = r.ep;
+    p->two_cf_passes = r.cf;
+    p->exhaustive = r.ex;
+    p->error_mode = r.em;
+    p->endpoint_mode = r.epm;
+    p->orderings4 = r.o4 < 1 ? 1u : (unsigned)r.o4;  // clamp to >= 1 (:247-248)
+    p->orderings3 = r.o3 < 1 ? 1u : (unsigned)r.o3;
+    p->search_rounds = (unsigned)r.sr;
+    p->power_iterations = (unsigned)r.pi;
+    return QT_OK;
+}
+
+int check_params(const qt_bc1_params *p, bool bc3) {
+    if (!p) return set_err(QT_ERR_ARG, "params is NULL");
+    if (!bc3 && p->color_mode != QT_COLOR_FOUR && p->color_mode != QT_COLOR_THREE && p->color_mode != QT_COLOR_THREE_BLACK)
+        return set_err(QT_ERR_ARG, "Encoder color mode must be FourColor, ThreeColor, or ThreeColorBlack");
+    if (int rc = check_interp(p->interpolator)) return rc;
+    if (p->error_mode < 0 || p->error_mode > 3) return set_err(QT_ERR_ARG, "Invalid error mode");
+    if (p->endpoint_mode < 0 || p->endpoint_mode > 3) return set_err(QT_ERR_ARG, "Invalid endpoint mode");
+    if (p->orderings4 < 1 || p->orderings4 > 128 || p->orderings3 < 1 || p->orderings3 > 32)
+        return set_err(QT_ERR_ARG, "orderings out of range (call qt_bc1_params_validate)");
+    if (p->power_iterations < 4 || p->power_iterations > 10)
+        return set_err(QT_ERR_ARG, "power_iterations out of range (call qt_bc1_params_validate)");
+    return QT_OK;
+}
+
+}  // namespace
+
+namespace qtk {
+const HostTables &host_tables() {
+    static const HostTables *t = make_tables();
+    return *t;
+}
+}  // namespace qtk
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+extern "C" {
+
+const char *qt_last_error(void) { return g_err.c_str(); }
+
+const char *qt_version(void) { return "quicktex-b200 0.1.0 (sm_100a)"; }
+
+int qt_bc1_params_for_level(unsigned level, int color_mode, int interpolator, qt_bc1_params *out) {
+    if (!out) return set_err(QT_ERR_ARG, "out is NULL");
+    if (color_mode != QT_COLOR_FOUR && color_mode != QT_COLOR_THREE && color_mode != QT_COLOR_THREE_BLACK)
+        return set_err(QT_ERR_ARG, "Encoder color mode must be FourColor, ThreeColor, or ThreeColorBlack");
+    if (int rc = check_interp(interpolator)) return rc;
+    qt_bc1_params p;
+    if (int rc = set_level(&p, level)) return rc;
+    p.color_mode = color_mode;
+    p.interpolator = interpolator;
+    *out = p;
+    return QT_OK;
+}
+
+int qt_bc1_params_validate(qt_bc1_params *p) {
+    if (!p) return set_err(QT_ERR_ARG, "params is NULL");
+    // SetOrderings4/3 and SetPowerIterations clamp (BC1Encoder.cpp:251-258)
+    if (p->orderings4 < 1) p->orderings4 = 1;
+    if (p->orderings4 > 128) p->orderings4 = 128;
+    if (p->orderings3 < 1) p->orderings3 = 1;
+    if (p->orderings3 > 32) p->orderings3 = 32;
+    if (p->power_iterations < 4) p->power_iterations = 4;
+    if (p->power_iterations > 10) p->power_iterations = 10;
+    return check_params(p, false);
+}
+
+int qt_init(int device) {
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return cuda_err(e, "cudaGetDevice");
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return cuda_err(e, "cudaSetDevice");
+    int rc = ensure_device(nullptr);
+    cudaSetDevice(prev);
+    return rc;
+}
+
+// ---- encoders ----
+int qt_bc1_encode_device(const uint8_t *rgba, int w, int h, const qt_bc1_params *p, uint8_t *blocks, void *stream) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_params(p, false)) || (rc = check_ptr(rgba, 4, "rgba")) ||
+        (rc = check_ptr(blocks, 8, "blocks")) || (rc = ensure_device(nullptr)))
+        return rc;
+    return finish_launch(qtk::launch_bc1_encode(rgba, w, h, *p, blocks, false, stream), "bc1 encode");
+}
+
+int qt_bc3_encode_device(const uint8_t *rgba, int w, int h, const qt_bc1_params *p, uint8_t *blocks, void *stream) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_params(p, true)) || (rc = check_ptr(rgba, 4, "rgba")) ||
+        (rc = check_ptr(blocks, 16, "blocks")) || (rc = ensure_device(nullptr)))
+        return rc;
+    return finish_launch(qtk::launch_bc1_encode(rgba, w, h, *p, blocks, true, stream), "bc3 encode");
+}
+
+int qt_bc4_encode_device(const uint8_t *rgba, int w, int h, int channel, uint8_t *blocks, void *stream) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_channel(channel)) || (rc = check_ptr(rgba, 4, "rgba")) ||
+        (rc = check_ptr(blocks, 8, "blocks")) || (rc = ensure_device(nullptr)))
+        return rc;
+    return finish_launch(qtk::launch_bc4_encode(rgba, w, h, channel, channel, false, blocks, stream), "bc4 encode");
+}
+
+int qt_bc5_encode_device(const uint8_t *rgba, int w, int h, int c0, int c1, uint8_t *blocks, void *stream) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_channel(c0)) || (rc = check_channel(c1)) ||
+        (rc = check_ptr(rgba, 4, "rgba")) || (rc = check_ptr(blocks, 16, "blocks")) || (rc = ensure_device(nullptr)))
+        return rc;
+    return finish_launch(qtk::launch_bc4_encode(rgba, w, h, c0, c1, true, blocks, stream), "bc5 encode");
+}
+
+int qt_bc1_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p, uint8_t *blocks) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_params(p, false)) || (rc = check_ptr(rgba, 1, "rgba")) ||
+        (rc = check_ptr(blocks, 1, "blocks")))
+        return rc;
+    const qt_bc1_params pp = *p;
+    return run_host(rgba, (size_t)w * h * 4, blocks, nblocks(w, h) * 8, false,
+                    [&](void *in, void *out, void *s) { return qtk::launch_bc1_encode((const uint8_t *)in, w, h, pp, (uint8_t *)out, false, s); },
+                    "bc1 encode");
+}
+
+int qt_bc3_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p, uint8_t *blocks) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_params(p, true)) || (rc = check_ptr(rgba, 1, "rgba")) ||
+        (rc = check_ptr(blocks, 1, "blocks")))
+        return rc;
+    const qt_bc1_params pp = *p;
+    return run_host(rgba, (size_t)w * h * 4, blocks, nblocks(w, h) * 16, false,
+                    [&](void *in, void *out, void *s) { return qtk::launch_bc1_encode((const uint8_t *)in, w, h, pp, (uint8_t *)out, true, s); },
+                    "bc3 encode");
+}
+
+int qt_bc4_encode_host(const uint8_t *rgba, int w, int h, int channel, uint8_t *blocks) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_channel(channel)) || (rc = check_ptr(rgba, 1, "rgba")) ||
+        (rc = check_ptr(blocks, 1, "blocks")))
+        return rc;
+    return run_host(rgba, (size_t)w * h * 4, blocks, nblocks(w, h) * 8, false,
+                    [&](void *in, void *out, void *s) { return qtk::launch_bc4_encode((const uint8_t *)in, w, h, channel, channel, false, (uint8_t *)out, s); },
+                    "bc4 encode");
+}
+
+int qt_bc5_encode_host(const uint8_t *rgba, int w, int h, int c0, int c1, uint8_t *blocks) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_channel(c0)) || (rc = check_channel(c1)) ||
+        (rc = check_ptr(rgba, 1, "rgba")) || (rc = check_ptr(blocks, 1, "blocks")))
+        return rc;
+    return run_host(rgba, (size_t)w * h * 4, blocks, nblocks(w, h) * 16, false,
+                    [&](void *in, void *out, void *s) { return qtk::launch_bc4_encode((const uint8_t *)in, w, h, c0, c1, true, (uint8_t *)out, s); },
+                    "bc5 encode");
+}
+
+// ---- decoders ----
+static int decode_device(int fmt, const uint8_t *blocks, int w, int h, int interp, int wa, int c0, int c1, uint8_t *rgba,
+                         void *stream) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_interp(interp)) || (rc = check_channel(c0)) || (rc = check_channel(c1)) ||
+        (rc = check_ptr(blocks, (fmt == 3 || fmt == 5) ? 16 : 8, "blocks")) || (rc = check_ptr(rgba, 4, "rgba")) ||
+        (rc = ensure_device(nullptr)))
+        return rc;
+    return finish_launch(qtk::launch_decode(fmt, blocks, w, h, interp, wa, c0, c1, rgba, stream), "decode");
+}
+
+static int decode_host(int fmt, const uint8_t *blocks, int w, int h, int interp, int wa, int c0, int c1, uint8_t *rgba) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_interp(interp)) || (rc = check_channel(c0)) || (rc = check_channel(c1)) ||
+        (rc = check_ptr(blocks, 1, "blocks")) || (rc = check_ptr(rgba, 1, "rgba")))
+        return rc;
+    const size_t bsize = (fmt == 3 || fmt == 5) ? 16 : 8;
+    return run_host(blocks, nblocks(w, h) * bsize, rgba, (size_t)w * h * 4, false,
+                    [&](void *in, void *out, void *s) { return qtk::launch_decode(fmt, (const uint8_t *)in, w, h, interp, wa, c0, c1, (uint8_t *)out, s); },
+                    "decode");
+}
+
+int qt_bc1_decode_device(const uint8_t *b, int w, int h, int interp, int wa, uint8_t *rgba, void *s) {
+    return decode_device(1, b, w, h, interp, wa != 0, 0, 0, rgba, s);
+}
+int qt_bc3_decode_device(const uint8_t *b, int w, int h, int interp, uint8_t *rgba, void *s) {
+    return decode_device(3, b, w, h, interp, 0, 0, 0, rgba, s);
+}
+int qt_bc4_decode_device(const uint8_t *b, int w, int h, int ch, uint8_t *rgba, void *s) {
+    return decode_device(4, b, w, h, 0, 0, ch, ch, rgba, s);
+}
+int qt_bc5_decode_device(const uint8_t *b, int w, int h, int c0, int c1, uint8_t *rgba, void *s) {
+    return decode_device(5, b, w, h, 0, 0, c0, c1, rgba, s);
+}
+int qt_bc1_decode_host(const uint8_t *b, int w, int h, int interp, int wa, uint8_t *rgba) {
+    return decode_host(1, b, w, h, interp, wa != 0, 0, 0, rgba);
+}
+int qt_bc3_decode_host(const uint8_t *b, int w, int h, int interp, uint8_t *rgba) {
+    return decode_host(3, b, w, h, interp, 0, 0, 0, rgba);
+}
+int qt_bc4_decode_host(const uint8_t *b, int w, int h, int ch, uint8_t *rgba) {
+    return decode_host(4, b, w, h, 0, 0, ch, ch, rgba);
+}
+int qt_bc5_decode_host(const uint8_t *b, int w, int h, int c0, int c1, uint8_t *rgba) {
+    return decode_host(5, b, w, h, 0, 0, c0, c1, rgba);
+}
+
+}  // extern "C"

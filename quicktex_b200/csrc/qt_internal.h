@@ -1,0 +1,41 @@
+// Internal interface between the host C-ABI (qt_capi.cpp) and the kernels
+// translation unit (qt_kernels.cu). Not part of the public boundary.
+#pragma once
+
+#include <cstddef>
+#include <cstdint>
+
+#include "quicktex_cuda.h"
+
+namespace qtk {
+
+// Host image of the device-resident constant tables.
+struct alignas(16) HostTables {
+    uint16_t best4[969 * 128];  // OrderTable<4>::BestOrders (OrderTable4.cpp:996-1965)
+    uint16_t best3[153 * 32];   // OrderTable<3>::BestOrders (OrderTable.cpp:165-320)
+    uint16_t hash4[4096];       // histogram -> ordering index (OrderTable.h:64)
+    uint16_t hash3[256];
+    float factors4[969][4];     // 2x2 LS inverse per ordering (OrderTable.h:65-83)
+    float factors3[153][4];
+    uint32_t orders4[969];      // histogram bytes h0 | h1<<8 | h2<<16 | h3<<24
+    uint32_t orders3[153];
+    uint32_t match5[4][256];    // single-colour tables per interpolator: high | low<<8 | err<<16
+    uint32_t match6[4][256];
+};
+
+// Builds the tables on the host (the factor matrices with the reference's
+// float operation order) from the embedded ordering-table blob.
+const HostTables &host_tables();
+
+// Kernel-side entry points (qt_kernels.cu). Each returns a cudaError_t value
+// cast to int (0 on success). All pointers are device pointers.
+int upload_tables(int device);
+
+int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
+                      void *stream);
+int launch_bc4_encode(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc5, uint8_t *out, void *stream);
+// fmt: 1 = BC1, 3 = BC3, 4 = BC4, 5 = BC5
+int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
+                  uint8_t *rgba, void *stream);
+
+}  // namespace qtk

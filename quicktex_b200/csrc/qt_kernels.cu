@@ -1,0 +1,1182 @@
+// qt_kernels.cu — sm_100a kernels of the S3TC encode/decode path.
+//
+// Mapping. BC1 (and the colour half of BC3) runs one 4x4 block per group of
+// 16 lanes (two blocks per warp). Each phase of the reference encoder
+// (BC1Encoder::EncodeBlock, BC1Encoder.cpp:261-342) picks its own lane
+// mapping:
+//   * texel-parallel  (lane = texel): metrics, FindEndpoints, FindSelectors,
+//     RefineEndpointsLS(pixels). Every sum the reference accumulates over texels
+//     is integer-valued (in int or in float below 2^24), so warp reductions
+//     (redux.sync) give the reference's exact values in any order.
+//   * ordering-parallel (lane = cluster-fit ordering): RefineBlockCF. All
+//     orderings start from the same `orig` result, so the reference's
+//     sequential "keep if strictly better, stop at zero error" loop equals an
+//     argmin over (error, ordering index).
+//   * round-parallel (lane = search round): EndpointSearch. Rounds between two
+//     improvements all start from the same result, so 16 consecutive rounds are
+//     evaluated speculatively and the first improving one (or the stop rule)
+//     decides, exactly as the sequential loop would.
+// The reference's FindSelectors early exits never change an accepted result
+// (every exit bound is >= the later acceptance bound), so full errors are
+// computed instead.
+//
+// Floating point. Every operation whose rounding matters is written with an
+// explicit round-to-nearest intrinsic (__fadd_rn, __fmul_rn, __fdiv_rn), in
+// the reference's operation order; the compiler never contracts these into
+// FMAs. Plain float arithmetic (and fmaf) is used only where every operand and
+// result is an integer below 2^24, i.e. exact.
+//
+// BC4/BC5 encode and all decoders are HBM-bound: one thread per block,
+// 16-byte row loads/stores where the texture is 4-aligned.
+
+#include <cuda_runtime.h>
+
+#include <cfloat>
+#include <climits>
+#include <cstdint>
+
+#include "qt_internal.h"
+
+namespace qtk {
+
+// ---------------------------------------------------------------------------
+// constant tables
+// ---------------------------------------------------------------------------
+struct DevTables {
+    uint16_t best4[969 * 128];
+    uint16_t best3[153 * 32];
+    uint16_t hash4[4096];
+    uint16_t hash3[256];
+    float4 factors4[969];
+    float4 factors3[153];
+    uint32_t orders4[969];
+    uint32_t orders3[153];
+    uint32_t match5[4][256];
+    uint32_t match6[4][256];
+};
+static_assert(sizeof(DevTables) == sizeof(HostTables), "device and host table images must match");
+
+__device__ DevTables g_tab;
+
+// Color::PreciseRound565 rounding points (Color.h:87-95); the values must be
+// these exact floats for the rounding to match.
+__constant__ float c_mid5[32] = {.015686f, .047059f, .078431f, .111765f, .145098f, .176471f, .207843f, .241176f,
+                                 .274510f, .305882f, .337255f, .370588f, .403922f, .435294f, .466667f, .5f,
+                                 .533333f, .564706f, .596078f, .629412f, .662745f, .694118f, .725490f, .758824f,
+                                 .792157f, .823529f, .854902f, .888235f, .921569f, .952941f, .984314f, 1e+37f};
+__constant__ float c_mid6[64] = {
+    .007843f, .023529f, .039216f, .054902f, .070588f, .086275f, .101961f, .117647f, .133333f, .149020f, .164706f,
+    .180392f, .196078f, .211765f, .227451f, .245098f, .262745f, .278431f, .294118f, .309804f, .325490f, .341176f,
+    .356863f, .372549f, .388235f, .403922f, .419608f, .435294f, .450980f, .466667f, .482353f, .500000f, .517647f,
+    .533333f, .549020f, .564706f, .580392f, .596078f, .611765f, .627451f, .643137f, .658824f, .674510f, .690196f,
+    .705882f, .721569f, .737255f, .754902f, .772549f, .788235f, .803922f, .819608f, .835294f, .850980f, .866667f,
+    .882353f, .898039f, .913725f, .929412f, .945098f, .960784f, .976471f, .992157f, 1e+37f};
+
+// EndpointSearch voxel steps (BC1Encoder.cpp:933-950): dr, dg, db in 2-bit
+// two's complement fields (bits 0-1, 2-3, 4-5) and the opposite step's index
+// in bits 8-11.
+__constant__ uint16_t c_voxels[16] = {
+    0x301, 0x404, 0x510, 0x003, 0x10C, 0x230, 0x905, 0xA11, 0xB14, 0x60F, 0x733, 0x83C, 0xD07, 0xC0D, 0xF1C, 0xE34};
+
+constexpr int CM_INCOMPLETE = 0x00, CM_THREE = 0x03, CM_FOUR = 0x04, CM_TB = 0x13;
+constexpr int EM_NONE = 0, EM_FASTER = 1, EM_CHECK2 = 2, EM_FULL = 3;
+constexpr int EP_LS = 0, EP_BB = 1, EP_BBINT = 2, EP_PCA = 3;
+constexpr int IT_IDEAL = 0, IT_ROUND = 1, IT_NVIDIA = 2, IT_AMD = 3;
+
+constexpr int kGroupsPerCta = 8;  // 16-lane groups per 128-thread CTA
+
+// BC4 selector for each threshold count (BC4Encoder.cpp:46 Levels {1,7,6,5,4,3,2,0}), 3 bits each
+constexpr uint32_t kBC4Levels = 1u | (7u << 3) | (6u << 6) | (5u << 9) | (4u << 12) | (3u << 15) | (2u << 18) | (0u << 21);
+
+// ---------------------------------------------------------------------------
+// scalar helpers (util.h:110-154, Color.cpp)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int s8to5(int v) { int v2 = v * 31 + 128; return (v2 + (v2 >> 8)) >> 8; }
+__device__ __forceinline__ int s8to6(int v) { int v2 = v * 63 + 128; return (v2 + (v2 >> 8)) >> 8; }
+__device__ __forceinline__ int s5to8(int v) { return (v << 3) | (v >> 2); }
+__device__ __forceinline__ int s6to8(int v) { return (v << 2) | (v >> 4); }
+__device__ __forceinline__ int clampi(int v, int lo, int hi) { return v < lo ? lo : (v > hi ? hi : v); }
+__device__ __forceinline__ int clamp255(int i) { return ((unsigned)i & 0xFFFFFF00u) ? ((~(i >> 31)) & 0xFF) : i; }
+// float -> int with x86 cvttss2si semantics (INT_MIN when out of range or NaN)
+__device__ __forceinline__ int f2i_x86(float v) {
+    return (v > -2147483904.0f && v < 2147483648.0f) ? __float2int_rz(v) : INT_MIN;
+}
+// 5:6:5 endpoint packed as Pack565Unscaled (Color.cpp:41-46)
+__device__ __forceinline__ int epr(int e) { return e >> 11; }
+__device__ __forceinline__ int epg(int e) { return (e >> 5) & 63; }
+__device__ __forceinline__ int epb(int e) { return e & 31; }
+__device__ __forceinline__ int eppack(int r, int g, int b) { return (r << 11) | (g << 5) | b; }
+__device__ __forceinline__ int sel4(int a0, int a1, int a2, int a3, int s) {
+    return s == 0 ? a0 : (s == 1 ? a1 : (s == 2 ? a2 : a3));
+}
+__device__ __forceinline__ float sel4f(float a0, float a1, float a2, float a3, int s) {
+    return s == 0 ? a0 : (s == 1 ? a1 : (s == 2 ? a2 : a3));
+}
+__device__ __forceinline__ unsigned sq3(int a, int b, int c) { return (unsigned)(a * a + b * b + c * c); }
+
+// Color::PreciseRound565 (Color.cpp:66-86)
+__device__ __forceinline__ int precise_round565(float v0, float v1, float v2, const float *mid5, const float *mid6) {
+    int r = clampi(f2i_x86(__fmul_rn(v0, 31.0f)), 0, 31);
+    int g = clampi(f2i_x86(__fmul_rn(v1, 63.0f)), 0, 63);
+    int b = clampi(f2i_x86(__fmul_rn(v2, 31.0f)), 0, 31);
+    r += v0 > mid5[r];
+    g += v1 > mid6[g];
+    b += v2 > mid5[b];
+    return eppack(r, g, b);
+}
+
+// ---------------------------------------------------------------------------
+// interpolators (Interpolator.cpp:47-138)
+// ---------------------------------------------------------------------------
+template <int IT> __device__ __forceinline__ int i8(int a, int b) {
+    if (IT == IT_ROUND) return (a * 2 + b + 1) / 3;
+    if (IT == IT_AMD) return (a * 43 + b * 21 + 32) >> 6;
+    return (a * 2 + b) / 3;
+}
+template <int IT> __device__ __forceinline__ int h8(int a, int b) { return IT == IT_AMD ? ((a + b + 1) >> 1) : ((a + b) / 2); }
+__device__ __forceinline__ int nv5(int a, int b) { return ((2 * a + b) * 22) / 8; }
+__device__ __forceinline__ int nv6(int a, int b) { int gd = b - a; return (256 * a + (gd / 4) + 128 + gd * 80) >> 8; }
+__device__ __forceinline__ int nvh5(int a, int b) { return ((a + b) * 33) / 8; }
+__device__ __forceinline__ int nvh6(int a, int b) { int gd = b - a; return (256 * a + gd / 4 + 128 + gd * 128) >> 8; }
+
+// Palette in FindSelectors' internal selector order (BC1Encoder.cpp:684-693):
+// four colours {c0, c2, c3, c1}, three colours {c0, c2, c1, c3=black}.
+struct Pal {
+    int r0, g0, b0, r1, g1, b1, r2, g2, b2, r3, g3, b3;
+};
+
+template <int IT> __device__ __forceinline__ Pal make_pal(int lo, int hi, bool three) {
+    const int lr = epr(lo), lg = epg(lo), lb = epb(lo), hr = epr(hi), hg = epg(hi), hb = epb(hi);
+    const int ar = s5to8(lr), ag = s6to8(lg), ab = s5to8(lb);  // colors[0]
+    const int br = s5to8(hr), bg = s6to8(hg), bb = s5to8(hb);  // colors[1]
+    int cr, cg, cb, dr, dg, db;                                // colors[2], colors[3]
+    if (IT == IT_NVIDIA) {
+        if (!three) {
+            cr = nv5(lr, hr); cg = nv6(lg, hg); cb = nv5(lb, hb);
+            dr = nv5(hr, lr); dg = nv6(hg, lg); db = nv5(hb, lb);
+        } else {
+            cr = nvh5(lr, hr); cg = nvh6(lg, hg); cb = nvh5(lb, hb);
+            dr = dg = db = 0;
+        }
+    } else if (three) {
+        cr = h8<IT>(ar, br); cg = h8<IT>(ag, bg); cb = h8<IT>(ab, bb);
+        dr = dg = db = 0;
+    } else {
+        cr = i8<IT>(ar, br); cg = i8<IT>(ag, bg); cb = i8<IT>(ab, bb);
+        dr = i8<IT>(br, ar); dg = i8<IT>(bg, ag); db = i8<IT>(bb, ab);
+    }
+    Pal p;
+    p.r0 = ar; p.g0 = ag; p.b0 = ab;
+    p.r1 = cr; p.g1 = cg; p.b1 = cb;
+    if (!three) {
+        p.r2 = dr; p.g2 = dg; p.b2 = db;
+        p.r3 = br; p.g3 = bg; p.b3 = bb;
+    } else {
+        p.r2 = br; p.g2 = bg; p.b2 = bb;
+        p.r3 = dr; p.g3 = dg; p.b3 = db;
+    }
+    return p;
+}
+
+// ---------------------------------------------------------------------------
+// per-group context
+// ---------------------------------------------------------------------------
+struct Ctx {
+    unsigned gm;     // this group's 16 lanes in the warp
+    int lane;        // 0..15 = texel index (x = lane & 3, y = lane >> 2)
+    int pr, pg, pb, pa;
+    uint32_t *spx;   // shared: the block's 16 texels (RGBA8 packed)
+    int *ssum;       // shared: cluster-fit prefix sums [17][3]
+    const float *mid5, *mid6;
+    const uint16_t *vox;
+};
+
+struct Res {  // EncodeResults (BC1Encoder.h:147-153); endpoints packed 5:6:5
+    int lo, hi;
+    uint32_t sel;  // 16 x 2-bit internal selectors, texel i at bits 2i
+    int mode;
+    uint32_t err;
+};
+
+__device__ __forceinline__ Res res_init() {
+    Res r;
+    r.lo = r.hi = 0;
+    r.sel = 0;
+    r.mode = CM_INCOMPLETE;
+    r.err = UINT_MAX;
+    return r;
+}
+
+struct Metrics {  // ColorBlock::Metrics (ColorBlock.h:30-37)
+    int mn[3], mx[3], av[3], sum[3];
+    bool grey, has_black;
+};
+
+__device__ __forceinline__ unsigned gsum(unsigned m, unsigned v) { return __reduce_add_sync(m, v); }
+__device__ __forceinline__ unsigned gmin(unsigned m, unsigned v) { return __reduce_min_sync(m, v); }
+__device__ __forceinline__ unsigned gmax(unsigned m, unsigned v) { return __reduce_max_sync(m, v); }
+__device__ __forceinline__ unsigned gor(unsigned m, unsigned v) { return __reduce_or_sync(m, v); }
+
+// ColorBlock::GetMetrics (ColorBlock.h:88-117)
+__device__ Metrics get_metrics(const Ctx &C, bool ignore_black) {
+    Metrics m;
+    const bool blk = (C.pr | C.pg | C.pb) < 4;
+    m.has_black = __any_sync(C.gm, blk);
+    const bool inc = !(ignore_black && blk);
+    m.grey = __all_sync(C.gm, !inc || (C.pr == C.pg && C.pr == C.pb));
+    const int p[3] = {C.pr, C.pg, C.pb};
+    const int total = __popc(__ballot_sync(C.gm, inc) & C.gm);
+#pragma unroll
+    for (int c = 0; c < 3; c++) {
+        m.mn[c] = (int)gmin(C.gm, inc ? p[c] : 255);
+        m.mx[c] = (int)gmax(C.gm, inc ? p[c] : 0);
+        m.sum[c] = (int)gsum(C.gm, inc ? p[c] : 0);
+        m.av[c] = total > 0 ? (m.sum[c] + total / 2) / total : 0;
+    }
+    return m;
+}
+
+// ---------------------------------------------------------------------------
+// FindSelectors<M>, texel-parallel (BC1Encoder.cpp:679-779)
+// ---------------------------------------------------------------------------
+template <int IT>
+__device__ __forceinline__ void find_selectors_tp(const Ctx &C, int M, int em, Res &r) {
+    const bool three = (M & 0x0F) == 3;
+    const Pal P = make_pal<IT>(r.lo, r.hi, three);
+    int s;
+    unsigned e;
+    if (em == EM_NONE || em == EM_FASTER) {
+        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
+        const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
+        const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
+        const int t0 = d0 + d1, t1 = d1 + d2, t2 = d2 + d3;
+        const int dot = 2 * ar * C.pr + 2 * ag * C.pg + 2 * ab * C.pb;
+        const int level = (dot <= t0) + (dot < t1) + (dot < t2);
+        s = 3 - level;
+        e = em == EM_FASTER ? sq3(C.pr - sel4(P.r0, P.r1, P.r2, P.r3, s), C.pg - sel4(P.g0, P.g1, P.g2, P.g3, s),
+                                  C.pb - sel4(P.b0, P.b1, P.b2, P.b3, s))
+                            : 0u;
+    } else if (em == EM_CHECK2) {
+        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
+        const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
+        const int dd = (C.pr - P.r0) * ar + (C.pg - P.g0) * ag + (C.pb - P.b0) * ab;
+        const float sf = __fadd_rn(__fmul_rn(__int2float_rn(dd), f), 0.5f);
+        const int sl = clampi(f2i_x86(sf), 1, 3);
+        const unsigned e0 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - C.pr, sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - C.pg,
+                                sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - C.pb);
+        const unsigned e1 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl) - C.pr, sel4(P.g0, P.g1, P.g2, P.g3, sl) - C.pg,
+                                sel4(P.b0, P.b1, P.b2, P.b3, sl) - C.pb);
+        s = sl;
+        e = e1;
+        if (e0 == e1) {
+            if (s == 1) s = 0;
+        } else if (e0 < e) {
+            s = sl - 1;
+            e = e0;
+        }
+    } else {
+        const unsigned e0 = sq3(P.r0 - C.pr, P.g0 - C.pg, P.b0 - C.pb);
+        const unsigned e1 = sq3(P.r1 - C.pr, P.g1 - C.pg, P.b1 - C.pb);
+        const unsigned e2 = sq3(P.r2 - C.pr, P.g2 - C.pg, P.b2 - C.pb);
+        s = 0;
+        e = e0;
+        if (e1 < e) { e = e1; s = 1; }
+        if (e2 < e) { e = e2; s = 2; }
+        if (M != CM_THREE) {
+            const unsigned e3 = sq3(P.r3 - C.pr, P.g3 - C.pg, P.b3 - C.pb);
+            if (e3 <= e) { e = e3; s = 3; }  // ties prefer selector 3 (:762)
+        }
+    }
+    r.err = gsum(C.gm, e);
+    r.sel = gor(C.gm, (unsigned)s << (2 * C.lane));
+    r.mode = M;
+}
+
+// ---------------------------------------------------------------------------
+// lane-serial block error: one lane evaluates all 16 texels for its own
+// endpoints (error only; selectors are recomputed texel-parallel for winners)
+// ---------------------------------------------------------------------------
+struct Px {
+    float r[16], g[16], b[16];
+};
+
+__device__ __forceinline__ void load_px(const Ctx &C, Px &X) {
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const uint32_t v = C.spx[i];
+        X.r[i] = (float)(v & 0xFF);
+        X.g[i] = (float)((v >> 8) & 0xFF);
+        X.b[i] = (float)((v >> 16) & 0xFF);
+    }
+}
+
+// kinds of lane-serial evaluation
+constexpr int K_NONE = 0, K_FASTER = 1, K_CHECK2 = 2, K_FULL4 = 3, K_FULL3 = 4;
+
+__device__ __forceinline__ int eval_kind(int M, int em) {
+    if (M == CM_FOUR) return em == EM_FULL ? K_FULL4 : (em == EM_CHECK2 ? K_CHECK2 : (em == EM_FASTER ? K_FASTER : K_NONE));
+    if (M == CM_THREE) return em == EM_FULL ? K_FULL3 : (em == EM_CHECK2 ? K_CHECK2 : (em == EM_FASTER ? K_FASTER : K_NONE));
+    return em == EM_FULL ? K_FULL4 : (em == EM_CHECK2 ? K_CHECK2 : (em == EM_FASTER ? K_FASTER : K_NONE));
+}
+
+template <int IT>
+__device__ __forceinline__ float block_err(const Px &X, int kind, int lo, int hi, bool three) {
+    const Pal P = make_pal<IT>(lo, hi, three);
+    float tot = 0.0f;
+    if (kind == K_FULL4 || kind == K_FULL3) {
+        // sum_t min_j |p_t - c_j|^2 = sum_t |p_t|^2 + sum_t min_j (|c_j|^2 - 2 p_t.c_j); all terms exact
+        const float v0 = (float)sq3(P.r0, P.g0, P.b0), v1 = (float)sq3(P.r1, P.g1, P.b1);
+        const float v2 = (float)sq3(P.r2, P.g2, P.b2), v3 = (float)sq3(P.r3, P.g3, P.b3);
+        const float r0 = -2.0f * P.r0, g0 = -2.0f * P.g0, b0 = -2.0f * P.b0;
+        const float r1 = -2.0f * P.r1, g1 = -2.0f * P.g1, b1 = -2.0f * P.b1;
+        const float r2 = -2.0f * P.r2, g2 = -2.0f * P.g2, b2 = -2.0f * P.b2;
+        const float r3 = -2.0f * P.r3, g3 = -2.0f * P.g3, b3 = -2.0f * P.b3;
+        const bool four = kind == K_FULL4;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const float pr = X.r[i], pg = X.g[i], pb = X.b[i];
+            float m = fmaf(pb, b0, fmaf(pg, g0, fmaf(pr, r0, v0)));
+            m = fminf(m, fmaf(pb, b1, fmaf(pg, g1, fmaf(pr, r1, v1))));
+            m = fminf(m, fmaf(pb, b2, fmaf(pg, g2, fmaf(pr, r2, v2))));
+            if (four) m = fminf(m, fmaf(pb, b3, fmaf(pg, g3, fmaf(pr, r3, v3))));
+            tot += fmaf(pb, pb, fmaf(pg, pg, fmaf(pr, pr, m)));
+        }
+    } else if (kind == K_FASTER) {
+        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
+        const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
+        const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
+        const float t0 = (float)(d0 + d1), t1 = (float)(d1 + d2), t2 = (float)(d2 + d3);
+        const float a2r = 2.0f * ar, a2g = 2.0f * ag, a2b = 2.0f * ab;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const float pr = X.r[i], pg = X.g[i], pb = X.b[i];
+            const float dot = fmaf(pb, a2b, fmaf(pg, a2g, pr * a2r));
+            const int s = 3 - ((int)(dot <= t0) + (int)(dot < t1) + (int)(dot < t2));  // selector = 3 - level
+            const float cr = (float)sel4(P.r0, P.r1, P.r2, P.r3, s), cg = (float)sel4(P.g0, P.g1, P.g2, P.g3, s);
+            const float cb = (float)sel4(P.b0, P.b1, P.b2, P.b3, s);
+            const float dr = pr - cr, dg = pg - cg, db = pb - cb;
+            tot += fmaf(db, db, fmaf(dg, dg, dr * dr));
+        }
+    } else if (kind == K_CHECK2) {
+        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
+        const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
+        const float far_ = (float)ar, fag = (float)ag, fab = (float)ab;
+        const float c0r = (float)P.r0, c0g = (float)P.g0, c0b = (float)P.b0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const float pr = X.r[i], pg = X.g[i], pb = X.b[i];
+            const float dd = fmaf(pb - c0b, fab, fmaf(pg - c0g, fag, (pr - c0r) * far_));
+            const float sf = __fadd_rn(__fmul_rn(dd, f), 0.5f);
+            const int sl = clampi(f2i_x86(sf), 1, 3);
+            const float ar0 = (float)sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - pr;
+            const float ag0 = (float)sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - pg;
+            const float ab0 = (float)sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - pb;
+            const float ar1 = (float)sel4(P.r0, P.r1, P.r2, P.r3, sl) - pr;
+            const float ag1 = (float)sel4(P.g0, P.g1, P.g2, P.g3, sl) - pg;
+            const float ab1 = (float)sel4(P.b0, P.b1, P.b2, P.b3, sl) - pb;
+            const float e0 = fmaf(ab0, ab0, fmaf(ag0, ag0, ar0 * ar0));
+            const float e1 = fmaf(ab1, ab1, fmaf(ag1, ag1, ar1 * ar1));
+            tot += fminf(e0, e1);
+        }
+    }
+    return tot;
+}
+
+// ---------------------------------------------------------------------------
+// FindEndpointsSingleColor(result, pixels, color, is_3color), texel-parallel
+// (BC1Encoder.cpp:443-471). The error is taken against colors[2] of the
+// endpoints held before the lookup, over RGBA (palette alpha 255).
+// ---------------------------------------------------------------------------
+template <int IT>
+__device__ __forceinline__ void single_color_px(const Ctx &C, int stale_lo, int stale_hi, const int av[3], bool is3,
+                                                int &lo, int &hi, uint32_t &err) {
+    const Pal P = make_pal<IT>(stale_lo, stale_hi, is3);  // colors[2] is internal index 1 in both orders
+    const int dr = C.pr - P.r1, dg = C.pg - P.g1, db = C.pb - P.b1, da = C.pa - 255;
+    err = gsum(C.gm, (unsigned)(dr * dr + dg * dg + db * db + da * da));
+    const uint32_t mr = g_tab.match5[IT][av[0]], mg = g_tab.match6[IT][av[1]], mb = g_tab.match5[IT][av[2]];
+    lo = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
+    hi = eppack(mr & 0xFF, mg & 0xFF, mb & 0xFF);
+}
+
+// ---------------------------------------------------------------------------
+// FindEndpoints (BC1Encoder.cpp:473-677), texel-parallel
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float fdot4_rn(float a0, float a1, float a2, float a3, float b0, float b1, float b2, float b3) {
+    // Vector4::Dot (Vector4.h:53-57): sum from 0, left to right
+    float s = __fadd_rn(0.0f, __fmul_rn(a0, b0));
+    s = __fadd_rn(s, __fmul_rn(a1, b1));
+    s = __fadd_rn(s, __fmul_rn(a2, b2));
+    return __fadd_rn(s, __fmul_rn(a3, b3));
+}
+
+template <int IT>
+__device__ void find_endpoints(const Ctx &C, Res &r, const Metrics &m, int mode, bool ignore_black, int power_iters) {
+    if (m.grey) {  // :474-494
+        const int fr = __shfl_sync(C.gm, C.pr, 0, 16);
+        if (m.mx[0] - m.mn[0] < 2) {
+            r.lo = r.hi = eppack(s8to5(fr), s8to6(fr), s8to5(fr));
+        } else {
+            r.lo = eppack(s8to5(m.mn[0]), s8to6(m.mn[0]), s8to5(m.mn[0]));
+            r.hi = eppack(s8to5(m.mx[0]), s8to6(m.mx[0]), s8to5(m.mx[0]));
+        }
+    } else if (mode == EP_LS) {  // :495-552
+        const int d0 = m.mx[0] - m.mn[0], d1 = m.mx[1] - m.mn[1], d2 = m.mx[2] - m.mn[2];
+        const int c0 = (d0 >= d1 && d0 >= d2) ? 0 : ((d1 >= d2 && d1 >= d0) ? 1 : 2);  // Color::MaxChannelRGB
+        const int p[3] = {C.pr, C.pg, C.pb};
+        const int px0 = c0 == 0 ? C.pr : (c0 == 1 ? C.pg : C.pb);
+        unsigned sxy[3];
+#pragma unroll
+        for (int c = 0; c < 3; c++) sxy[c] = gsum(C.gm, (unsigned)(px0 * p[c]));  // zero-initialised (:510 is not)
+        float l[3] = {0.f, 0.f, 0.f}, h[3] = {0.f, 0.f, 0.f};
+        const float mn0 = (float)m.mn[c0];
+        l[c0] = mn0;
+        h[c0] = mn0;
+        const unsigned sum_x = (unsigned)m.sum[c0], sum_xx = sxy[c0];
+        const float den = __fsub_rn(__uint2float_rn(16u * sum_xx), __uint2float_rn(sum_x * sum_x));
+        if (fabsf(den) > 1e-8f) {
+#pragma unroll
+            for (int i = 1; i < 3; i++) {
+                const int c = (c0 + i) % 3;
+                const unsigned sum_y = (unsigned)m.sum[c], sum_xy = sxy[c];
+                const float a = __fdiv_rn(__uint2float_rn((16u * sum_xy) - (sum_x * sum_y)), den);
+                const float b = __fdiv_rn(__uint2float_rn((sum_xx * sum_y) - (sum_xy * sum_x)), den);
+                l[c] = __fadd_rn(b, __fmul_rn(a, l[c0]));
+                h[c] = __fadd_rn(b, __fmul_rn(a, h[c0]));
+            }
+        }
+#pragma unroll
+        for (int c = 0; c < 3; c++) {
+            const float inset = __fdiv_rn(__fsub_rn(h[c], l[c]), 16.0f);
+            l[c] = __fdiv_rn(__fadd_rn(l[c], inset), 255.0f);
+            h[c] = __fdiv_rn(__fsub_rn(h[c], inset), 255.0f);
+        }
+        r.lo = precise_round565(l[0], l[1], l[2], C.mid5, C.mid6);
+        r.hi = precise_round565(h[0], h[1], h[2], C.mid5, C.mid6);
+    } else if (mode == EP_BB || mode == EP_BBINT) {  // :553-605
+        const int b = C.pb - m.av[2];
+        const int cxz = (int)gsum(C.gm, (unsigned)(b * C.pr - m.av[0]));  // b * r - avg.r, as written (:572)
+        const int cyz = (int)gsum(C.gm, (unsigned)(b * C.pg - m.av[1]));
+        if (mode == EP_BB) {
+            const float bias = __fdiv_rn(8.0f, 255.0f);
+            float l[3], h[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                l[c] = __fdiv_rn((float)m.mn[c], 255.0f);
+                h[c] = __fdiv_rn((float)m.mx[c], 255.0f);
+                const float inset = __fdiv_rn(__fsub_rn(__fsub_rn(h[c], l[c]), bias), 16.0f);
+                l[c] = __fadd_rn(l[c], inset);
+                h[c] = __fsub_rn(h[c], inset);
+            }
+            if (cxz < 0) { const float t = l[0]; l[0] = h[0]; h[0] = t; }
+            if (cyz < 0) { const float t = l[1]; l[1] = h[1]; h[1] = t; }
+            r.lo = precise_round565(l[0], l[1], l[2], C.mid5, C.mid6);
+            r.hi = precise_round565(h[0], h[1], h[2], C.mid5, C.mid6);
+        } else {
+            int mn[3], mx[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) {
+                const int inset = ((m.mx[c] - m.mn[c]) - 8) >> 4;
+                mn[c] = clamp255(m.mn[c] + inset);
+                mx[c] = clamp255(m.mx[c] - inset);
+            }
+            if (cxz < 0) { const int t = mn[0]; mn[0] = mx[0]; mx[0] = t; }
+            if (cyz < 0) { const int t = mn[1]; mn[1] = mx[1]; mx[1] = t; }
+            r.lo = eppack(s8to5(mn[0]), s8to6(mn[1]), s8to5(mn[2]));
+            r.hi = eppack(s8to5(mx[0]), s8to6(mx[1]), s8to5(mx[2]));
+        }
+    } else {  // PCA, :606-674
+        const bool blk = (C.pr | C.pg | C.pb) < 4;
+        const bool inc = !(ignore_black && blk);
+        const int dr = C.pr - m.av[0], dg = C.pg - m.av[1], db = C.pb - m.av[2];
+        // covariance from identity, accumulated over included texels: exact integers
+        const int s00 = (int)gsum(C.gm, inc ? (unsigned)(dr * dr) : 0u);
+        const int s01 = (int)gsum(C.gm, inc ? (unsigned)(dr * dg) : 0u);
+        const int s02 = (int)gsum(C.gm, inc ? (unsigned)(dr * db) : 0u);
+        const int s11 = (int)gsum(C.gm, inc ? (unsigned)(dg * dg) : 0u);
+        const int s12 = (int)gsum(C.gm, inc ? (unsigned)(dg * db) : 0u);
+        const int s22 = (int)gsum(C.gm, inc ? (unsigned)(db * db) : 0u);
+        const float k255 = 255.0f;
+        const float c00 = __fdiv_rn((float)(1 + s00), k255), c01 = __fdiv_rn((float)s01, k255);
+        const float c02 = __fdiv_rn((float)s02, k255), c11 = __fdiv_rn((float)(1 + s11), k255);
+        const float c12 = __fdiv_rn((float)s12, k255), c22 = __fdiv_rn((float)(1 + s22), k255);
+        const float c33 = __fdiv_rn(1.0f, k255), z = __fdiv_rn(0.0f, k255);
+        float d0 = __fsub_rn((float)m.mx[0], (float)m.mn[0]);
+        float d1 = __fsub_rn((float)m.mx[1], (float)m.mn[1]);
+        float d2 = __fsub_rn((float)m.mx[2], (float)m.mn[2]);
+        float d3 = __fsub_rn(0.0f, 0.0f);
+        if (c02 < 0) d0 = -d0;
+        if (c12 < 0) d1 = -d1;
+        for (int it = 0; it < power_iters; it++) {  // Matrix4x4 * Vector4 (Matrix4x4.cpp:33-39), mirrored rows
+            const float n0 = fdot4_rn(d0, d1, d2, d3, c00, c01, c02, z);
+            const float n1 = fdot4_rn(d0, d1, d2, d3, c01, c11, c12, z);
+            const float n2 = fdot4_rn(d0, d1, d2, d3, c02, c12, c22, z);
+            const float n3 = fdot4_rn(d0, d1, d2, d3, z, z, z, c33);
+            d0 = n0; d1 = n1; d2 = n2; d3 = n3;
+        }
+        float k = 0.0f;  // Vector4::MaxAbs(3)
+        if (fabsf(d0) > k) k = fabsf(d0);
+        if (fabsf(d1) > k) k = fabsf(d1);
+        if (fabsf(d2) > k) k = fabsf(d2);
+        float a0 = 306.0f, a1 = 601.0f, a2 = 117.0f, a3 = 0.0f;
+        if (k >= 2) {
+            const float s = __fdiv_rn(2048.0f, k);
+            a0 = __fmul_rn(d0, s); a1 = __fmul_rn(d1, s); a2 = __fmul_rn(d2, s); a3 = __fmul_rn(d3, s);
+        }
+        a0 = __fmul_rn(a0, 16.0f); a1 = __fmul_rn(a1, 16.0f); a2 = __fmul_rn(a2, 16.0f); a3 = __fmul_rn(a3, 16.0f);
+        const float dot = fdot4_rn((float)C.pr, (float)C.pg, (float)C.pb, 0.0f, a0, a1, a2, a3);
+        // first index of the maximum / minimum (strict > / < scan, :654-670)
+        float vmax = inc ? dot : -INFINITY, vmin = inc ? dot : INFINITY;
+        int imax = C.lane, imin = C.lane;
+#pragma unroll
+        for (int off = 8; off >= 1; off >>= 1) {
+            const float ov = __shfl_xor_sync(C.gm, vmax, off, 16);
+            const int oi = __shfl_xor_sync(C.gm, imax, off, 16);
+            if (ov > vmax || (ov == vmax && oi < imax)) { vmax = ov; imax = oi; }
+            const float ow = __shfl_xor_sync(C.gm, vmin, off, 16);
+            const int oj = __shfl_xor_sync(C.gm, imin, off, 16);
+            if (ow < vmin || (ow == vmin && oj < imin)) { vmin = ow; imin = oj; }
+        }
+        const uint32_t pmin = C.spx[imin], pmax = C.spx[imax];
+        r.lo = eppack(s8to5(pmin & 0xFF), s8to6((pmin >> 8) & 0xFF), s8to5((pmin >> 16) & 0xFF));
+        r.hi = eppack(s8to5(pmax & 0xFF), s8to6((pmax >> 8) & 0xFF), s8to5((pmax >> 16) & 0xFF));
+    }
+    r.mode = CM_INCOMPLETE;
+}
+
+// ---------------------------------------------------------------------------
+// RefineEndpointsLS<FourColor>(result, pixels, metrics) (BC1Encoder.cpp:781-825).
+// Only the FourColor instantiation is ever called (RefineBlockLS, :860): no
+// texel is skipped and the 4-colour weights apply to every colour mode.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool refine_endpoints_ls_px(const Ctx &C, Res &r, const Metrics &m) {
+    const int s = (r.sel >> (2 * C.lane)) & 3;
+    const unsigned b1 = __ballot_sync(C.gm, s == 1) & C.gm, b2 = __ballot_sync(C.gm, s == 2) & C.gm;
+    const unsigned b3 = __ballot_sync(C.gm, s == 3) & C.gm;
+    const int n1 = __popc(b1), n2 = __popc(b2), n3 = __popc(b3), n0 = 16 - n1 - n2 - n3;
+    // sum of OrderTable<4>::Weights[sel]: {s^2, s(3-s), s(3-s), (3-s)^2}
+    float m0 = (float)(n1 + 4 * n2 + 9 * n3), m1 = (float)(2 * n1 + 2 * n2), m2 = m1, m3 = (float)(9 * n0 + 4 * n1 + n2);
+    const float q00r = (float)(int)gsum(C.gm, (unsigned)(C.pr * s));
+    const float q00g = (float)(int)gsum(C.gm, (unsigned)(C.pg * s));
+    const float q00b = (float)(int)gsum(C.gm, (unsigned)(C.pb * s));
+    const float det = __fsub_rn(__fmul_rn(m0, m3), __fmul_rn(m1, m2));
+    if (fabsf(det) < 1e-8f) {
+        r.mode = CM_INCOMPLETE;
+        return false;
+    }
+    const float t = m0; m0 = m3; m3 = t;
+    m1 = -m1;
+    m2 = -m2;
+    const float sc = __fdiv_rn(__fdiv_rn(3.0f, 255.0f), det);
+    m0 = __fmul_rn(m0, sc); m1 = __fmul_rn(m1, sc); m2 = __fmul_rn(m2, sc); m3 = __fmul_rn(m3, sc);
+    const float q10r = (float)(m.sum[0] * 3) - q00r, q10g = (float)(m.sum[1] * 3) - q00g, q10b = (float)(m.sum[2] * 3) - q00b;
+    r.mode = CM_FOUR;
+    r.lo = precise_round565(__fadd_rn(__fmul_rn(m0, q00r), __fmul_rn(m1, q10r)),
+                            __fadd_rn(__fmul_rn(m0, q00g), __fmul_rn(m1, q10g)),
+                            __fadd_rn(__fmul_rn(m0, q00b), __fmul_rn(m1, q10b)), C.mid5, C.mid6);
+    r.hi = precise_round565(__fadd_rn(__fmul_rn(m2, q00r), __fmul_rn(m3, q10r)),
+                            __fadd_rn(__fmul_rn(m2, q00g), __fmul_rn(m3, q10g)),
+                            __fadd_rn(__fmul_rn(m2, q00b), __fmul_rn(m3, q10b)), C.mid5, C.mid6);
+    return true;
+}
+
+// RefineBlockLS<M> (BC1Encoder.cpp:852-875)
+template <int IT>
+__device__ void refine_block_ls(const Ctx &C, int M, Res &r, const Metrics &m, int em, int passes) {
+    for (int pass = 0; pass < passes; pass++) {
+        Res t = r;
+        if (!refine_endpoints_ls_px(C, t, m)) {
+            int lo, hi;
+            uint32_t err;
+            single_color_px<IT>(C, t.lo, t.hi, m.av, M != CM_FOUR, lo, hi, err);
+            t.lo = lo;
+            t.hi = hi;
+            t.err = err;
+            t.sel = 0x55555555u;
+            t.mode = M != CM_FOUR ? CM_THREE : CM_FOUR;
+        } else {
+            find_selectors_tp<IT>(C, M, em, t);
+        }
+        if (t.lo == r.lo && t.hi == r.hi) break;
+        if (em == EM_NONE || t.err < r.err) r = t;
+        else return;
+    }
+}
+
+__device__ __forceinline__ bool is_single_hash(bool four, int h) {
+    return four ? (h == 15 || h == 700 || h == 753 || h == 515) : (h == 12 || h == 15 || h == 89);
+}
+
+// ---------------------------------------------------------------------------
+// RefineBlockCF<M> (BC1Encoder.cpp:877-928), ordering-parallel
+// ---------------------------------------------------------------------------
+template <int IT>
+__device__ void refine_block_cf(const Ctx &C, int M, Res &r, const Metrics &m, int em, unsigned orderings, bool exhaustive) {
+    const bool four = (M & 0x0F) == 4;
+    const Res orig = r;
+    // Histogram of the selectors -> start ordering (OrderTable::GetHash, OrderTable.h:91-104)
+    const uint32_t w = orig.sel;
+    const int n1 = __popc(w & ~(w >> 1) & 0x55555555u), n2 = __popc(~w & (w >> 1) & 0x55555555u);
+    const int n3 = __popc(w & (w >> 1) & 0x55555555u), n0 = 16 - n1 - n2 - n3;
+    int start;
+    if (four) {  // SingleColorHashes (OrderTable.cpp:43-44), looked up by bin
+        start = n0 == 16 ? 15 : n1 == 16 ? 700 : n2 == 16 ? 753 : n3 == 16 ? 515 : (int)g_tab.hash4[n0 | (n1 << 4) | (n2 << 8)];
+    } else {
+        start = n0 == 16 ? 12 : n1 == 16 ? 15 : n2 == 16 ? 89 : (int)g_tab.hash3[n0 | (n1 << 4)];
+    }
+    // projection onto high - low, sort, prefix sums (:891-909); all values exact integers
+    const int axr = s5to8(epr(orig.hi)) - s5to8(epr(orig.lo));
+    const int axg = s6to8(epg(orig.hi)) - s6to8(epg(orig.lo));
+    const int axb = s5to8(epb(orig.hi)) - s5to8(epb(orig.lo));
+    const int dot = C.pr * axr + C.pg * axg + C.pb * axb;
+    const uint32_t key = ((uint32_t)(0x1000000 + dot) << 4) | (uint32_t)C.lane;
+    int rank = 0;  // keys are distinct (the texel index is in the low bits)
+#pragma unroll
+    for (int i = 0; i < 16; i++) rank += __shfl_sync(C.gm, key, i, 16) < key;
+    int sr = 0, sg = 0, sb = 0;  // sum of the texels ranked at or below this lane's position
+#pragma unroll
+    for (int j = 0; j < 16; j++) {
+        if (__shfl_sync(C.gm, rank, j, 16) <= C.lane) {
+            const uint32_t v = C.spx[j];
+            sr += v & 0xFF;
+            sg += (v >> 8) & 0xFF;
+            sb += (v >> 16) & 0xFF;
+        }
+    }
+    C.ssum[3 * (C.lane + 1) + 0] = sr;
+    C.ssum[3 * (C.lane + 1) + 1] = sg;
+    C.ssum[3 * (C.lane + 1) + 2] = sb;
+    if (C.lane == 0) C.ssum[0] = C.ssum[1] = C.ssum[2] = 0;
+    __syncwarp(C.gm);
+
+    // the single-colour trial is the same for every single-colour ordering of this call
+    int sc_lo, sc_hi;
+    uint32_t sc_err;
+    single_color_px<IT>(C, orig.lo, orig.hi, m.av, !four, sc_lo, sc_hi, sc_err);
+
+    Px X;
+    load_px(C, X);
+    const int kind = eval_kind(M, em);
+    const float denom = four ? 3.0f : 2.0f;
+    const float t16r = (float)C.ssum[48], t16g = (float)C.ssum[49], t16b = (float)C.ssum[50];
+    const unsigned total = exhaustive ? (four ? 969u : 153u) : orderings;
+    float best = INFINITY;
+    int bq = 0x7FFF, blo = 0, bhi = 0;
+    for (unsigned q = C.lane; q < total; q += 16) {
+        const int th = exhaustive ? (int)q : (four ? (int)g_tab.best4[start * 128 + q] : (int)g_tab.best3[start * 32 + q]);
+        int lo, hi;
+        float e;
+        if (is_single_hash(four, th)) {
+            lo = sc_lo;
+            hi = sc_hi;
+            e = (float)sc_err;
+        } else {
+            // RefineEndpointsLS<M>(result, sums, matrix, hash), :827-850
+            const float4 f = four ? g_tab.factors4[th] : g_tab.factors3[th];
+            const uint32_t o = four ? g_tab.orders4[th] : g_tab.orders3[th];
+            const int l1 = o & 0xFF, l2 = l1 + ((o >> 8) & 0xFF), l3 = l2 + ((o >> 16) & 0xFF);
+            int q10r = C.ssum[3 * l1] + C.ssum[3 * l2], q10g = C.ssum[3 * l1 + 1] + C.ssum[3 * l2 + 1];
+            int q10b = C.ssum[3 * l1 + 2] + C.ssum[3 * l2 + 2];
+            if (four) {
+                q10r += C.ssum[3 * l3];
+                q10g += C.ssum[3 * l3 + 1];
+                q10b += C.ssum[3 * l3 + 2];
+            }
+            const float fr = (float)q10r, fg = (float)q10g, fb = (float)q10b;
+            const float q00r = t16r * denom - fr, q00g = t16g * denom - fg, q00b = t16b * denom - fb;
+            lo = precise_round565(__fadd_rn(__fmul_rn(f.x, q00r), __fmul_rn(f.y, fr)),
+                                  __fadd_rn(__fmul_rn(f.x, q00g), __fmul_rn(f.y, fg)),
+                                  __fadd_rn(__fmul_rn(f.x, q00b), __fmul_rn(f.y, fb)), C.mid5, C.mid6);
+            hi = precise_round565(__fadd_rn(__fmul_rn(f.z, q00r), __fmul_rn(f.w, fr)),
+                                  __fadd_rn(__fmul_rn(f.z, q00g), __fmul_rn(f.w, fg)),
+                                  __fadd_rn(__fmul_rn(f.z, q00b), __fmul_rn(f.w, fb)), C.mid5, C.mid6);
+            e = block_err<IT>(X, kind, lo, hi, !four);
+        }
+        if (e < best) {
+            best = e;
+            bq = (int)q;
+            blo = lo;
+            bhi = hi;
+        }
+    }
+    const uint32_t be = best == INFINITY ? UINT_MAX : (uint32_t)best;
+    const uint32_t min_e = gmin(C.gm, be);
+    const uint32_t min_q = gmin(C.gm, be == min_e ? (uint32_t)bq : 0xFFFFu);
+    if (min_e < orig.err) {
+        const int wl = (int)(min_q & 15);
+        r.lo = __shfl_sync(C.gm, blo, wl, 16);
+        r.hi = __shfl_sync(C.gm, bhi, wl, 16);
+        r.err = min_e;
+        r.mode = M;
+        const int wth = exhaustive ? (int)min_q : (four ? (int)g_tab.best4[start * 128 + min_q] : (int)g_tab.best3[start * 32 + min_q]);
+        if (is_single_hash(four, wth)) {
+            r.sel = 0x55555555u;
+        } else {
+            Res t = r;
+            find_selectors_tp<IT>(C, M, em, t);
+            r.sel = t.sel;
+        }
+    }
+    __syncwarp(C.gm);  // ssum is rewritten by the next call
+}
+
+// ---------------------------------------------------------------------------
+// EndpointSearch (BC1Encoder.cpp:930-996), round-parallel speculation
+// ---------------------------------------------------------------------------
+template <int IT>
+__device__ void endpoint_search(const Ctx &C, Res &r, int em4, unsigned rounds) {
+    Px X;
+    load_px(C, X);
+    unsigned prev = 0, i0 = 0;
+    int forbidden = -1;
+    bool moved = false;
+    while (i0 < rounds) {
+        const unsigned i = i0 + (unsigned)C.lane;
+        const bool active = i < rounds && (int)(i & 31) != forbidden;
+        const int M = r.mode == CM_THREE ? CM_THREE : (r.mode == CM_TB ? CM_TB : CM_FOUR);
+        const int kind = eval_kind(M, M == CM_FOUR ? em4 : EM_FULL);
+        const uint16_t v = C.vox[i & 15];
+        const int ddr = ((int)((unsigned)v << 30)) >> 30, ddg = ((int)((unsigned)v << 28)) >> 30;
+        const int ddb = ((int)((unsigned)v << 26)) >> 30;
+        int lo = r.lo, hi = r.hi;
+        if (i & 16) lo = eppack(clampi(epr(lo) + ddr, 0, 31), clampi(epg(lo) + ddg, 0, 63), clampi(epb(lo) + ddb, 0, 31));
+        else hi = eppack(clampi(epr(hi) + ddr, 0, 31), clampi(epg(hi) + ddg, 0, 63), clampi(epb(hi) + ddb, 0, 31));
+        float e = INFINITY;
+        if (active) e = block_err<IT>(X, kind, lo, hi, M != CM_FOUR);
+        const bool improve = active && e < (float)r.err;
+        const bool stop = active && (i - prev > 32);
+        const unsigned sh = C.gm & 0xFFFFu ? 0 : 16;
+        const unsigned bi = (__ballot_sync(C.gm, improve) >> sh) & 0xFFFFu;
+        const unsigned bs = (__ballot_sync(C.gm, stop) >> sh) & 0xFFFFu;
+        const int fi = bi ? __ffs(bi) - 1 : 16, fs = bs ? __ffs(bs) - 1 : 16;
+        if (bi && fi <= fs) {  // the first improving round is accepted
+            const unsigned j = i0 + (unsigned)fi;
+            r.lo = __shfl_sync(C.gm, lo, fi, 16);
+            r.hi = __shfl_sync(C.gm, hi, fi, 16);
+            r.err = (uint32_t)__shfl_sync(C.gm, e, fi, 16);
+            forbidden = (int)((C.vox[j & 15] >> 8) & 15) | (int)(j & 16);
+            prev = j;
+            i0 = j + 1;
+            moved = true;
+        } else if (bs) {  // that round did not improve and i - prev > 32: stop
+            break;
+        } else {
+            i0 += 16;
+        }
+    }
+    if (moved) {  // selectors of the accepted endpoints
+        const int M = r.mode == CM_THREE ? CM_THREE : (r.mode == CM_TB ? CM_TB : CM_FOUR);
+        Res t = r;
+        find_selectors_tp<IT>(C, M, M == CM_FOUR ? em4 : EM_FULL, t);
+        r.sel = t.sel;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// block writers (BC1Encoder.cpp:345-441, BC1Block.h:66-80)
+// ---------------------------------------------------------------------------
+template <int IT>
+__device__ __forceinline__ uint2 write_block_solid(int cr, int cg, int cb, int color_mode) {
+    uint32_t mask = 0xAA;
+    int mn, mx;
+    if ((cr | cg | cb) == 0) {
+        mn = 0; mx = 1; mask = 0x55;
+    } else {
+        // FindEndpointsSingleColor(color); the 3-colour tables equal the 4-colour
+        // ones (SingleColorTable.h: N unused), so the 3-colour trial never wins.
+        const uint32_t mr = g_tab.match5[IT][cr], mg = g_tab.match6[IT][cg], mb = g_tab.match5[IT][cb];
+        const int lo = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
+        const int hi = eppack(mr & 0xFF, mg & 0xFF, mb & 0xFF);
+        mn = lo; mx = hi;
+        if (mn == mx) {
+            if (mn > 0) { mn--; mask = 0; }
+            else { mx = 1; mn = 0; mask = 0x55; }
+        } else if (mx < mn) {
+            const int t = mn; mn = mx; mx = t;
+            mask = 0xFF;
+        }
+        (void)color_mode;
+    }
+    return make_uint2((uint32_t)mx | ((uint32_t)mn << 16), mask * 0x01010101u);
+}
+
+__device__ __forceinline__ uint2 write_block(const Res &r) {
+    int ep1 = r.lo, ep0 = r.hi;
+    uint32_t lut;  // 4 x 2-bit entries
+    if (r.mode & CM_FOUR) {
+        lut = 1 | (3 << 2) | (2 << 4) | (0 << 6);
+        if (ep1 > ep0) {
+            const int t = ep1; ep1 = ep0; ep0 = t;
+            lut = 0 | (2 << 2) | (3 << 4) | (1 << 6);
+        } else if (ep1 == ep0) {
+            if (ep1 > 0) { ep1--; lut = 0; }
+            else { ep0 = 1; ep1 = 0; lut = 0x55; }
+        }
+    } else {
+        lut = 1 | (2 << 2) | (0 << 4) | (3 << 6);
+        if (ep1 < ep0) {
+            const int t = ep1; ep1 = ep0; ep0 = t;
+            lut = 0 | (2 << 2) | (1 << 4) | (3 << 6);
+        }
+    }
+    uint32_t sel = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) sel |= ((lut >> (2 * ((r.sel >> (2 * i)) & 3))) & 3) << (2 * i);
+    return make_uint2((uint32_t)ep0 | ((uint32_t)ep1 << 16), sel);
+}
+
+// ---------------------------------------------------------------------------
+// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342) for one group
+// ---------------------------------------------------------------------------
+template <int IT>
+__device__ uint2 encode_bc1_group(const Ctx &C, const qt_bc1_params &p) {
+    const uint32_t own = C.spx[C.lane];
+    if (__all_sync(C.gm, own == C.spx[0])) return write_block_solid<IT>(C.pr, C.pg, C.pb, p.color_mode);
+
+    const Metrics m = get_metrics(C, false);
+    const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
+    bool needs_err = use_likely;
+    needs_err |= p.color_mode == CM_THREE;
+    needs_err |= (p.color_mode == CM_TB) && m.has_black;
+    needs_err |= p.error_mode != EM_NONE;
+    needs_err |= p.search_rounds > 0;
+    const int em = needs_err ? p.error_mode : EM_NONE;
+    const int ls_passes = p.two_ls_passes ? 2 : 1, cf_passes = p.two_cf_passes ? 2 : 1;
+    const int ep_passes = (needs_err && p.two_ep_passes) ? 2 : 1;
+
+    Res orig = res_init(), res = res_init();
+    for (int round = 0; round < ep_passes; round++) {
+        const int mode = round == 1 ? EP_BB : p.endpoint_mode;
+        Res to = res_init();
+        find_endpoints<IT>(C, to, m, mode, false, (int)p.power_iterations);
+        Res tr = to;
+        find_selectors_tp<IT>(C, CM_FOUR, em, tr);
+        refine_block_ls<IT>(C, CM_FOUR, tr, m, em, ls_passes);
+        if (!needs_err || tr.err < res.err) {
+            res = tr;
+            orig = to;
+        }
+    }
+    if (res.err > 0 && use_likely)
+        for (int it = 0; it < cf_passes; it++) refine_block_cf<IT>(C, CM_FOUR, res, m, p.error_mode, p.orderings4, p.exhaustive);
+
+    if (res.err > 0 && (p.color_mode & CM_THREE)) {
+        Res t = orig;
+        find_selectors_tp<IT>(C, CM_THREE, EM_FULL, t);
+        refine_block_ls<IT>(C, CM_THREE, t, m, EM_FULL, ls_passes);
+        if (t.err > 0 && use_likely)
+            for (int it = 0; it < cf_passes; it++) refine_block_cf<IT>(C, CM_THREE, t, m, EM_FULL, p.orderings3, p.exhaustive);
+        if (t.err < res.err) res = t;
+    }
+
+    if (res.err > 0 && p.color_mode == CM_TB && m.has_black && !((m.mx[0] | m.mx[1] | m.mx[2]) < 4)) {
+        Res t = res_init();
+        const Metrics mnb = get_metrics(C, true);
+        find_endpoints<IT>(C, t, mnb, EP_PCA, true, (int)p.power_iterations);
+        find_selectors_tp<IT>(C, CM_TB, EM_FULL, t);
+        refine_block_ls<IT>(C, CM_TB, t, mnb, EM_FULL, ls_passes);
+        if (t.err < res.err) res = t;
+    }
+
+    if (res.err > 0 && p.search_rounds > 0) endpoint_search<IT>(C, res, p.error_mode, p.search_rounds);
+    return write_block(res);
+}
+
+// BC4Encoder::EncodeBlock (BC4Encoder.cpp:30-71) for one group; returns the 8 bytes
+__device__ __forceinline__ uint2 encode_bc4_group(const Ctx &C, int ch) {
+    const int v = ch == 0 ? C.pr : (ch == 1 ? C.pg : (ch == 2 ? C.pb : C.pa));
+    const int mn = (int)gmin(C.gm, (unsigned)v), mx = (int)gmax(C.gm, (unsigned)v);
+    if (mn == mx) return make_uint2((uint32_t)mn | ((uint32_t)mn << 8), 0u);
+    const int bias = 4 - mn * 14, delta = mx - mn, x = v * 14;
+    int lvl = 0;
+#pragma unroll
+    for (int c = 0; c < 7; c++) lvl += x >= delta * (1 + 2 * c) - bias;
+    const uint32_t s = (kBC4Levels >> (3 * lvl)) & 7u;
+    const int bit = 3 * C.lane;
+    const uint32_t lo = gor(C.gm, bit < 32 ? s << bit : 0u);
+    const uint32_t hi = gor(C.gm, bit >= 32 ? s << (bit - 32) : (bit + 3 > 32 ? s >> (32 - bit) : 0u));
+    // bytes: a0=max, a1=min, then 48 selector bits little endian
+    return make_uint2((uint32_t)mx | ((uint32_t)mn << 8) | (lo << 16), (lo >> 16) | (hi << 16));
+}
+
+// ---------------------------------------------------------------------------
+// BC1 / BC3 encode kernel: one block per 16-lane group, grid-stride
+// ---------------------------------------------------------------------------
+template <int IT>
+__global__ void __launch_bounds__(128) k_bc1_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long nblocks,
+                                                    qt_bc1_params p, uint8_t *__restrict__ out, int bc3) {
+    __shared__ float s_mid5[32], s_mid6[64];
+    __shared__ uint16_t s_vox[16];
+    __shared__ uint32_t s_px[kGroupsPerCta][16];
+    __shared__ int s_sum[kGroupsPerCta][51];
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+        if (i < 32) s_mid5[i] = c_mid5[i];
+        s_mid6[i] = c_mid6[i];
+        if (i < 16) s_vox[i] = c_voxels[i];
+    }
+    __syncthreads();
+
+    const int grp = threadIdx.x >> 4;
+    Ctx C;
+    C.lane = threadIdx.x & 15;
+    C.gm = 0xFFFFu << (threadIdx.x & 16);
+    C.spx = s_px[grp];
+    C.ssum = s_sum[grp];
+    C.mid5 = s_mid5;
+    C.mid6 = s_mid6;
+    C.vox = s_vox;
+    if (bc3) p.color_mode = CM_FOUR;  // BC3Encoder.h:39-40
+
+    for (long b = (long)blockIdx.x * kGroupsPerCta + grp; b < nblocks; b += (long)gridDim.x * kGroupsPerCta) {
+        const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+        int sx = bx * 4 + (C.lane & 3), sy = by * 4 + (C.lane >> 2);
+        if (sx >= w) sx %= w;  // RawTexture::GetBlock wraps at the edges (Texture.h:105-108)
+        if (sy >= h) sy %= h;
+        const uint32_t v = *reinterpret_cast<const uint32_t *>(rgba + ((size_t)sy * w + sx) * 4);
+        C.spx[C.lane] = v;
+        C.pr = v & 0xFF;
+        C.pg = (v >> 8) & 0xFF;
+        C.pb = (v >> 16) & 0xFF;
+        C.pa = v >> 24;
+        __syncwarp(C.gm);
+        const uint2 blk = encode_bc1_group<IT>(C, p);
+        if (bc3) {
+            const uint2 a = encode_bc4_group(C, 3);
+            if (C.lane == 0) reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
+        } else if (C.lane == 0) {
+            reinterpret_cast<uint2 *>(out)[b] = blk;
+        }
+        __syncwarp(C.gm);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// thread-per-block kernels: BC4/BC5 encode, all decoders
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void load_block_thread(const uint8_t *__restrict__ rgba, int w, int h, int bx, int by,
+                                                  bool fast, uint32_t px[16]) {
+    if (fast) {
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(rgba + ((size_t)(by * 4 + y) * w + bx * 4) * 4));
+            px[4 * y] = q.x; px[4 * y + 1] = q.y; px[4 * y + 2] = q.z; px[4 * y + 3] = q.w;
+        }
+    } else {
+#pragma unroll
+        for (int y = 0; y < 4; y++)
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+                const int sx = (bx * 4 + x) % w, sy = (by * 4 + y) % h;
+                px[4 * y + x] = __ldg(reinterpret_cast<const uint32_t *>(rgba + ((size_t)sy * w + sx) * 4));
+            }
+    }
+}
+
+__device__ __forceinline__ uint2 bc4_block_thread(const uint32_t px[16], int ch) {
+    int mn = 255, mx = 0;
+    int v[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        v[i] = (px[i] >> (8 * ch)) & 0xFF;
+        mn = min(mn, v[i]);
+        mx = max(mx, v[i]);
+    }
+    if (mn == mx) return make_uint2((uint32_t)mn | ((uint32_t)mn << 8), 0u);
+    const int bias = 4 - mn * 14, delta = mx - mn;
+    int th[7];
+#pragma unroll
+    for (int c = 0; c < 7; c++) th[c] = delta * (1 + 2 * c) - bias;
+    uint64_t bits = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const int x = v[i] * 14;
+        int lvl = 0;
+#pragma unroll
+        for (int c = 0; c < 7; c++) lvl += x >= th[c];
+        bits |= (uint64_t)((kBC4Levels >> (3 * lvl)) & 7u) << (3 * i);
+    }
+    return make_uint2((uint32_t)mx | ((uint32_t)mn << 8) | ((uint32_t)bits << 16), (uint32_t)(bits >> 16));
+}
+
+__global__ void __launch_bounds__(256) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long nblocks,
+                                                    int c0, int c1, int bc5, int aligned, uint8_t *__restrict__ out) {
+    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x) {
+        const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+        const bool fast = aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h);
+        uint32_t px[16];
+        load_block_thread(rgba, w, h, bx, by, fast, px);
+        const uint2 a = bc4_block_thread(px, c0);
+        if (bc5) {
+            const uint2 c = bc4_block_thread(px, c1);
+            reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, c.x, c.y);
+        } else {
+            reinterpret_cast<uint2 *>(out)[b] = a;
+        }
+    }
+}
+
+// BC1 palette for decoding: Interpolator::Interpolate565BC1 (Interpolator.cpp:52-55)
+template <int IT>
+__device__ __forceinline__ void bc1_palette(uint32_t c0, uint32_t c1, bool allow3, bool write_alpha, uint32_t col[4]) {
+    const int lo = (int)c0, hi = (int)c1;  // packed 5:6:5 == eppack layout
+    const bool three = allow3 && (c1 >= c0);
+    const Pal P = make_pal<IT>(lo, hi, three);
+    // back to BC1 index order: colors[0]=c0, [1]=c1, [2], [3]
+    uint32_t a3 = three ? 0u : 255u;
+    if (!write_alpha) a3 = 255u;
+    col[0] = (uint32_t)P.r0 | ((uint32_t)P.g0 << 8) | ((uint32_t)P.b0 << 16) | 0xFF000000u;
+    col[2] = (uint32_t)P.r1 | ((uint32_t)P.g1 << 8) | ((uint32_t)P.b1 << 16) | 0xFF000000u;
+    if (!three) {
+        col[3] = (uint32_t)P.r2 | ((uint32_t)P.g2 << 8) | ((uint32_t)P.b2 << 16) | 0xFF000000u;
+        col[1] = (uint32_t)P.r3 | ((uint32_t)P.g3 << 8) | ((uint32_t)P.b3 << 16) | 0xFF000000u;
+    } else {
+        col[1] = (uint32_t)P.r2 | ((uint32_t)P.g2 << 8) | ((uint32_t)P.b2 << 16) | 0xFF000000u;
+        col[3] = (uint32_t)P.r3 | ((uint32_t)P.g3 << 8) | ((uint32_t)P.b3 << 16) | (a3 << 24);
+    }
+}
+
+__device__ __forceinline__ void bc4_values(uint32_t a0, uint32_t a1, uint32_t v[8]) {
+    v[0] = a0;
+    v[1] = a1;
+    if (a0 <= a1) {  // BC4Block::GetValues6 (BC4Block.cpp:44-53)
+        v[2] = (a0 * 4 + a1) / 5; v[3] = (a0 * 3 + a1 * 2) / 5; v[4] = (a0 * 2 + a1 * 3) / 5; v[5] = (a0 + a1 * 4) / 5;
+        v[6] = 0; v[7] = 255;
+    } else {  // GetValues8 (:55-64)
+        v[2] = (a0 * 6 + a1) / 7; v[3] = (a0 * 5 + a1 * 2) / 7; v[4] = (a0 * 4 + a1 * 3) / 7;
+        v[5] = (a0 * 3 + a1 * 4) / 7; v[6] = (a0 * 2 + a1 * 5) / 7; v[7] = (a0 + a1 * 6) / 7;
+    }
+}
+
+__device__ __forceinline__ void bc4_decode_into(uint2 blk, int ch, uint32_t px[16]) {
+    uint32_t v[8];
+    bc4_values(blk.x & 0xFF, (blk.x >> 8) & 0xFF, v);
+    const uint64_t bits = ((uint64_t)blk.y << 16) | (blk.x >> 16);
+    const int sh = 8 * ch;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const uint32_t s = (uint32_t)(bits >> (3 * i)) & 7u;
+        uint32_t val = v[0];
+#pragma unroll
+        for (int k = 1; k < 8; k++) val = s == (uint32_t)k ? v[k] : val;
+        px[i] = (px[i] & ~(0xFFu << sh)) | (val << sh);
+    }
+}
+
+// Decode: every texel of every block is decoded, and a texel is stored only
+// if no later block (in the reference's by, bx, x, y write order) writes the
+// same wrapped position: source (px, py) is final iff px + w >= 4*bw and
+// py + h >= 4*bh (RawTexture::SetBlock, Texture.h:114-134).
+template <int IT>
+__global__ void __launch_bounds__(256) k_decode(const uint8_t *__restrict__ blocks, int w, int h, int bw, int bh,
+                                                long nblocks, int fmt, int write_alpha, int c0, int c1, int aligned,
+                                                uint8_t *__restrict__ rgba) {
+    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x) {
+        const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+        uint32_t px[16];
+        if (fmt == 1 || fmt == 3) {
+            const uint2 cb = fmt == 1 ? __ldg(reinterpret_cast<const uint2 *>(blocks) + b)
+                                      : make_uint2(__ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 2),
+                                                   __ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 3));
+            uint32_t col[4];
+            bc1_palette<IT>(cb.x & 0xFFFF, cb.x >> 16, fmt == 1, fmt == 1 && write_alpha, col);
+#pragma unroll
+            for (int i = 0; i < 16; i++) {
+                const uint32_t s = (cb.y >> (2 * i)) & 3;
+                px[i] = s == 0 ? col[0] : (s == 1 ? col[1] : (s == 2 ? col[2] : col[3]));
+            }
+            if (fmt == 3) bc4_decode_into(make_uint2(__ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b),
+                                                     __ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 1)), 3, px);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; i++) px[i] = 0xFF000000u;  // ColorBlock default texel (0,0,0,255)
+            if (fmt == 4) {
+                bc4_decode_into(__ldg(reinterpret_cast<const uint2 *>(blocks) + b), c0, px);
+            } else {
+                const uint4 q = __ldg(reinterpret_cast<const uint4 *>(blocks) + b);
+                bc4_decode_into(make_uint2(q.x, q.y), c0, px);
+                bc4_decode_into(make_uint2(q.z, q.w), c1, px);
+            }
+        }
+        const bool interior = aligned && bx > 0 && by > 0 && bx * 4 + 4 <= w && by * 4 + 4 <= h;
+        if (interior) {
+#pragma unroll
+            for (int y = 0; y < 4; y++)
+                *reinterpret_cast<uint4 *>(rgba + ((size_t)(by * 4 + y) * w + bx * 4) * 4) =
+                    make_uint4(px[4 * y], px[4 * y + 1], px[4 * y + 2], px[4 * y + 3]);
+        } else {
+#pragma unroll
+            for (int y = 0; y < 4; y++)
+#pragma unroll
+                for (int x = 0; x < 4; x++) {
+                    const int sx = bx * 4 + x, sy = by * 4 + y;
+                    if (sx + w >= 4 * bw && sy + h >= 4 * bh)
+                        *reinterpret_cast<uint32_t *>(rgba + ((size_t)(sy % h) * w + (sx % w)) * 4) = px[4 * y + x];
+                }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// host-side launchers
+// ---------------------------------------------------------------------------
+static int grid_for(long work, int per_cta) {
+    static int sms = 0;
+    if (sms == 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (sms <= 0) sms = 148;
+    }
+    long need = (work + per_cta - 1) / per_cta;
+    long cap = (long)sms * 64;
+    return (int)(need < cap ? (need > 0 ? need : 1) : cap);
+}
+
+int upload_tables(int device) {
+    int prev = 0;
+    cudaGetDevice(&prev);
+    cudaError_t e = cudaSetDevice(device);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_tab, &host_tables(), sizeof(DevTables));
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    cudaSetDevice(prev);
+    return (int)e;
+}
+
+int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3, void *stream) {
+    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    const long n = (long)bw * bh;
+    const int grid = grid_for(n, kGroupsPerCta);
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (p.interpolator) {
+        case IT_IDEAL: k_bc1_encode<IT_IDEAL><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
+        case IT_ROUND: k_bc1_encode<IT_ROUND><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
+        case IT_NVIDIA: k_bc1_encode<IT_NVIDIA><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
+        default: k_bc1_encode<IT_AMD><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
+    }
+    return (int)cudaGetLastError();
+}
+
+int launch_bc4_encode(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc5, uint8_t *out, void *stream) {
+    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    const long n = (long)bw * bh;
+    const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
+    k_bc4_encode<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(rgba, w, h, bw, n, c0, c1, bc5, aligned, out);
+    return (int)cudaGetLastError();
+}
+
+int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
+                  uint8_t *rgba, void *stream) {
+    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    const long n = (long)bw * bh;
+    const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
+    const int grid = grid_for(n, 256);
+    cudaStream_t s = (cudaStream_t)stream;
+    switch (interp) {
+        case IT_IDEAL: k_decode<IT_IDEAL><<<grid, 256, 0, s>>>(blocks, w, h, bw, bh, n, fmt, write_alpha, c0, c1, aligned, rgba); break;
+        case IT_ROUND: k_decode<IT_ROUND><<<grid, 256, 0, s>>>(blocks, w, h, bw, bh, n, fmt, write_alpha, c0, c1, aligned, rgba); break;
+        case IT_NVIDIA: k_decode<IT_NVIDIA><<<grid, 256, 0, s>>>(blocks, w, h, bw, bh, n, fmt, write_alpha, c0, c1, aligned, rgba); break;
+        default: k_decode<IT_AMD><<<grid, 256, 0, s>>>(blocks, w, h, bw, bh, n, fmt, write_alpha, c0, c1, aligned, rgba); break;
+    }
+    return (int)cudaGetLastError();
+}
+
+}  // namespace qtk

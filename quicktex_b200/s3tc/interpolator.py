@@ -1,0 +1,7 @@
+"""Reference counterpart: ``quicktex.s3tc.interpolator``."""
+
+from .._quicktex import _s3tc as _s
+
+_m = _s._interpolator
+__all__ = [n for n in dir(_m) if not n.startswith("_")]
+globals().update({n: getattr(_m, n) for n in __all__})
