@@ -1,0 +1,352 @@
+#!/usr/bin/env python3
+"""Benchmark of the S3TC encode path on B200.
+
+Workload (one "step"): BC1-encode one seeded 4096x4096 RGBA8 texture
+(1,048,576 blocks; 40% gradient / 30% random / 20% two-colour edge / 10% solid
+blocks) once for each of the 36 settings {level 0, 10, 18} x {four-colour,
+three-colour, three-colour+black} x {Ideal, IdealRound, Nvidia, AMD}:
+37.7 M blocks per step, every output bit-exact with the reference encoder
+(checked by the parity tests against the committed reference hashes).
+
+  value   Mblocks/s with the texture resident in HBM (device entry point
+          qt_bc1_encode_device), L2 flushed between steps, CUDA-event timed.
+  e2e     the same metric through the host-buffer entry point
+          qt_bc1_encode_host from pinned host memory: every call copies the
+          texture in and the blocks out.
+  roofline  the BC1 kernel against the CUDA-core issue rate (it is an FP32/INT32
+          issue-bound kernel, not HBM- or tensor-bound): algorithmic work =
+          10 lane-ops per candidate evaluation x the oracle-counted candidate
+          evaluations per block of each setting (tests/golden/ce_counts.json).
+  cpu_baseline  the unmodified reference encoder (oracle/_ref) on this host's
+          cores, OpenMP as shipped, on a 512x512 crop of the same texture for
+          each of the 36 settings.
+
+Multi-GPU (torchrun, one process per GPU): every rank encodes its own replica
+of the workload (the path shards by texture; no collective on the data path),
+value = all ranks' blocks / max-over-ranks time.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "BC1/BC3 encode Mblocks/s bit-exact, batched vs plain on 1 B200; serve p50/p99 ms"
+LEVELS = (0, 10, 18)
+MODES = (("four", 0x04), ("three", 0x03), ("three_black", 0x13))
+INTERPS = (("ideal", 0), ("round", 1), ("nvidia", 2), ("amd", 3))
+W = H = 4096
+NB = (W // 4) * (H // 4)
+SETTINGS = [(L, mn, m, iname, it) for L in LEVELS for mn, m in MODES for iname, it in INTERPS]
+
+
+def configure(size: int, levels) -> None:
+    """Profiling variants (--size / --levels); the default is the benchmark workload."""
+    global W, H, NB, SETTINGS
+    W = H = size
+    NB = (W // 4) * (H // 4)
+    SETTINGS = [(L, mn, m, iname, it) for L in levels for mn, m in MODES for iname, it in INTERPS]
+    CONFIG["levels"] = list(levels)
+    CONFIG["blocks_per_step"] = NB * len(SETTINGS)
+    if size != 4096 or tuple(levels) != LEVELS:
+        CONFIG["workload"] = f"bc1_encode_{size}x{size}_mix_{len(SETTINGS)}settings (profiling variant)"
+CONFIG = {
+    "workload": "bc1_encode_4096x4096_mix_36settings",
+    "texture": "4096x4096 RGBA8, seeded block mix (40% gradient, 30% random, 20% edge, 10% solid)",
+    "levels": list(LEVELS),
+    "color_modes": [m for m, _ in MODES],
+    "interpolators": [i for i, _ in INTERPS],
+    "blocks_per_step": NB * len(SETTINGS),
+    "l2": "flushed between steps (256 MiB write)",
+}
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return {"hbm_gbs": 6650.0, "sm_max_mhz": 1965.0}, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.lines = []
+        if self.proc:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_init(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", local))
+    return world, rank, local
+
+
+def reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def cpu_reference_sample(img: np.ndarray, repeats: int = 1):
+    """The reference encoder (as shipped: BlockEncoder::Encode with OpenMP) on a
+    512x512 crop for each of the 36 settings. Returns (Mblocks/s, seconds, cores, kind)."""
+    import oracle
+
+    crop = np.ascontiguousarray(img[:512, :512])
+    if oracle.reference_available():
+        lib, kind = oracle.Reference(), "reference"
+    else:
+        lib, kind = oracle.Oracle(), "port"
+    cores = os.cpu_count() or 1
+    lib.set_threads(cores)
+    blocks = 0
+    t0 = time.perf_counter()
+    for _ in range(repeats):
+        for L, _mn, m, _in, it in SETTINGS:
+            lib.bc1_encode(crop, 512, 512, oracle.BC1Params(level=L, color_mode=m, interpolator=it), mode=0)
+            blocks += 128 * 128
+    dt = time.perf_counter() - t0
+    return blocks / dt / 1e6, dt, cores, kind
+
+
+def run_reference_arm(args, world, rank):
+    if rank != 0:
+        return
+    import quicktex_b200.synth as syn
+
+    img = syn.block_mix(W, H)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        v, dt, cores, kind = cpu_reference_sample(img)
+        if i >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    sample = "512x512 crop (16,384 blocks) of the workload texture for each of the 36 settings per step"
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "Mblocks/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 36 * 16384 / value / 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8",
+        "data": "synthetic (seeded PCG64 block mix)", "config": CONFIG,
+        "cpu_baseline": {"value": value, "unit": "Mblocks/s", "cores": cores, "kind": kind, "sample": sample},
+        "e2e": {"value": value, "unit": "Mblocks/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, world, rank, local):
+    import torch
+
+    import quicktex_b200.synth as syn
+    from quicktex_b200 import capi
+
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    img = syn.block_mix(4096, 4096)[:H, :W] if W <= 4096 else syn.block_mix(W, H)
+    img = np.ascontiguousarray(img)
+    host_in = torch.from_numpy(img.reshape(-1)).pin_memory()
+    d_in = host_in.to(dev)
+    d_out = torch.empty(NB * 8, dtype=torch.uint8, device=dev)
+    host_out = torch.empty(NB * 8, dtype=torch.uint8).pin_memory()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    params = [capi.params_for_level(L, m, it) for L, _mn, m, _in, it in SETTINGS]
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+
+    def step():
+        for p in params:
+            capi.bc1_encode_device(d_in.data_ptr(), W, H, p, d_out.data_ptr(), sptr)
+
+    # per-setting kernel times (one pass, for the roofline and the level breakdown)
+    per = []
+    for p in params:
+        capi.bc1_encode_device(d_in.data_ptr(), W, H, p, d_out.data_ptr(), sptr)
+    torch.cuda.synchronize()
+    for p in params:
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        flush.zero_()
+        a.record(stream)
+        capi.bc1_encode_device(d_in.data_ptr(), W, H, p, d_out.data_ptr(), sptr)
+        b.record(stream)
+        b.synchronize()
+        per.append(a.elapsed_time(b))
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    times = []
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            step()
+            b.record(stream)
+            times.append((a, b))
+        torch.cuda.synchronize()
+    barrier(world)
+    ms = sum(a.elapsed_time(b) for a, b in times) / args.steps
+    ms = reduce_max(ms, world)
+    blocks_step = NB * len(SETTINGS)
+    value = world * blocks_step / (ms / 1e3) / 1e6
+
+    # end to end through the host-buffer C-ABI call (pinned host memory in and out)
+    hin, hout = host_in.numpy(), host_out.numpy()
+
+    def e2e_step():
+        for p in params:
+            capi.check(capi.lib().qt_bc1_encode_host(capi._p(hin), W, H, capi.ctypes.byref(p), capi._p(hout)))
+
+    e2e_value = None
+    if not args.no_e2e:
+        for _ in range(max(1, args.warmup)):
+            e2e_step()
+        barrier(world)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            e2e_step()
+        e2e_s = reduce_max((time.perf_counter() - t0) / args.steps, world)
+        e2e_value = world * blocks_step / e2e_s / 1e6
+
+    # roofline: algorithmic lane-ops (10 per candidate evaluation) / kernel time
+    peaks, peaks_kind = load_peaks()
+    with open(os.path.join(ROOT, "tests", "golden", "ce_counts.json")) as f:
+        ce = json.load(f)["per_block"]
+    ops = sum(10.0 * ce[f"L{L}_{mn}_{iname}"] * NB for L, mn, _m, iname, _it in SETTINGS)
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    peak_tops = sms * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
+    achieved = ops / (sum(per) / 1e3) / 1e12
+    by_level = {}
+    for (L, _mn, _m, _in, _it), t in zip(SETTINGS, per):
+        by_level.setdefault(f"L{L}", [0.0, 0])
+        by_level[f"L{L}"][0] += t
+        by_level[f"L{L}"][1] += NB
+    line = {
+        "metric": METRIC, "value": value, "unit": "Mblocks/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "u8", "data": "synthetic (seeded PCG64 block mix; no public corpus exists)", "config": CONFIG,
+        "roofline": {
+            "bound": "fp32_issue", "achieved": achieved, "peak": peak_tops, "unit": "Tlane-op/s",
+            "frac": achieved / peak_tops, "traffic": None,
+            "kernel": "qtk::k_bc1_encode (all 36 settings)",
+            "work": "10 lane-ops x oracle-counted candidate evaluations per block",
+            "peak_source": f"{sms} SMs x 128 lanes x sm_max_mhz ({peaks_kind})",
+        },
+        "by_level_mblocks_s": {k: v[1] / (v[0] / 1e3) / 1e6 for k, v in by_level.items()},
+        "e2e": {"value": e2e_value, "unit": "Mblocks/s", "h2d_bytes_per_step": W * H * 4 * len(SETTINGS),
+                "d2h_bytes_per_step": NB * 8 * len(SETTINGS)},
+        "gpu_launches": len(SETTINGS) * args.steps,
+        "clocks": clk.summary(),
+    }
+    if world == 1 and rank == 0 and not args.no_cpu:
+        v, dt, cores, kind = cpu_reference_sample(img)
+        line["cpu_baseline"] = {"value": v, "unit": "Mblocks/s", "cores": cores, "kind": kind,
+                                "sample": f"512x512 crop x 36 settings, as-shipped OpenMP encode, {dt:.1f} s"}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--size", type=int, default=4096, help="texture side (profiling variants only)")
+    ap.add_argument("--levels", type=str, default="0,10,18", help="levels (profiling variants only)")
+    args = ap.parse_args()
+    configure(args.size, tuple(int(x) for x in args.levels.split(",")))
+    if args.impl == "reference":  # CPU only: rank 0 runs it, the other ranks exit without work
+        run_reference_arm(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))
+        return
+    world, rank, local = dist_init(args)
+    try:
+        run_ours(args, world, rank, local)
+    finally:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

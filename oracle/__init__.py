@@ -127,19 +127,20 @@ class _Lib:
             f = getattr(self.lib, p + name)
             f.argtypes = args
             f.restype = None if name == "set_threads" else _i
-        self.lib[p + "last_error"].restype = ctypes.c_char_p
-        self.lib[p + "num_threads"].restype = _i
+        # getattr (not lib[...]) so the restype sticks to the cached function object
+        getattr(self.lib, p + "last_error").restype = ctypes.c_char_p
+        getattr(self.lib, p + "num_threads").restype = _i
 
     def _call(self, name, *args):
         rc = getattr(self.lib, self.prefix + name)(*args)
         if rc != 0:
-            raise RuntimeError(self.lib[self.prefix + "last_error"]().decode())
+            raise RuntimeError(getattr(self.lib, self.prefix + "last_error")().decode())
 
     def set_threads(self, n: int) -> None:
         getattr(self.lib, self.prefix + "set_threads")(int(n))
 
     def num_threads(self) -> int:
-        return self.lib[self.prefix + "num_threads"]()
+        return getattr(self.lib, self.prefix + "num_threads")()
 
     def level_params(self, level: int, color_mode: int = FOUR_COLOR):
         out = (ctypes.c_int * 10)()
@@ -213,10 +214,20 @@ class Oracle(_Lib):
 
     def __init__(self, path: str = ORACLE_SO, tables: str = ORDER_TABLES):
         super().__init__(path)
+        self.lib.qo_ce_count.restype = ctypes.c_ulonglong
         self.lib.qo_init.argtypes = [ctypes.c_char_p]
         self.lib.qo_init.restype = _i
         if self.lib.qo_init(tables.encode()) != 0:
             raise RuntimeError(self.lib.qo_last_error().decode())
+
+
+    def ce_count(self) -> int:
+        """Candidate evaluations (SSD + select of one texel vs one palette colour)
+        performed by the encodes since the last ``ce_reset``."""
+        return int(self.lib.qo_ce_count())
+
+    def ce_reset(self) -> None:
+        self.lib.qo_ce_reset()
 
 
 def reference_available() -> bool:

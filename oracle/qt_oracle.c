@@ -31,6 +31,16 @@ enum { EP_LS = 0, EP_BB = 1, EP_BBINT = 2, EP_PCA = 3 };
 enum { IT_IDEAL = 0, IT_ROUND = 1, IT_NVIDIA = 2, IT_AMD = 3 };
 
 static __thread char g_err[256];
+
+/* Candidate-evaluation (CE) counter: one CE = the SSD of one texel against
+ * one palette colour plus its compare/select. Counted per FindSelectors call
+ * without the reference's early exits (a full call always costs its texels x
+ * candidates): Full 4-colour 64, Full 3-colour 48, Check2 32 + 16
+ * projections = 48, Faster/None 16 projections = 16, and the single-colour
+ * trial 16. Data-dependent stops (cluster fit at zero error, LS convergence,
+ * the endpoint search stop rule) are honoured because they stop the calls. */
+static __thread unsigned long long t_ce;
+static unsigned long long g_ce;
 static int fail(const char *m) { snprintf(g_err, sizeof g_err, "%s", m); return 1; }
 const char *qo_last_error(void) { return g_err; }
 
@@ -341,6 +351,7 @@ static void find_endpoints_single_color_px(const bc1p_t *p, result_t *r, const c
     color_t cols[4];
     interpolate_bc1(p->interp, r->low, r->high, is3, cols);
     color_t rv = cols[2];
+    t_ce += 16;
     find_endpoints_single_color(p, r, c, is3);
     r->error = 0;
     for (int i = 0; i < 16; i++) {
@@ -494,6 +505,7 @@ static void find_selectors(const bc1p_t *p, int M, result_t *r, const color_t px
     else { order[0] = 0; order[1] = 2; order[2] = 1; order[3] = 3; }
     for (int j = 0; j < 4; j++) { cv[j][0] = cols[order[j]].r; cv[j][1] = cols[order[j]].g; cv[j][2] = cols[order[j]].b; }
     unsigned total = 0;
+    t_ce += (em == EM_FULL) ? (M == CM_THREE ? 48u : 64u) : (em == EM_CHECK2 ? 48u : 16u);
     if (em == EM_NONE || em == EM_FASTER) {
         int ax[3] = {cv[3][0] - cv[0][0], cv[3][1] - cv[0][1], cv[3][2] - cv[0][2]};
         int dots[4];
@@ -906,13 +918,18 @@ static int encode_texture(const uint8_t *rgba, int w, int h, const void *ctx, bl
         for (long i = 0; i < n; i++) {
             color_t px[16];
             get_block(rgba, w, h, (int)(i % bw), (int)(i / bw), px);
+            t_ce = 0;
             fn(ctx, px, out + i * bsize);
+#pragma omp atomic
+            g_ce += t_ce;
         }
     } else {
         for (long i = 0; i < n; i++) {
             color_t px[16];
             get_block(rgba, w, h, (int)(i % bw), (int)(i / bw), px);
+            t_ce = 0;
             fn(ctx, px, out + i * bsize);
+            g_ce += t_ce;
         }
     }
     return 0;
@@ -955,6 +972,10 @@ static int make_params(bc1p_t *p, int level, int color_mode, int interp, const i
 /* ------------------------------------------------------------------------- */
 /* exported C-ABI (mirrors oracle/ref_harness.cpp)                           */
 /* ------------------------------------------------------------------------- */
+/* total candidate evaluations of the encodes since the last reset */
+unsigned long long qo_ce_count(void) { return g_ce; }
+void qo_ce_reset(void) { g_ce = 0; }
+
 int qo_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -1,0 +1,167 @@
+"""Generate the committed golden fixtures under tests/golden/.
+
+Run where the reference source tree exists (it builds and runs the unmodified
+reference, oracle/_ref/libqtref.so):
+
+    python tests/golden/make_golden.py [--skip-full]
+
+Writes
+  kat.json         the reference's own known-answer vectors: the 4x4 PNG
+                   fixtures of tests/images/{bc1,bc4} as raw RGBA8 bytes, with
+                   the expected blocks of tests/images/__init__.py:18-32.
+  ref_hashes.json  sha256 of the reference's output on the seeded workloads at
+                   full size (512^2 BC1 L5 encode+decode; 4096^2 BC1 at levels
+                   {0,10,18} x 3 colour modes x 4 interpolators; 8192^2 BC3 L5,
+                   BC5, BC4 channels {0,1,3} and their decodes), plus a 512^2
+                   sweep of every level 0-19. Each entry also records the
+                   sha256 of its input so a mismatch in the generator is caught
+                   before the codec is blamed. Every hash is cross-checked
+                   against the oracle restatement (qt_oracle.c) before writing.
+  ce_counts.json   candidate evaluations per block (the algorithmic work unit
+                   of the BC1 issue roofline) counted by the oracle on the
+                   4096^2 workload for each of its 36 settings.
+"""
+
+from __future__ import annotations
+
+import argparse
+import hashlib
+import json
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+import oracle  # noqa: E402
+import quicktex_b200.synth as syn  # noqa: E402
+from oracle import BC1Params  # noqa: E402
+
+REF_IMAGES = os.path.join(os.environ.get("QT_REFERENCE_ROOT", "/root/reference"), "tests", "images")
+MODES = {"four": 0x04, "three": 0x03, "three_black": 0x13}
+INTERPS = {"ideal": 0, "round": 1, "nvidia": 2, "amd": 3}
+
+
+def sha(b) -> str:
+    return hashlib.sha256(bytes(b)).hexdigest()
+
+
+def kat() -> dict:
+    from PIL import Image
+
+    def rgba(path):
+        im = Image.open(path).convert("RGBA")
+        return {"w": im.size[0], "h": im.size[1], "rgba": im.tobytes("raw", "RGBA").hex()}
+
+    out = {"bc1": {}, "bc4": {}}
+    # tests/images/__init__.py:18-20
+    for name, fname, block in [("greyscale", "greyscale_unpacked.png", "ffff494a78787878"),
+                               ("three_color", "3color_unpacked.png", "e00700f829292929"),
+                               ("three_color_black", "3color_black_unpacked.png", "e00700f827272727")]:
+        out["bc1"][name] = dict(rgba(os.path.join(REF_IMAGES, "bc1", fname)), block=block)
+    # tests/images/__init__.py:31-32: BC4Block(8, 248, ...) and BC4Block(240, 16, ...), selectors [[0,1,2,3]]*2+[[4,5,6,7]]*2
+    sel = 0
+    for i, s in enumerate([0, 1, 2, 3] * 2 + [4, 5, 6, 7] * 2):
+        sel |= s << (3 * i)
+    selhex = sel.to_bytes(6, "little").hex()
+    out["bc4"]["six_value"] = dict(rgba(os.path.join(REF_IMAGES, "bc4", "6value.png")), block="08f8" + selhex)
+    out["bc4"]["eight_value"] = dict(rgba(os.path.join(REF_IMAGES, "bc4", "8value.png")), block="f010" + selhex)
+    # block byte strings of tests/test_bc1.py:9-12 and tests/test_bc4.py:9-11
+    out["bc1_block_bytes"] = "ffff284278787878"
+    out["bc4_block_bytes"] = "f010888668accffa"
+    return out
+
+
+def checked(name, ref_out, orc_out):
+    if ref_out != orc_out:
+        raise SystemExit(f"oracle disagrees with the reference on {name}")
+    return sha(ref_out)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--skip-full", action="store_true", help="only the 512^2 cases")
+    args = ap.parse_args()
+
+    oracle.build(with_ref=True)
+    ref, orc = oracle.Reference(), oracle.Oracle()
+    ref.set_threads(os.cpu_count())
+    orc.set_threads(os.cpu_count())
+
+    with open(os.path.join(HERE, "kat.json"), "w") as f:
+        json.dump(kat(), f, indent=1)
+
+    hashes: dict = {}
+    t0 = time.time()
+
+    # workload 1: 512x512 gradient + noise, BC1 L5 four-colour Ideal, encode + decode
+    img = syn.gradient_noise(512, 512)
+    enc = ref.bc1_encode(img, 512, 512, BC1Params(level=5))
+    hashes["gradient_512"] = {
+        "input": {"gen": "gradient_noise", "w": 512, "h": 512, "sha256": sha(img)},
+        "bc1_L5_four_ideal": checked("g512 enc", enc, orc.bc1_encode(img, 512, 512, BC1Params(level=5))),
+        "bc1_decode_ideal": checked("g512 dec", ref.bc1_decode(enc, 512, 512), orc.bc1_decode(enc, 512, 512)),
+    }
+
+    # 512^2 sweep of every level, mode and interpolator (LeastSquares x Nvidia excluded: reference UB)
+    img = syn.block_mix(512, 512, workload=2, stream=1)
+    sweep = {}
+    for L in range(20):
+        for mn, m in MODES.items():
+            for iname, it in INTERPS.items():
+                if it == 2 and oracle.Reference().level_params(L, m)[1] == 0:
+                    continue
+                p = BC1Params(level=L, color_mode=m, interpolator=it)
+                sweep[f"L{L}_{mn}_{iname}"] = checked(f"sweep L{L}", ref.bc1_encode(img, 512, 512, p), orc.bc1_encode(img, 512, 512, p))
+    hashes["mix_512_sweep"] = {"input": {"gen": "block_mix", "w": 512, "h": 512, "workload": 2, "stream": 1,
+                                         "sha256": sha(img)}, "bc1": sweep}
+    print(f"512 cases done in {time.time() - t0:.0f}s", flush=True)
+
+    ce = {}
+    if not args.skip_full:
+        img = syn.block_mix(4096, 4096)
+        runs = {}
+        for L in (0, 10, 18):
+            for mn, m in MODES.items():
+                for iname, it in INTERPS.items():
+                    p = BC1Params(level=L, color_mode=m, interpolator=it)
+                    r = ref.bc1_encode(img, 4096, 4096, p)
+                    orc.ce_reset()
+                    o = orc.bc1_encode(img, 4096, 4096, p)
+                    ce[f"L{L}_{mn}_{iname}"] = orc.ce_count() / (1024 * 1024)
+                    runs[f"L{L}_{mn}_{iname}"] = checked(f"4096 L{L} {mn} {iname}", r, o)
+                    print(f"  4096 L{L} {mn} {iname} ({time.time() - t0:.0f}s)", flush=True)
+        hashes["mix_4096"] = {"input": {"gen": "block_mix", "w": 4096, "h": 4096, "sha256": sha(img)}, "bc1": runs}
+
+        img = syn.alpha_mix(8192, 8192)
+        e3 = ref.bc3_encode(img, 8192, 8192, BC1Params(level=5))
+        entry = {"input": {"gen": "alpha_mix", "w": 8192, "h": 8192, "sha256": sha(img)},
+                 "bc3_L5_ideal": checked("bc3", e3, orc.bc3_encode(img, 8192, 8192, BC1Params(level=5))),
+                 "bc3_decode_ideal": checked("bc3 dec", ref.bc3_decode(e3, 8192, 8192), orc.bc3_decode(e3, 8192, 8192))}
+        for c in (0, 1, 3):
+            e4 = ref.bc4_encode(img, 8192, 8192, c)
+            entry[f"bc4_ch{c}"] = checked(f"bc4 {c}", e4, orc.bc4_encode(img, 8192, 8192, c))
+            entry[f"bc4_decode_ch{c}"] = checked(f"bc4 dec {c}", ref.bc4_decode(e4, 8192, 8192, c), orc.bc4_decode(e4, 8192, 8192, c))
+        hashes["alpha_8192"] = entry
+        print(f"  8192 bc3/bc4 ({time.time() - t0:.0f}s)", flush=True)
+
+        img = syn.normal_map(8192, 8192)
+        e5 = ref.bc5_encode(img, 8192, 8192, 0, 1)
+        hashes["normal_8192"] = {"input": {"gen": "normal_map", "w": 8192, "h": 8192, "sha256": sha(img)},
+                                 "bc5_01": checked("bc5", e5, orc.bc5_encode(img, 8192, 8192, 0, 1)),
+                                 "bc5_decode_01": checked("bc5 dec", ref.bc5_decode(e5, 8192, 8192, 0, 1),
+                                                          orc.bc5_decode(e5, 8192, 8192, 0, 1))}
+        with open(os.path.join(HERE, "ce_counts.json"), "w") as f:
+            json.dump({"unit": "candidate evaluations per 4x4 block, 4096^2 block_mix workload", "per_block": ce}, f, indent=1)
+
+    with open(os.path.join(HERE, "ref_hashes.json"), "w") as f:
+        json.dump(hashes, f, indent=1)
+    print(f"done in {time.time() - t0:.0f}s")
+
+
+if __name__ == "__main__":
+    main()
