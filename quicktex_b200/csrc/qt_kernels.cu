@@ -179,17 +179,33 @@ template <int IT> __device__ __forceinline__ Pal make_pal(int lo, int hi, bool t
 }
 
 // ---------------------------------------------------------------------------
-// per-group context
+// per-CTA shared state of the BC1 kernel. File scope, so that the phase
+// functions below (kept __noinline__: one copy each, a small instruction
+// working set per launch) reach the block being encoded without passing it.
 // ---------------------------------------------------------------------------
-struct Ctx {
-    unsigned gm;     // this group's 16 lanes in the warp
-    int lane;        // 0..15 = texel index (x = lane & 3, y = lane >> 2)
-    int pr, pg, pb, pa;
-    uint32_t *spx;   // shared: the block's 16 texels (RGBA8 packed)
-    int *ssum;       // shared: cluster-fit prefix sums [17][3]
-    const float *mid5, *mid6;
-    const uint16_t *vox;
+__shared__ float s_mid5[32], s_mid6[64];
+__shared__ uint16_t s_vox[16];
+__shared__ uint32_t s_px[kGroupsPerCta][16];      // the block's texels, RGBA8
+__shared__ float4 s_pf[kGroupsPerCta][16];        // (r, g, b, r^2+g^2+b^2) as exact floats
+__shared__ int s_sum[kGroupsPerCta][17 * 3];       // cluster-fit prefix sums
+__shared__ uint16_t s_row[kGroupsPerCta][128];     // BestOrders row of the current cluster fit
+__shared__ int s_met[kGroupsPerCta][2][16];        // metrics: [0] all texels, [1] ignoring black
+
+// metric slots
+constexpr int MT_MN = 0, MT_MX = 3, MT_AV = 6, MT_SUM = 9, MT_GREY = 12, MT_BLACK = 13;
+
+struct Grp {
+    unsigned gm;  // the group's 16 lanes within the warp
+    int lane;     // texel index in phases that map lanes to texels
+    int g;        // group index within the CTA
 };
+__device__ __forceinline__ Grp grp() {
+    Grp G;
+    G.lane = threadIdx.x & 15;
+    G.g = threadIdx.x >> 4;
+    G.gm = 0xFFFFu << (threadIdx.x & 16);
+    return G;
+}
 
 struct Res {  // EncodeResults (BC1Encoder.h:147-153); endpoints packed 5:6:5
     int lo, hi;
@@ -207,9 +223,8 @@ __device__ __forceinline__ Res res_init() {
     return r;
 }
 
-struct Metrics {  // ColorBlock::Metrics (ColorBlock.h:30-37)
-    int mn[3], mx[3], av[3], sum[3];
-    bool grey, has_black;
+struct SelErr {
+    uint32_t sel, err;
 };
 
 __device__ __forceinline__ unsigned gsum(unsigned m, unsigned v) { return __reduce_add_sync(m, v); }
@@ -217,131 +232,138 @@ __device__ __forceinline__ unsigned gmin(unsigned m, unsigned v) { return __redu
 __device__ __forceinline__ unsigned gmax(unsigned m, unsigned v) { return __reduce_max_sync(m, v); }
 __device__ __forceinline__ unsigned gor(unsigned m, unsigned v) { return __reduce_or_sync(m, v); }
 
-// ColorBlock::GetMetrics (ColorBlock.h:88-117)
-__device__ Metrics get_metrics(const Ctx &C, bool ignore_black) {
-    Metrics m;
-    const bool blk = (C.pr | C.pg | C.pb) < 4;
-    m.has_black = __any_sync(C.gm, blk);
+// Selector-search kinds: the (colour mode, error mode) pairs FindSelectors is
+// ever called with. Three-colour searches are always ErrorMode::Full
+// (BC1Encoder.cpp:313-333, 978-984).
+constexpr int K_F4_NONE = 0, K_F4_FASTER = 1, K_F4_CHECK2 = 2, K_F4_FULL = 3, K_T3 = 4, K_TB = 5;
+__host__ __device__ constexpr bool kind_three(int k) { return k >= K_T3; }
+__host__ __device__ constexpr int kind_mode(int k) { return k == K_T3 ? CM_THREE : (k == K_TB ? CM_TB : CM_FOUR); }
+__device__ __forceinline__ int kind_for(int M, int em) { return M == CM_THREE ? K_T3 : (M == CM_TB ? K_TB : em); }
+
+// ColorBlock::GetMetrics (ColorBlock.h:88-117), into s_met[g][which]
+__device__ __noinline__ void get_metrics(int which, bool ignore_black) {
+    const Grp G = grp();
+    const uint32_t v = s_px[G.g][G.lane];
+    const int p[3] = {(int)(v & 0xFF), (int)((v >> 8) & 0xFF), (int)((v >> 16) & 0xFF)};
+    const bool blk = (p[0] | p[1] | p[2]) < 4;
+    const bool has_black = __any_sync(G.gm, blk);
     const bool inc = !(ignore_black && blk);
-    m.grey = __all_sync(C.gm, !inc || (C.pr == C.pg && C.pr == C.pb));
-    const int p[3] = {C.pr, C.pg, C.pb};
-    const int total = __popc(__ballot_sync(C.gm, inc) & C.gm);
+    const bool grey = __all_sync(G.gm, !inc || (p[0] == p[1] && p[0] == p[2]));
+    const int total = __popc(__ballot_sync(G.gm, inc) & G.gm);
+    int *M = s_met[G.g][which];
 #pragma unroll
     for (int c = 0; c < 3; c++) {
-        m.mn[c] = (int)gmin(C.gm, inc ? p[c] : 255);
-        m.mx[c] = (int)gmax(C.gm, inc ? p[c] : 0);
-        m.sum[c] = (int)gsum(C.gm, inc ? p[c] : 0);
-        m.av[c] = total > 0 ? (m.sum[c] + total / 2) / total : 0;
+        const int mn = (int)gmin(G.gm, inc ? p[c] : 255), mx = (int)gmax(G.gm, inc ? p[c] : 0);
+        const int sm = (int)gsum(G.gm, inc ? p[c] : 0);
+        if (G.lane == 0) {
+            M[MT_MN + c] = mn;
+            M[MT_MX + c] = mx;
+            M[MT_SUM + c] = sm;
+            M[MT_AV + c] = total > 0 ? (sm + total / 2) / total : 0;
+        }
     }
-    return m;
+    if (G.lane == 0) {
+        M[MT_GREY] = grey;
+        M[MT_BLACK] = has_black;
+    }
+    __syncwarp(G.gm);
 }
 
 // ---------------------------------------------------------------------------
-// FindSelectors<M>, texel-parallel (BC1Encoder.cpp:679-779)
+// FindSelectors<M>(error_mode), texel-parallel (BC1Encoder.cpp:679-779)
 // ---------------------------------------------------------------------------
-template <int IT>
-__device__ __forceinline__ void find_selectors_tp(const Ctx &C, int M, int em, Res &r) {
-    const bool three = (M & 0x0F) == 3;
-    const Pal P = make_pal<IT>(r.lo, r.hi, three);
+template <int IT, int K> __device__ __noinline__ SelErr fs_tp(int lo, int hi) {
+    const Grp G = grp();
+    const uint32_t v = s_px[G.g][G.lane];
+    const int pr = v & 0xFF, pg = (v >> 8) & 0xFF, pb = (v >> 16) & 0xFF;
+    const Pal P = make_pal<IT>(lo, hi, kind_three(K));
     int s;
     unsigned e;
-    if (em == EM_NONE || em == EM_FASTER) {
+    if (K == K_F4_NONE || K == K_F4_FASTER) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
         const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
         const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
         const int t0 = d0 + d1, t1 = d1 + d2, t2 = d2 + d3;
-        const int dot = 2 * ar * C.pr + 2 * ag * C.pg + 2 * ab * C.pb;
-        const int level = (dot <= t0) + (dot < t1) + (dot < t2);
-        s = 3 - level;
-        e = em == EM_FASTER ? sq3(C.pr - sel4(P.r0, P.r1, P.r2, P.r3, s), C.pg - sel4(P.g0, P.g1, P.g2, P.g3, s),
-                                  C.pb - sel4(P.b0, P.b1, P.b2, P.b3, s))
-                            : 0u;
-    } else if (em == EM_CHECK2) {
+        const int dot = 2 * ar * pr + 2 * ag * pg + 2 * ab * pb;
+        s = 3 - ((dot <= t0) + (dot < t1) + (dot < t2));
+        e = K == K_F4_FASTER ? sq3(pr - sel4(P.r0, P.r1, P.r2, P.r3, s), pg - sel4(P.g0, P.g1, P.g2, P.g3, s),
+                                   pb - sel4(P.b0, P.b1, P.b2, P.b3, s))
+                             : 0u;
+    } else if (K == K_F4_CHECK2) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
         const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
-        const int dd = (C.pr - P.r0) * ar + (C.pg - P.g0) * ag + (C.pb - P.b0) * ab;
+        const int dd = (pr - P.r0) * ar + (pg - P.g0) * ag + (pb - P.b0) * ab;
         const float sf = __fadd_rn(__fmul_rn(__int2float_rn(dd), f), 0.5f);
         const int sl = clampi(f2i_x86(sf), 1, 3);
-        const unsigned e0 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - C.pr, sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - C.pg,
-                                sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - C.pb);
-        const unsigned e1 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl) - C.pr, sel4(P.g0, P.g1, P.g2, P.g3, sl) - C.pg,
-                                sel4(P.b0, P.b1, P.b2, P.b3, sl) - C.pb);
+        const unsigned e0 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - pr, sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - pg,
+                                sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - pb);
+        const unsigned e1 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl) - pr, sel4(P.g0, P.g1, P.g2, P.g3, sl) - pg,
+                                sel4(P.b0, P.b1, P.b2, P.b3, sl) - pb);
         s = sl;
         e = e1;
         if (e0 == e1) {
-            if (s == 1) s = 0;
+            if (s == 1) s = 0;  // prefer the endpoint (:736-738)
         } else if (e0 < e) {
             s = sl - 1;
             e = e0;
         }
     } else {
-        const unsigned e0 = sq3(P.r0 - C.pr, P.g0 - C.pg, P.b0 - C.pb);
-        const unsigned e1 = sq3(P.r1 - C.pr, P.g1 - C.pg, P.b1 - C.pb);
-        const unsigned e2 = sq3(P.r2 - C.pr, P.g2 - C.pg, P.b2 - C.pb);
+        const unsigned e0 = sq3(P.r0 - pr, P.g0 - pg, P.b0 - pb), e1 = sq3(P.r1 - pr, P.g1 - pg, P.b1 - pb);
+        const unsigned e2 = sq3(P.r2 - pr, P.g2 - pg, P.b2 - pb);
         s = 0;
         e = e0;
         if (e1 < e) { e = e1; s = 1; }
         if (e2 < e) { e = e2; s = 2; }
-        if (M != CM_THREE) {
-            const unsigned e3 = sq3(P.r3 - C.pr, P.g3 - C.pg, P.b3 - C.pb);
+        if (K != K_T3) {
+            const unsigned e3 = sq3(P.r3 - pr, P.g3 - pg, P.b3 - pb);
             if (e3 <= e) { e = e3; s = 3; }  // ties prefer selector 3 (:762)
         }
     }
-    r.err = gsum(C.gm, e);
-    r.sel = gor(C.gm, (unsigned)s << (2 * C.lane));
-    r.mode = M;
+    SelErr o;
+    o.err = gsum(G.gm, e);
+    o.sel = gor(G.gm, (unsigned)s << (2 * G.lane));
+    return o;
+}
+
+template <int IT> __device__ __forceinline__ SelErr fs_any(int K, int lo, int hi) {
+    switch (K) {
+        case K_F4_NONE: return fs_tp<IT, K_F4_NONE>(lo, hi);
+        case K_F4_FASTER: return fs_tp<IT, K_F4_FASTER>(lo, hi);
+        case K_F4_CHECK2: return fs_tp<IT, K_F4_CHECK2>(lo, hi);
+        case K_F4_FULL: return fs_tp<IT, K_F4_FULL>(lo, hi);
+        case K_T3: return fs_tp<IT, K_T3>(lo, hi);
+        default: return fs_tp<IT, K_TB>(lo, hi);
+    }
 }
 
 // ---------------------------------------------------------------------------
 // lane-serial block error: one lane evaluates all 16 texels for its own
-// endpoints (error only; selectors are recomputed texel-parallel for winners)
+// endpoints (error only; the winner's selectors come from fs_tp)
 // ---------------------------------------------------------------------------
-struct Px {
-    float r[16], g[16], b[16];
-};
-
-__device__ __forceinline__ void load_px(const Ctx &C, Px &X) {
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const uint32_t v = C.spx[i];
-        X.r[i] = (float)(v & 0xFF);
-        X.g[i] = (float)((v >> 8) & 0xFF);
-        X.b[i] = (float)((v >> 16) & 0xFF);
-    }
-}
-
-// kinds of lane-serial evaluation
-constexpr int K_NONE = 0, K_FASTER = 1, K_CHECK2 = 2, K_FULL4 = 3, K_FULL3 = 4;
-
-__device__ __forceinline__ int eval_kind(int M, int em) {
-    if (M == CM_FOUR) return em == EM_FULL ? K_FULL4 : (em == EM_CHECK2 ? K_CHECK2 : (em == EM_FASTER ? K_FASTER : K_NONE));
-    if (M == CM_THREE) return em == EM_FULL ? K_FULL3 : (em == EM_CHECK2 ? K_CHECK2 : (em == EM_FASTER ? K_FASTER : K_NONE));
-    return em == EM_FULL ? K_FULL4 : (em == EM_CHECK2 ? K_CHECK2 : (em == EM_FASTER ? K_FASTER : K_NONE));
-}
-
-template <int IT>
-__device__ __forceinline__ float block_err(const Px &X, int kind, int lo, int hi, bool three) {
-    const Pal P = make_pal<IT>(lo, hi, three);
+template <int IT, int K> __device__ __forceinline__ float block_err(const float4 *pf, int lo, int hi) {
+    const Pal P = make_pal<IT>(lo, hi, kind_three(K));
     float tot = 0.0f;
-    if (kind == K_FULL4 || kind == K_FULL3) {
-        // sum_t min_j |p_t - c_j|^2 = sum_t |p_t|^2 + sum_t min_j (|c_j|^2 - 2 p_t.c_j); all terms exact
+    if (K == K_F4_FULL || K == K_T3 || K == K_TB) {
+        // sum_t min_j |p_t - c_j|^2 = sum_t (|p_t|^2 + min_j (|c_j|^2 - 2 p_t.c_j)); every term is an exact integer
         const float v0 = (float)sq3(P.r0, P.g0, P.b0), v1 = (float)sq3(P.r1, P.g1, P.b1);
         const float v2 = (float)sq3(P.r2, P.g2, P.b2), v3 = (float)sq3(P.r3, P.g3, P.b3);
         const float r0 = -2.0f * P.r0, g0 = -2.0f * P.g0, b0 = -2.0f * P.b0;
         const float r1 = -2.0f * P.r1, g1 = -2.0f * P.g1, b1 = -2.0f * P.b1;
         const float r2 = -2.0f * P.r2, g2 = -2.0f * P.g2, b2 = -2.0f * P.b2;
         const float r3 = -2.0f * P.r3, g3 = -2.0f * P.g3, b3 = -2.0f * P.b3;
-        const bool four = kind == K_FULL4;
+        float t0 = 0.0f, t1 = 0.0f;  // two accumulators: shorter dependency chain, still exact
 #pragma unroll
         for (int i = 0; i < 16; i++) {
-            const float pr = X.r[i], pg = X.g[i], pb = X.b[i];
-            float m = fmaf(pb, b0, fmaf(pg, g0, fmaf(pr, r0, v0)));
-            m = fminf(m, fmaf(pb, b1, fmaf(pg, g1, fmaf(pr, r1, v1))));
-            m = fminf(m, fmaf(pb, b2, fmaf(pg, g2, fmaf(pr, r2, v2))));
-            if (four) m = fminf(m, fmaf(pb, b3, fmaf(pg, g3, fmaf(pr, r3, v3))));
-            tot += fmaf(pb, pb, fmaf(pg, pg, fmaf(pr, pr, m)));
+            const float4 p = pf[i];
+            float m = fmaf(p.z, b0, fmaf(p.y, g0, fmaf(p.x, r0, v0)));
+            m = fminf(m, fmaf(p.z, b1, fmaf(p.y, g1, fmaf(p.x, r1, v1))));
+            m = fminf(m, fmaf(p.z, b2, fmaf(p.y, g2, fmaf(p.x, r2, v2))));
+            if (K != K_T3) m = fminf(m, fmaf(p.z, b3, fmaf(p.y, g3, fmaf(p.x, r3, v3))));
+            if (i & 1) t1 += p.w + m;
+            else t0 += p.w + m;
         }
-    } else if (kind == K_FASTER) {
+        tot = t0 + t1;
+    } else if (K == K_F4_FASTER) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
         const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
         const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
@@ -349,34 +371,32 @@ __device__ __forceinline__ float block_err(const Px &X, int kind, int lo, int hi
         const float a2r = 2.0f * ar, a2g = 2.0f * ag, a2b = 2.0f * ab;
 #pragma unroll
         for (int i = 0; i < 16; i++) {
-            const float pr = X.r[i], pg = X.g[i], pb = X.b[i];
-            const float dot = fmaf(pb, a2b, fmaf(pg, a2g, pr * a2r));
+            const float4 p = pf[i];
+            const float dot = fmaf(p.z, a2b, fmaf(p.y, a2g, p.x * a2r));
             const int s = 3 - ((int)(dot <= t0) + (int)(dot < t1) + (int)(dot < t2));  // selector = 3 - level
-            const float cr = (float)sel4(P.r0, P.r1, P.r2, P.r3, s), cg = (float)sel4(P.g0, P.g1, P.g2, P.g3, s);
-            const float cb = (float)sel4(P.b0, P.b1, P.b2, P.b3, s);
-            const float dr = pr - cr, dg = pg - cg, db = pb - cb;
+            const float dr = p.x - (float)sel4(P.r0, P.r1, P.r2, P.r3, s);
+            const float dg = p.y - (float)sel4(P.g0, P.g1, P.g2, P.g3, s);
+            const float db = p.z - (float)sel4(P.b0, P.b1, P.b2, P.b3, s);
             tot += fmaf(db, db, fmaf(dg, dg, dr * dr));
         }
-    } else if (kind == K_CHECK2) {
+    } else if (K == K_F4_CHECK2) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
         const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
         const float far_ = (float)ar, fag = (float)ag, fab = (float)ab;
         const float c0r = (float)P.r0, c0g = (float)P.g0, c0b = (float)P.b0;
 #pragma unroll
         for (int i = 0; i < 16; i++) {
-            const float pr = X.r[i], pg = X.g[i], pb = X.b[i];
-            const float dd = fmaf(pb - c0b, fab, fmaf(pg - c0g, fag, (pr - c0r) * far_));
+            const float4 p = pf[i];
+            const float dd = fmaf(p.z - c0b, fab, fmaf(p.y - c0g, fag, (p.x - c0r) * far_));
             const float sf = __fadd_rn(__fmul_rn(dd, f), 0.5f);
             const int sl = clampi(f2i_x86(sf), 1, 3);
-            const float ar0 = (float)sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - pr;
-            const float ag0 = (float)sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - pg;
-            const float ab0 = (float)sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - pb;
-            const float ar1 = (float)sel4(P.r0, P.r1, P.r2, P.r3, sl) - pr;
-            const float ag1 = (float)sel4(P.g0, P.g1, P.g2, P.g3, sl) - pg;
-            const float ab1 = (float)sel4(P.b0, P.b1, P.b2, P.b3, sl) - pb;
-            const float e0 = fmaf(ab0, ab0, fmaf(ag0, ag0, ar0 * ar0));
-            const float e1 = fmaf(ab1, ab1, fmaf(ag1, ag1, ar1 * ar1));
-            tot += fminf(e0, e1);
+            const float ar0 = (float)sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - p.x;
+            const float ag0 = (float)sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - p.y;
+            const float ab0 = (float)sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - p.z;
+            const float ar1 = (float)sel4(P.r0, P.r1, P.r2, P.r3, sl) - p.x;
+            const float ag1 = (float)sel4(P.g0, P.g1, P.g2, P.g3, sl) - p.y;
+            const float ab1 = (float)sel4(P.b0, P.b1, P.b2, P.b3, sl) - p.z;
+            tot += fminf(fmaf(ab0, ab0, fmaf(ag0, ag0, ar0 * ar0)), fmaf(ab1, ab1, fmaf(ag1, ag1, ar1 * ar1)));
         }
     }
     return tot;
@@ -384,18 +404,27 @@ __device__ __forceinline__ float block_err(const Px &X, int kind, int lo, int hi
 
 // ---------------------------------------------------------------------------
 // FindEndpointsSingleColor(result, pixels, color, is_3color), texel-parallel
-// (BC1Encoder.cpp:443-471). The error is taken against colors[2] of the
-// endpoints held before the lookup, over RGBA (palette alpha 255).
+// (BC1Encoder.cpp:443-471): the error is taken against colors[2] of the
+// endpoints held BEFORE the table lookup, over RGBA (palette alpha 255).
 // ---------------------------------------------------------------------------
-template <int IT>
-__device__ __forceinline__ void single_color_px(const Ctx &C, int stale_lo, int stale_hi, const int av[3], bool is3,
-                                                int &lo, int &hi, uint32_t &err) {
+struct SC {
+    int lo, hi;
+    uint32_t err;
+};
+
+template <int IT> __device__ __noinline__ SC single_color_px(int stale_lo, int stale_hi, bool is3, int which) {
+    const Grp G = grp();
+    const uint32_t v = s_px[G.g][G.lane];
     const Pal P = make_pal<IT>(stale_lo, stale_hi, is3);  // colors[2] is internal index 1 in both orders
-    const int dr = C.pr - P.r1, dg = C.pg - P.g1, db = C.pb - P.b1, da = C.pa - 255;
-    err = gsum(C.gm, (unsigned)(dr * dr + dg * dg + db * db + da * da));
-    const uint32_t mr = g_tab.match5[IT][av[0]], mg = g_tab.match6[IT][av[1]], mb = g_tab.match5[IT][av[2]];
-    lo = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
-    hi = eppack(mr & 0xFF, mg & 0xFF, mb & 0xFF);
+    const int dr = (int)(v & 0xFF) - P.r1, dg = (int)((v >> 8) & 0xFF) - P.g1, db = (int)((v >> 16) & 0xFF) - P.b1;
+    const int da = (int)(v >> 24) - 255;
+    SC o;
+    o.err = gsum(G.gm, (unsigned)(dr * dr + dg * dg + db * db + da * da));
+    const int *M = s_met[G.g][which];
+    const uint32_t mr = g_tab.match5[IT][M[MT_AV]], mg = g_tab.match6[IT][M[MT_AV + 1]], mb = g_tab.match5[IT][M[MT_AV + 2]];
+    o.lo = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
+    o.hi = eppack(mr & 0xFF, mg & 0xFF, mb & 0xFF);
+    return o;
 }
 
 // ---------------------------------------------------------------------------
@@ -409,39 +438,46 @@ __device__ __forceinline__ float fdot4_rn(float a0, float a1, float a2, float a3
     return __fadd_rn(s, __fmul_rn(a3, b3));
 }
 
-template <int IT>
-__device__ void find_endpoints(const Ctx &C, Res &r, const Metrics &m, int mode, bool ignore_black, int power_iters) {
-    if (m.grey) {  // :474-494
-        const int fr = __shfl_sync(C.gm, C.pr, 0, 16);
-        if (m.mx[0] - m.mn[0] < 2) {
-            r.lo = r.hi = eppack(s8to5(fr), s8to6(fr), s8to5(fr));
+__device__ __noinline__ int2 find_endpoints(int mode, bool ignore_black, int power_iters, int which) {
+    const Grp G = grp();
+    const uint32_t v = s_px[G.g][G.lane];
+    const int pr = v & 0xFF, pg = (v >> 8) & 0xFF, pb = (v >> 16) & 0xFF;
+    const int *M = s_met[G.g][which];
+    const int mn[3] = {M[MT_MN], M[MT_MN + 1], M[MT_MN + 2]}, mx[3] = {M[MT_MX], M[MT_MX + 1], M[MT_MX + 2]};
+    const int av[3] = {M[MT_AV], M[MT_AV + 1], M[MT_AV + 2]};
+    int lo, hi;
+    if (M[MT_GREY]) {  // :474-494
+        const int fr = (int)(s_px[G.g][0] & 0xFF);
+        if (mx[0] - mn[0] < 2) {
+            lo = hi = eppack(s8to5(fr), s8to6(fr), s8to5(fr));
         } else {
-            r.lo = eppack(s8to5(m.mn[0]), s8to6(m.mn[0]), s8to5(m.mn[0]));
-            r.hi = eppack(s8to5(m.mx[0]), s8to6(m.mx[0]), s8to5(m.mx[0]));
+            lo = eppack(s8to5(mn[0]), s8to6(mn[0]), s8to5(mn[0]));
+            hi = eppack(s8to5(mx[0]), s8to6(mx[0]), s8to5(mx[0]));
         }
     } else if (mode == EP_LS) {  // :495-552
-        const int d0 = m.mx[0] - m.mn[0], d1 = m.mx[1] - m.mn[1], d2 = m.mx[2] - m.mn[2];
+        const int d0 = mx[0] - mn[0], d1 = mx[1] - mn[1], d2 = mx[2] - mn[2];
         const int c0 = (d0 >= d1 && d0 >= d2) ? 0 : ((d1 >= d2 && d1 >= d0) ? 1 : 2);  // Color::MaxChannelRGB
-        const int p[3] = {C.pr, C.pg, C.pb};
-        const int px0 = c0 == 0 ? C.pr : (c0 == 1 ? C.pg : C.pb);
+        const int p[3] = {pr, pg, pb};
+        const int px0 = c0 == 0 ? pr : (c0 == 1 ? pg : pb);
         unsigned sxy[3];
 #pragma unroll
-        for (int c = 0; c < 3; c++) sxy[c] = gsum(C.gm, (unsigned)(px0 * p[c]));  // zero-initialised (:510 is not)
+        for (int c = 0; c < 3; c++) sxy[c] = gsum(G.gm, (unsigned)(px0 * p[c]));  // zero-initialised (:510 is not)
         float l[3] = {0.f, 0.f, 0.f}, h[3] = {0.f, 0.f, 0.f};
-        const float mn0 = (float)m.mn[c0];
-        l[c0] = mn0;
-        h[c0] = mn0;
-        const unsigned sum_x = (unsigned)m.sum[c0], sum_xx = sxy[c0];
+        const float mn0 = (float)(c0 == 0 ? mn[0] : (c0 == 1 ? mn[1] : mn[2]));
+        const unsigned sum_x = (unsigned)M[MT_SUM + c0], sum_xx = c0 == 0 ? sxy[0] : (c0 == 1 ? sxy[1] : sxy[2]);
+#pragma unroll
+        for (int c = 0; c < 3; c++)
+            if (c == c0) l[c] = h[c] = mn0;
         const float den = __fsub_rn(__uint2float_rn(16u * sum_xx), __uint2float_rn(sum_x * sum_x));
         if (fabsf(den) > 1e-8f) {
 #pragma unroll
-            for (int i = 1; i < 3; i++) {
-                const int c = (c0 + i) % 3;
-                const unsigned sum_y = (unsigned)m.sum[c], sum_xy = sxy[c];
+            for (int c = 0; c < 3; c++) {
+                if (c == c0) continue;
+                const unsigned sum_y = (unsigned)M[MT_SUM + c], sum_xy = sxy[c];
                 const float a = __fdiv_rn(__uint2float_rn((16u * sum_xy) - (sum_x * sum_y)), den);
                 const float b = __fdiv_rn(__uint2float_rn((sum_xx * sum_y) - (sum_xy * sum_x)), den);
-                l[c] = __fadd_rn(b, __fmul_rn(a, l[c0]));
-                h[c] = __fadd_rn(b, __fmul_rn(a, h[c0]));
+                l[c] = __fadd_rn(b, __fmul_rn(a, mn0));
+                h[c] = __fadd_rn(b, __fmul_rn(a, mn0));
             }
         }
 #pragma unroll
@@ -450,59 +486,59 @@ __device__ void find_endpoints(const Ctx &C, Res &r, const Metrics &m, int mode,
             l[c] = __fdiv_rn(__fadd_rn(l[c], inset), 255.0f);
             h[c] = __fdiv_rn(__fsub_rn(h[c], inset), 255.0f);
         }
-        r.lo = precise_round565(l[0], l[1], l[2], C.mid5, C.mid6);
-        r.hi = precise_round565(h[0], h[1], h[2], C.mid5, C.mid6);
+        lo = precise_round565(l[0], l[1], l[2], s_mid5, s_mid6);
+        hi = precise_round565(h[0], h[1], h[2], s_mid5, s_mid6);
     } else if (mode == EP_BB || mode == EP_BBINT) {  // :553-605
-        const int b = C.pb - m.av[2];
-        const int cxz = (int)gsum(C.gm, (unsigned)(b * C.pr - m.av[0]));  // b * r - avg.r, as written (:572)
-        const int cyz = (int)gsum(C.gm, (unsigned)(b * C.pg - m.av[1]));
+        const int b = pb - av[2];
+        const int cxz = (int)gsum(G.gm, (unsigned)(b * pr - av[0]));  // b * r - avg.r, as written (:572)
+        const int cyz = (int)gsum(G.gm, (unsigned)(b * pg - av[1]));
         if (mode == EP_BB) {
             const float bias = __fdiv_rn(8.0f, 255.0f);
             float l[3], h[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                l[c] = __fdiv_rn((float)m.mn[c], 255.0f);
-                h[c] = __fdiv_rn((float)m.mx[c], 255.0f);
+                l[c] = __fdiv_rn((float)mn[c], 255.0f);
+                h[c] = __fdiv_rn((float)mx[c], 255.0f);
                 const float inset = __fdiv_rn(__fsub_rn(__fsub_rn(h[c], l[c]), bias), 16.0f);
                 l[c] = __fadd_rn(l[c], inset);
                 h[c] = __fsub_rn(h[c], inset);
             }
             if (cxz < 0) { const float t = l[0]; l[0] = h[0]; h[0] = t; }
             if (cyz < 0) { const float t = l[1]; l[1] = h[1]; h[1] = t; }
-            r.lo = precise_round565(l[0], l[1], l[2], C.mid5, C.mid6);
-            r.hi = precise_round565(h[0], h[1], h[2], C.mid5, C.mid6);
+            lo = precise_round565(l[0], l[1], l[2], s_mid5, s_mid6);
+            hi = precise_round565(h[0], h[1], h[2], s_mid5, s_mid6);
         } else {
-            int mn[3], mx[3];
+            int a[3], z[3];
 #pragma unroll
             for (int c = 0; c < 3; c++) {
-                const int inset = ((m.mx[c] - m.mn[c]) - 8) >> 4;
-                mn[c] = clamp255(m.mn[c] + inset);
-                mx[c] = clamp255(m.mx[c] - inset);
+                const int inset = ((mx[c] - mn[c]) - 8) >> 4;
+                a[c] = clamp255(mn[c] + inset);
+                z[c] = clamp255(mx[c] - inset);
             }
-            if (cxz < 0) { const int t = mn[0]; mn[0] = mx[0]; mx[0] = t; }
-            if (cyz < 0) { const int t = mn[1]; mn[1] = mx[1]; mx[1] = t; }
-            r.lo = eppack(s8to5(mn[0]), s8to6(mn[1]), s8to5(mn[2]));
-            r.hi = eppack(s8to5(mx[0]), s8to6(mx[1]), s8to5(mx[2]));
+            if (cxz < 0) { const int t = a[0]; a[0] = z[0]; z[0] = t; }
+            if (cyz < 0) { const int t = a[1]; a[1] = z[1]; z[1] = t; }
+            lo = eppack(s8to5(a[0]), s8to6(a[1]), s8to5(a[2]));
+            hi = eppack(s8to5(z[0]), s8to6(z[1]), s8to5(z[2]));
         }
     } else {  // PCA, :606-674
-        const bool blk = (C.pr | C.pg | C.pb) < 4;
+        const bool blk = (pr | pg | pb) < 4;
         const bool inc = !(ignore_black && blk);
-        const int dr = C.pr - m.av[0], dg = C.pg - m.av[1], db = C.pb - m.av[2];
+        const int dr = pr - av[0], dg = pg - av[1], db = pb - av[2];
         // covariance from identity, accumulated over included texels: exact integers
-        const int s00 = (int)gsum(C.gm, inc ? (unsigned)(dr * dr) : 0u);
-        const int s01 = (int)gsum(C.gm, inc ? (unsigned)(dr * dg) : 0u);
-        const int s02 = (int)gsum(C.gm, inc ? (unsigned)(dr * db) : 0u);
-        const int s11 = (int)gsum(C.gm, inc ? (unsigned)(dg * dg) : 0u);
-        const int s12 = (int)gsum(C.gm, inc ? (unsigned)(dg * db) : 0u);
-        const int s22 = (int)gsum(C.gm, inc ? (unsigned)(db * db) : 0u);
+        const int s00 = (int)gsum(G.gm, inc ? (unsigned)(dr * dr) : 0u);
+        const int s01 = (int)gsum(G.gm, inc ? (unsigned)(dr * dg) : 0u);
+        const int s02 = (int)gsum(G.gm, inc ? (unsigned)(dr * db) : 0u);
+        const int s11 = (int)gsum(G.gm, inc ? (unsigned)(dg * dg) : 0u);
+        const int s12 = (int)gsum(G.gm, inc ? (unsigned)(dg * db) : 0u);
+        const int s22 = (int)gsum(G.gm, inc ? (unsigned)(db * db) : 0u);
         const float k255 = 255.0f;
         const float c00 = __fdiv_rn((float)(1 + s00), k255), c01 = __fdiv_rn((float)s01, k255);
         const float c02 = __fdiv_rn((float)s02, k255), c11 = __fdiv_rn((float)(1 + s11), k255);
         const float c12 = __fdiv_rn((float)s12, k255), c22 = __fdiv_rn((float)(1 + s22), k255);
         const float c33 = __fdiv_rn(1.0f, k255), z = __fdiv_rn(0.0f, k255);
-        float d0 = __fsub_rn((float)m.mx[0], (float)m.mn[0]);
-        float d1 = __fsub_rn((float)m.mx[1], (float)m.mn[1]);
-        float d2 = __fsub_rn((float)m.mx[2], (float)m.mn[2]);
+        float d0 = __fsub_rn((float)mx[0], (float)mn[0]);
+        float d1 = __fsub_rn((float)mx[1], (float)mn[1]);
+        float d2 = __fsub_rn((float)mx[2], (float)mn[2]);
         float d3 = __fsub_rn(0.0f, 0.0f);
         if (c02 < 0) d0 = -d0;
         if (c12 < 0) d1 = -d1;
@@ -523,82 +559,89 @@ __device__ void find_endpoints(const Ctx &C, Res &r, const Metrics &m, int mode,
             a0 = __fmul_rn(d0, s); a1 = __fmul_rn(d1, s); a2 = __fmul_rn(d2, s); a3 = __fmul_rn(d3, s);
         }
         a0 = __fmul_rn(a0, 16.0f); a1 = __fmul_rn(a1, 16.0f); a2 = __fmul_rn(a2, 16.0f); a3 = __fmul_rn(a3, 16.0f);
-        const float dot = fdot4_rn((float)C.pr, (float)C.pg, (float)C.pb, 0.0f, a0, a1, a2, a3);
+        const float dot = fdot4_rn((float)pr, (float)pg, (float)pb, 0.0f, a0, a1, a2, a3);
         // first index of the maximum / minimum (strict > / < scan, :654-670)
         float vmax = inc ? dot : -INFINITY, vmin = inc ? dot : INFINITY;
-        int imax = C.lane, imin = C.lane;
+        int imax = G.lane, imin = G.lane;
 #pragma unroll
         for (int off = 8; off >= 1; off >>= 1) {
-            const float ov = __shfl_xor_sync(C.gm, vmax, off, 16);
-            const int oi = __shfl_xor_sync(C.gm, imax, off, 16);
+            const float ov = __shfl_xor_sync(G.gm, vmax, off, 16);
+            const int oi = __shfl_xor_sync(G.gm, imax, off, 16);
             if (ov > vmax || (ov == vmax && oi < imax)) { vmax = ov; imax = oi; }
-            const float ow = __shfl_xor_sync(C.gm, vmin, off, 16);
-            const int oj = __shfl_xor_sync(C.gm, imin, off, 16);
+            const float ow = __shfl_xor_sync(G.gm, vmin, off, 16);
+            const int oj = __shfl_xor_sync(G.gm, imin, off, 16);
             if (ow < vmin || (ow == vmin && oj < imin)) { vmin = ow; imin = oj; }
         }
-        const uint32_t pmin = C.spx[imin], pmax = C.spx[imax];
-        r.lo = eppack(s8to5(pmin & 0xFF), s8to6((pmin >> 8) & 0xFF), s8to5((pmin >> 16) & 0xFF));
-        r.hi = eppack(s8to5(pmax & 0xFF), s8to6((pmax >> 8) & 0xFF), s8to5((pmax >> 16) & 0xFF));
+        const uint32_t pmin = s_px[G.g][imin], pmax = s_px[G.g][imax];
+        lo = eppack(s8to5(pmin & 0xFF), s8to6((pmin >> 8) & 0xFF), s8to5((pmin >> 16) & 0xFF));
+        hi = eppack(s8to5(pmax & 0xFF), s8to6((pmax >> 8) & 0xFF), s8to5((pmax >> 16) & 0xFF));
     }
-    r.mode = CM_INCOMPLETE;
+    return make_int2(lo, hi);
 }
 
 // ---------------------------------------------------------------------------
-// RefineEndpointsLS<FourColor>(result, pixels, metrics) (BC1Encoder.cpp:781-825).
-// Only the FourColor instantiation is ever called (RefineBlockLS, :860): no
-// texel is skipped and the 4-colour weights apply to every colour mode.
+// RefineBlockLS<M> (BC1Encoder.cpp:852-875) with
+// RefineEndpointsLS<FourColor>(result, pixels, metrics) (:781-825). Only the
+// FourColor instantiation of the latter is ever called (:860): no texel is
+// skipped and the 4-colour weights apply to every colour mode.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ bool refine_endpoints_ls_px(const Ctx &C, Res &r, const Metrics &m) {
-    const int s = (r.sel >> (2 * C.lane)) & 3;
-    const unsigned b1 = __ballot_sync(C.gm, s == 1) & C.gm, b2 = __ballot_sync(C.gm, s == 2) & C.gm;
-    const unsigned b3 = __ballot_sync(C.gm, s == 3) & C.gm;
-    const int n1 = __popc(b1), n2 = __popc(b2), n3 = __popc(b3), n0 = 16 - n1 - n2 - n3;
-    // sum of OrderTable<4>::Weights[sel]: {s^2, s(3-s), s(3-s), (3-s)^2}
-    float m0 = (float)(n1 + 4 * n2 + 9 * n3), m1 = (float)(2 * n1 + 2 * n2), m2 = m1, m3 = (float)(9 * n0 + 4 * n1 + n2);
-    const float q00r = (float)(int)gsum(C.gm, (unsigned)(C.pr * s));
-    const float q00g = (float)(int)gsum(C.gm, (unsigned)(C.pg * s));
-    const float q00b = (float)(int)gsum(C.gm, (unsigned)(C.pb * s));
-    const float det = __fsub_rn(__fmul_rn(m0, m3), __fmul_rn(m1, m2));
-    if (fabsf(det) < 1e-8f) {
-        r.mode = CM_INCOMPLETE;
-        return false;
-    }
-    const float t = m0; m0 = m3; m3 = t;
-    m1 = -m1;
-    m2 = -m2;
-    const float sc = __fdiv_rn(__fdiv_rn(3.0f, 255.0f), det);
-    m0 = __fmul_rn(m0, sc); m1 = __fmul_rn(m1, sc); m2 = __fmul_rn(m2, sc); m3 = __fmul_rn(m3, sc);
-    const float q10r = (float)(m.sum[0] * 3) - q00r, q10g = (float)(m.sum[1] * 3) - q00g, q10b = (float)(m.sum[2] * 3) - q00b;
-    r.mode = CM_FOUR;
-    r.lo = precise_round565(__fadd_rn(__fmul_rn(m0, q00r), __fmul_rn(m1, q10r)),
-                            __fadd_rn(__fmul_rn(m0, q00g), __fmul_rn(m1, q10g)),
-                            __fadd_rn(__fmul_rn(m0, q00b), __fmul_rn(m1, q10b)), C.mid5, C.mid6);
-    r.hi = precise_round565(__fadd_rn(__fmul_rn(m2, q00r), __fmul_rn(m3, q10r)),
-                            __fadd_rn(__fmul_rn(m2, q00g), __fmul_rn(m3, q10g)),
-                            __fadd_rn(__fmul_rn(m2, q00b), __fmul_rn(m3, q10b)), C.mid5, C.mid6);
-    return true;
-}
-
-// RefineBlockLS<M> (BC1Encoder.cpp:852-875)
-template <int IT>
-__device__ void refine_block_ls(const Ctx &C, int M, Res &r, const Metrics &m, int em, int passes) {
+template <int IT, int K> __device__ __noinline__ Res refine_ls(Res r, int passes, int which) {
+    const Grp G = grp();
+    const uint32_t v = s_px[G.g][G.lane];
+    const int pr = v & 0xFF, pg = (v >> 8) & 0xFF, pb = (v >> 16) & 0xFF;
+    const int *M = s_met[G.g][which];
     for (int pass = 0; pass < passes; pass++) {
         Res t = r;
-        if (!refine_endpoints_ls_px(C, t, m)) {
-            int lo, hi;
-            uint32_t err;
-            single_color_px<IT>(C, t.lo, t.hi, m.av, M != CM_FOUR, lo, hi, err);
-            t.lo = lo;
-            t.hi = hi;
-            t.err = err;
+        const int s = (t.sel >> (2 * G.lane)) & 3;
+        const int n1 = __popc(__ballot_sync(G.gm, s == 1) & G.gm), n2 = __popc(__ballot_sync(G.gm, s == 2) & G.gm);
+        const int n3 = __popc(__ballot_sync(G.gm, s == 3) & G.gm), n0 = 16 - n1 - n2 - n3;
+        // sum of OrderTable<4>::Weights[sel] = {s^2, s(3-s), s(3-s), (3-s)^2}: exact small integers
+        float m0 = (float)(n1 + 4 * n2 + 9 * n3), m1 = (float)(2 * n1 + 2 * n2), m2 = m1, m3 = (float)(9 * n0 + 4 * n1 + n2);
+        const float q00r = (float)(int)gsum(G.gm, (unsigned)(pr * s));
+        const float q00g = (float)(int)gsum(G.gm, (unsigned)(pg * s));
+        const float q00b = (float)(int)gsum(G.gm, (unsigned)(pb * s));
+        const float det = __fsub_rn(__fmul_rn(m0, m3), __fmul_rn(m1, m2));
+        if (fabsf(det) < 1e-8f) {  // not multicolour: FindEndpointsSingleColor on the average
+            const SC sc = single_color_px<IT>(t.lo, t.hi, K != K_F4_NONE && kind_three(K), which);
+            t.lo = sc.lo;
+            t.hi = sc.hi;
+            t.err = sc.err;
             t.sel = 0x55555555u;
-            t.mode = M != CM_FOUR ? CM_THREE : CM_FOUR;
+            t.mode = kind_three(K) ? CM_THREE : CM_FOUR;
         } else {
-            find_selectors_tp<IT>(C, M, em, t);
+            const float tt = m0; m0 = m3; m3 = tt;
+            m1 = -m1;
+            m2 = -m2;
+            const float sc = __fdiv_rn(__fdiv_rn(3.0f, 255.0f), det);
+            m0 = __fmul_rn(m0, sc); m1 = __fmul_rn(m1, sc); m2 = __fmul_rn(m2, sc); m3 = __fmul_rn(m3, sc);
+            const float q10r = (float)(M[MT_SUM] * 3) - q00r, q10g = (float)(M[MT_SUM + 1] * 3) - q00g;
+            const float q10b = (float)(M[MT_SUM + 2] * 3) - q00b;
+            t.lo = precise_round565(__fadd_rn(__fmul_rn(m0, q00r), __fmul_rn(m1, q10r)),
+                                    __fadd_rn(__fmul_rn(m0, q00g), __fmul_rn(m1, q10g)),
+                                    __fadd_rn(__fmul_rn(m0, q00b), __fmul_rn(m1, q10b)), s_mid5, s_mid6);
+            t.hi = precise_round565(__fadd_rn(__fmul_rn(m2, q00r), __fmul_rn(m3, q10r)),
+                                    __fadd_rn(__fmul_rn(m2, q00g), __fmul_rn(m3, q10g)),
+                                    __fadd_rn(__fmul_rn(m2, q00b), __fmul_rn(m3, q10b)), s_mid5, s_mid6);
+            const SelErr se = fs_tp<IT, K>(t.lo, t.hi);
+            t.sel = se.sel;
+            t.err = se.err;
+            t.mode = kind_mode(K);
         }
         if (t.lo == r.lo && t.hi == r.hi) break;
-        if (em == EM_NONE || t.err < r.err) r = t;
-        else return;
+        if (K == K_F4_NONE || t.err < r.err) r = t;
+        else break;
+    }
+    return r;
+}
+
+template <int IT> __device__ __forceinline__ Res refine_ls_any(int K, Res r, int passes, int which) {
+    switch (K) {
+        case K_F4_NONE: return refine_ls<IT, K_F4_NONE>(r, passes, which);
+        case K_F4_FASTER: return refine_ls<IT, K_F4_FASTER>(r, passes, which);
+        case K_F4_CHECK2: return refine_ls<IT, K_F4_CHECK2>(r, passes, which);
+        case K_F4_FULL: return refine_ls<IT, K_F4_FULL>(r, passes, which);
+        case K_T3: return refine_ls<IT, K_T3>(r, passes, which);
+        default: return refine_ls<IT, K_TB>(r, passes, which);
     }
 }
 
@@ -606,12 +649,35 @@ __device__ __forceinline__ bool is_single_hash(bool four, int h) {
     return four ? (h == 15 || h == 700 || h == 753 || h == 515) : (h == 12 || h == 15 || h == 89);
 }
 
+// RefineEndpointsLS<M>(result, sums, matrix, hash) (BC1Encoder.cpp:827-850):
+// q10 = sums at the ordering's cumulative selector counts (exact integers)
+__device__ __forceinline__ int2 ls_from_sums(const int *S, float4 f, uint32_t o, bool four) {
+    const int l1 = o & 0xFF, l2 = l1 + ((o >> 8) & 0xFF), l3 = l2 + ((o >> 16) & 0xFF);
+    int qr = S[3 * l1] + S[3 * l2], qg = S[3 * l1 + 1] + S[3 * l2 + 1], qb = S[3 * l1 + 2] + S[3 * l2 + 2];
+    if (four) {
+        qr += S[3 * l3];
+        qg += S[3 * l3 + 1];
+        qb += S[3 * l3 + 2];
+    }
+    const float denom = four ? 3.0f : 2.0f;
+    const float fr = (float)qr, fg = (float)qg, fb = (float)qb;
+    const float q0r = (float)S[48] * denom - fr, q0g = (float)S[49] * denom - fg, q0b = (float)S[50] * denom - fb;
+    const int lo = precise_round565(__fadd_rn(__fmul_rn(f.x, q0r), __fmul_rn(f.y, fr)),
+                                    __fadd_rn(__fmul_rn(f.x, q0g), __fmul_rn(f.y, fg)),
+                                    __fadd_rn(__fmul_rn(f.x, q0b), __fmul_rn(f.y, fb)), s_mid5, s_mid6);
+    const int hi = precise_round565(__fadd_rn(__fmul_rn(f.z, q0r), __fmul_rn(f.w, fr)),
+                                    __fadd_rn(__fmul_rn(f.z, q0g), __fmul_rn(f.w, fg)),
+                                    __fadd_rn(__fmul_rn(f.z, q0b), __fmul_rn(f.w, fb)), s_mid5, s_mid6);
+    return make_int2(lo, hi);
+}
+
 // ---------------------------------------------------------------------------
-// RefineBlockCF<M> (BC1Encoder.cpp:877-928), ordering-parallel
+// RefineBlockCF<M> (BC1Encoder.cpp:877-928)
 // ---------------------------------------------------------------------------
-template <int IT>
-__device__ void refine_block_cf(const Ctx &C, int M, Res &r, const Metrics &m, int em, unsigned orderings, bool exhaustive) {
-    const bool four = (M & 0x0F) == 4;
+template <int IT, int K> __device__ __noinline__ Res refine_cf(Res r, unsigned orderings, bool exhaustive, int which) {
+    constexpr bool four = !kind_three(K);
+    constexpr int M = kind_mode(K);
+    const Grp G = grp();
     const Res orig = r;
     // Histogram of the selectors -> start ordering (OrderTable::GetHash, OrderTable.h:91-104)
     const uint32_t w = orig.sel;
@@ -623,137 +689,171 @@ __device__ void refine_block_cf(const Ctx &C, int M, Res &r, const Metrics &m, i
     } else {
         start = n0 == 16 ? 12 : n1 == 16 ? 15 : n2 == 16 ? 89 : (int)g_tab.hash3[n0 | (n1 << 4)];
     }
+    const unsigned total = exhaustive ? (four ? 969u : 153u) : orderings;
+    uint16_t *row = s_row[G.g];
+    if (!exhaustive) {  // stage the BestOrders row (8 or 2 entries per lane)
+        const uint16_t *src = four ? g_tab.best4 + start * 128 : g_tab.best3 + start * 32;
+        for (unsigned q = G.lane; q < total; q += 16) row[q] = src[q];
+    }
     // projection onto high - low, sort, prefix sums (:891-909); all values exact integers
+    const uint32_t v = s_px[G.g][G.lane];
+    const int pr = v & 0xFF, pg = (v >> 8) & 0xFF, pb = (v >> 16) & 0xFF;
     const int axr = s5to8(epr(orig.hi)) - s5to8(epr(orig.lo));
     const int axg = s6to8(epg(orig.hi)) - s6to8(epg(orig.lo));
     const int axb = s5to8(epb(orig.hi)) - s5to8(epb(orig.lo));
-    const int dot = C.pr * axr + C.pg * axg + C.pb * axb;
-    const uint32_t key = ((uint32_t)(0x1000000 + dot) << 4) | (uint32_t)C.lane;
+    const uint32_t key = ((uint32_t)(0x1000000 + pr * axr + pg * axg + pb * axb) << 4) | (uint32_t)G.lane;
     int rank = 0;  // keys are distinct (the texel index is in the low bits)
 #pragma unroll
-    for (int i = 0; i < 16; i++) rank += __shfl_sync(C.gm, key, i, 16) < key;
+    for (int i = 0; i < 16; i++) rank += __shfl_sync(G.gm, key, i, 16) < key;
     int sr = 0, sg = 0, sb = 0;  // sum of the texels ranked at or below this lane's position
 #pragma unroll
     for (int j = 0; j < 16; j++) {
-        if (__shfl_sync(C.gm, rank, j, 16) <= C.lane) {
-            const uint32_t v = C.spx[j];
-            sr += v & 0xFF;
-            sg += (v >> 8) & 0xFF;
-            sb += (v >> 16) & 0xFF;
+        if (__shfl_sync(G.gm, rank, j, 16) <= G.lane) {
+            const uint32_t u = s_px[G.g][j];
+            sr += u & 0xFF;
+            sg += (u >> 8) & 0xFF;
+            sb += (u >> 16) & 0xFF;
         }
     }
-    C.ssum[3 * (C.lane + 1) + 0] = sr;
-    C.ssum[3 * (C.lane + 1) + 1] = sg;
-    C.ssum[3 * (C.lane + 1) + 2] = sb;
-    if (C.lane == 0) C.ssum[0] = C.ssum[1] = C.ssum[2] = 0;
-    __syncwarp(C.gm);
+    int *S = s_sum[G.g];
+    S[3 * (G.lane + 1) + 0] = sr;
+    S[3 * (G.lane + 1) + 1] = sg;
+    S[3 * (G.lane + 1) + 2] = sb;
+    if (G.lane == 0) S[0] = S[1] = S[2] = 0;
+    __syncwarp(G.gm);
 
     // the single-colour trial is the same for every single-colour ordering of this call
-    int sc_lo, sc_hi;
-    uint32_t sc_err;
-    single_color_px<IT>(C, orig.lo, orig.hi, m.av, !four, sc_lo, sc_hi, sc_err);
+    const SC sc = single_color_px<IT>(orig.lo, orig.hi, !four, which);
 
-    Px X;
-    load_px(C, X);
-    const int kind = eval_kind(M, em);
-    const float denom = four ? 3.0f : 2.0f;
-    const float t16r = (float)C.ssum[48], t16g = (float)C.ssum[49], t16b = (float)C.ssum[50];
-    const unsigned total = exhaustive ? (four ? 969u : 153u) : orderings;
-    float best = INFINITY;
-    int bq = 0x7FFF, blo = 0, bhi = 0;
-    for (unsigned q = C.lane; q < total; q += 16) {
-        const int th = exhaustive ? (int)q : (four ? (int)g_tab.best4[start * 128 + q] : (int)g_tab.best3[start * 32 + q]);
-        int lo, hi;
-        float e;
-        if (is_single_hash(four, th)) {
-            lo = sc_lo;
-            hi = sc_hi;
-            e = (float)sc_err;
-        } else {
-            // RefineEndpointsLS<M>(result, sums, matrix, hash), :827-850
-            const float4 f = four ? g_tab.factors4[th] : g_tab.factors3[th];
-            const uint32_t o = four ? g_tab.orders4[th] : g_tab.orders3[th];
-            const int l1 = o & 0xFF, l2 = l1 + ((o >> 8) & 0xFF), l3 = l2 + ((o >> 16) & 0xFF);
-            int q10r = C.ssum[3 * l1] + C.ssum[3 * l2], q10g = C.ssum[3 * l1 + 1] + C.ssum[3 * l2 + 1];
-            int q10b = C.ssum[3 * l1 + 2] + C.ssum[3 * l2 + 2];
-            if (four) {
-                q10r += C.ssum[3 * l3];
-                q10g += C.ssum[3 * l3 + 1];
-                q10b += C.ssum[3 * l3 + 2];
+    if (total <= 4) {
+        // few orderings: evaluate them in sequence, texel-parallel (the reference's loop as written)
+        for (unsigned q = 0; q < total; q++) {
+            const int th = exhaustive ? (int)q : (int)row[q];
+            Res t;
+            if (is_single_hash(four, th)) {
+                t.lo = sc.lo;
+                t.hi = sc.hi;
+                t.err = sc.err;
+                t.sel = 0x55555555u;
+            } else {
+                const int2 e = ls_from_sums(S, four ? g_tab.factors4[th] : g_tab.factors3[th],
+                                            four ? g_tab.orders4[th] : g_tab.orders3[th], four);
+                t.lo = e.x;
+                t.hi = e.y;
+                const SelErr se = fs_tp<IT, K>(t.lo, t.hi);
+                t.sel = se.sel;
+                t.err = se.err;
             }
-            const float fr = (float)q10r, fg = (float)q10g, fb = (float)q10b;
-            const float q00r = t16r * denom - fr, q00g = t16g * denom - fg, q00b = t16b * denom - fb;
-            lo = precise_round565(__fadd_rn(__fmul_rn(f.x, q00r), __fmul_rn(f.y, fr)),
-                                  __fadd_rn(__fmul_rn(f.x, q00g), __fmul_rn(f.y, fg)),
-                                  __fadd_rn(__fmul_rn(f.x, q00b), __fmul_rn(f.y, fb)), C.mid5, C.mid6);
-            hi = precise_round565(__fadd_rn(__fmul_rn(f.z, q00r), __fmul_rn(f.w, fr)),
-                                  __fadd_rn(__fmul_rn(f.z, q00g), __fmul_rn(f.w, fg)),
-                                  __fadd_rn(__fmul_rn(f.z, q00b), __fmul_rn(f.w, fb)), C.mid5, C.mid6);
-            e = block_err<IT>(X, kind, lo, hi, !four);
+            t.mode = M;
+            if (t.err < r.err) r = t;
+            if (t.err == 0) break;
         }
-        if (e < best) {
-            best = e;
-            bq = (int)q;
-            blo = lo;
-            bhi = hi;
+    } else {
+        // ordering-parallel: lane l evaluates orderings l, l+16, ...; argmin over (error, index)
+        const float4 *pf = s_pf[G.g];
+        float best = INFINITY;
+        int bq = 0x7FFF, blo = 0, bhi = 0;
+        unsigned q = G.lane;
+        int th = 0;
+        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
+        uint32_t o = 0;
+        if (q < total) {
+            th = exhaustive ? (int)q : (int)row[q];
+            f = four ? g_tab.factors4[th] : g_tab.factors3[th];
+            o = four ? g_tab.orders4[th] : g_tab.orders3[th];
+        }
+        for (; q < total; q += 16) {
+            // prefetch the next ordering's table entries while this one is evaluated
+            const unsigned qn = q + 16;
+            int thn = 0;
+            float4 fn = f;
+            uint32_t on = o;
+            if (qn < total) {
+                thn = exhaustive ? (int)qn : (int)row[qn];
+                fn = four ? g_tab.factors4[thn] : g_tab.factors3[thn];
+                on = four ? g_tab.orders4[thn] : g_tab.orders3[thn];
+            }
+            int lo, hi;
+            float e;
+            if (is_single_hash(four, th)) {
+                lo = sc.lo;
+                hi = sc.hi;
+                e = (float)sc.err;
+            } else {
+                const int2 ep = ls_from_sums(S, f, o, four);
+                lo = ep.x;
+                hi = ep.y;
+                e = block_err<IT, K>(pf, lo, hi);
+            }
+            if (e < best) {
+                best = e;
+                bq = (int)q;
+                blo = lo;
+                bhi = hi;
+            }
+            th = thn;
+            f = fn;
+            o = on;
+        }
+        const uint32_t be = best == INFINITY ? UINT_MAX : (uint32_t)best;
+        const uint32_t min_e = gmin(G.gm, be);
+        const uint32_t min_q = gmin(G.gm, be == min_e ? (uint32_t)bq : 0xFFFFu);
+        if (min_e < orig.err) {
+            const int wl = (int)(min_q & 15);
+            r.lo = __shfl_sync(G.gm, blo, wl, 16);
+            r.hi = __shfl_sync(G.gm, bhi, wl, 16);
+            r.err = min_e;
+            r.mode = M;
+            const int wth = exhaustive ? (int)min_q : (int)row[min_q];
+            r.sel = is_single_hash(four, wth) ? 0x55555555u : fs_tp<IT, K>(r.lo, r.hi).sel;
         }
     }
-    const uint32_t be = best == INFINITY ? UINT_MAX : (uint32_t)best;
-    const uint32_t min_e = gmin(C.gm, be);
-    const uint32_t min_q = gmin(C.gm, be == min_e ? (uint32_t)bq : 0xFFFFu);
-    if (min_e < orig.err) {
-        const int wl = (int)(min_q & 15);
-        r.lo = __shfl_sync(C.gm, blo, wl, 16);
-        r.hi = __shfl_sync(C.gm, bhi, wl, 16);
-        r.err = min_e;
-        r.mode = M;
-        const int wth = exhaustive ? (int)min_q : (four ? (int)g_tab.best4[start * 128 + min_q] : (int)g_tab.best3[start * 32 + min_q]);
-        if (is_single_hash(four, wth)) {
-            r.sel = 0x55555555u;
-        } else {
-            Res t = r;
-            find_selectors_tp<IT>(C, M, em, t);
-            r.sel = t.sel;
-        }
+    __syncwarp(G.gm);  // s_sum and s_row are rewritten by the next call
+    return r;
+}
+
+template <int IT> __device__ __forceinline__ Res refine_cf_any(int K, Res r, unsigned orderings, bool exhaustive, int which) {
+    switch (K) {
+        case K_F4_NONE: return refine_cf<IT, K_F4_NONE>(r, orderings, exhaustive, which);
+        case K_F4_FASTER: return refine_cf<IT, K_F4_FASTER>(r, orderings, exhaustive, which);
+        case K_F4_CHECK2: return refine_cf<IT, K_F4_CHECK2>(r, orderings, exhaustive, which);
+        case K_F4_FULL: return refine_cf<IT, K_F4_FULL>(r, orderings, exhaustive, which);
+        default: return refine_cf<IT, K_T3>(r, orderings, exhaustive, which);
     }
-    __syncwarp(C.gm);  // ssum is rewritten by the next call
 }
 
 // ---------------------------------------------------------------------------
 // EndpointSearch (BC1Encoder.cpp:930-996), round-parallel speculation
 // ---------------------------------------------------------------------------
-template <int IT>
-__device__ void endpoint_search(const Ctx &C, Res &r, int em4, unsigned rounds) {
-    Px X;
-    load_px(C, X);
+template <int IT, int K> __device__ __noinline__ Res endpoint_search(Res r, unsigned rounds) {
+    const Grp G = grp();
+    const float4 *pf = s_pf[G.g];
+    const unsigned sh = (G.gm & 0xFFFFu) ? 0 : 16;
     unsigned prev = 0, i0 = 0;
     int forbidden = -1;
     bool moved = false;
     while (i0 < rounds) {
-        const unsigned i = i0 + (unsigned)C.lane;
+        const unsigned i = i0 + (unsigned)G.lane;
         const bool active = i < rounds && (int)(i & 31) != forbidden;
-        const int M = r.mode == CM_THREE ? CM_THREE : (r.mode == CM_TB ? CM_TB : CM_FOUR);
-        const int kind = eval_kind(M, M == CM_FOUR ? em4 : EM_FULL);
-        const uint16_t v = C.vox[i & 15];
-        const int ddr = ((int)((unsigned)v << 30)) >> 30, ddg = ((int)((unsigned)v << 28)) >> 30;
-        const int ddb = ((int)((unsigned)v << 26)) >> 30;
+        const uint16_t vx = s_vox[i & 15];
+        const int ddr = ((int)((unsigned)vx << 30)) >> 30, ddg = ((int)((unsigned)vx << 28)) >> 30;
+        const int ddb = ((int)((unsigned)vx << 26)) >> 30;
         int lo = r.lo, hi = r.hi;
         if (i & 16) lo = eppack(clampi(epr(lo) + ddr, 0, 31), clampi(epg(lo) + ddg, 0, 63), clampi(epb(lo) + ddb, 0, 31));
         else hi = eppack(clampi(epr(hi) + ddr, 0, 31), clampi(epg(hi) + ddg, 0, 63), clampi(epb(hi) + ddb, 0, 31));
         float e = INFINITY;
-        if (active) e = block_err<IT>(X, kind, lo, hi, M != CM_FOUR);
+        if (active) e = block_err<IT, K>(pf, lo, hi);
         const bool improve = active && e < (float)r.err;
         const bool stop = active && (i - prev > 32);
-        const unsigned sh = C.gm & 0xFFFFu ? 0 : 16;
-        const unsigned bi = (__ballot_sync(C.gm, improve) >> sh) & 0xFFFFu;
-        const unsigned bs = (__ballot_sync(C.gm, stop) >> sh) & 0xFFFFu;
+        const unsigned bi = (__ballot_sync(G.gm, improve) >> sh) & 0xFFFFu;
+        const unsigned bs = (__ballot_sync(G.gm, stop) >> sh) & 0xFFFFu;
         const int fi = bi ? __ffs(bi) - 1 : 16, fs = bs ? __ffs(bs) - 1 : 16;
         if (bi && fi <= fs) {  // the first improving round is accepted
             const unsigned j = i0 + (unsigned)fi;
-            r.lo = __shfl_sync(C.gm, lo, fi, 16);
-            r.hi = __shfl_sync(C.gm, hi, fi, 16);
-            r.err = (uint32_t)__shfl_sync(C.gm, e, fi, 16);
-            forbidden = (int)((C.vox[j & 15] >> 8) & 15) | (int)(j & 16);
+            r.lo = __shfl_sync(G.gm, lo, fi, 16);
+            r.hi = __shfl_sync(G.gm, hi, fi, 16);
+            r.err = (uint32_t)__shfl_sync(G.gm, e, fi, 16);
+            forbidden = (int)((s_vox[j & 15] >> 8) & 15) | (int)(j & 16);
             prev = j;
             i0 = j + 1;
             moved = true;
@@ -763,19 +863,26 @@ __device__ void endpoint_search(const Ctx &C, Res &r, int em4, unsigned rounds) 
             i0 += 16;
         }
     }
-    if (moved) {  // selectors of the accepted endpoints
-        const int M = r.mode == CM_THREE ? CM_THREE : (r.mode == CM_TB ? CM_TB : CM_FOUR);
-        Res t = r;
-        find_selectors_tp<IT>(C, M, M == CM_FOUR ? em4 : EM_FULL, t);
-        r.sel = t.sel;
+    if (moved) r.sel = fs_tp<IT, K>(r.lo, r.hi).sel;  // selectors of the accepted endpoints
+    return r;
+}
+
+template <int IT> __device__ __forceinline__ Res endpoint_search_any(int K, Res r, unsigned rounds) {
+    switch (K) {
+        case K_F4_NONE: return endpoint_search<IT, K_F4_NONE>(r, rounds);
+        case K_F4_FASTER: return endpoint_search<IT, K_F4_FASTER>(r, rounds);
+        case K_F4_CHECK2: return endpoint_search<IT, K_F4_CHECK2>(r, rounds);
+        case K_F4_FULL: return endpoint_search<IT, K_F4_FULL>(r, rounds);
+        case K_T3: return endpoint_search<IT, K_T3>(r, rounds);
+        default: return endpoint_search<IT, K_TB>(r, rounds);
     }
 }
 
 // ---------------------------------------------------------------------------
 // block writers (BC1Encoder.cpp:345-441, BC1Block.h:66-80)
 // ---------------------------------------------------------------------------
-template <int IT>
-__device__ __forceinline__ uint2 write_block_solid(int cr, int cg, int cb, int color_mode) {
+template <int IT> __device__ __forceinline__ uint2 write_block_solid(uint32_t c) {
+    const int cr = c & 0xFF, cg = (c >> 8) & 0xFF, cb = (c >> 16) & 0xFF;
     uint32_t mask = 0xAA;
     int mn, mx;
     if ((cr | cg | cb) == 0) {
@@ -784,9 +891,8 @@ __device__ __forceinline__ uint2 write_block_solid(int cr, int cg, int cb, int c
         // FindEndpointsSingleColor(color); the 3-colour tables equal the 4-colour
         // ones (SingleColorTable.h: N unused), so the 3-colour trial never wins.
         const uint32_t mr = g_tab.match5[IT][cr], mg = g_tab.match6[IT][cg], mb = g_tab.match5[IT][cb];
-        const int lo = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
-        const int hi = eppack(mr & 0xFF, mg & 0xFF, mb & 0xFF);
-        mn = lo; mx = hi;
+        mn = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
+        mx = eppack(mr & 0xFF, mg & 0xFF, mb & 0xFF);
         if (mn == mx) {
             if (mn > 0) { mn--; mask = 0; }
             else { mx = 1; mn = 0; mask = 0x55; }
@@ -794,7 +900,6 @@ __device__ __forceinline__ uint2 write_block_solid(int cr, int cg, int cb, int c
             const int t = mn; mn = mx; mx = t;
             mask = 0xFF;
         }
-        (void)color_mode;
     }
     return make_uint2((uint32_t)mx | ((uint32_t)mn << 16), mask * 0x01010101u);
 }
@@ -825,75 +930,93 @@ __device__ __forceinline__ uint2 write_block(const Res &r) {
 }
 
 // ---------------------------------------------------------------------------
-// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342) for one group
+// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342) for the group's block
 // ---------------------------------------------------------------------------
-template <int IT>
-__device__ uint2 encode_bc1_group(const Ctx &C, const qt_bc1_params &p) {
-    const uint32_t own = C.spx[C.lane];
-    if (__all_sync(C.gm, own == C.spx[0])) return write_block_solid<IT>(C.pr, C.pg, C.pb, p.color_mode);
+template <int IT> __device__ __forceinline__ uint2 encode_bc1_group(const Grp &G, const qt_bc1_params &p) {
+    if (__all_sync(G.gm, s_px[G.g][G.lane] == s_px[G.g][0])) return write_block_solid<IT>(s_px[G.g][0]);
 
-    const Metrics m = get_metrics(C, false);
+    get_metrics(0, false);
+    const bool has_black = s_met[G.g][0][MT_BLACK] != 0;
     const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
     bool needs_err = use_likely;
     needs_err |= p.color_mode == CM_THREE;
-    needs_err |= (p.color_mode == CM_TB) && m.has_black;
+    needs_err |= (p.color_mode == CM_TB) && has_black;
     needs_err |= p.error_mode != EM_NONE;
     needs_err |= p.search_rounds > 0;
     const int em = needs_err ? p.error_mode : EM_NONE;
     const int ls_passes = p.two_ls_passes ? 2 : 1, cf_passes = p.two_cf_passes ? 2 : 1;
     const int ep_passes = (needs_err && p.two_ep_passes) ? 2 : 1;
+    const int k4 = kind_for(CM_FOUR, em);
 
     Res orig = res_init(), res = res_init();
     for (int round = 0; round < ep_passes; round++) {
-        const int mode = round == 1 ? EP_BB : p.endpoint_mode;
+        const int2 ep = find_endpoints(round == 1 ? EP_BB : p.endpoint_mode, false, (int)p.power_iterations, 0);
         Res to = res_init();
-        find_endpoints<IT>(C, to, m, mode, false, (int)p.power_iterations);
+        to.lo = ep.x;
+        to.hi = ep.y;
         Res tr = to;
-        find_selectors_tp<IT>(C, CM_FOUR, em, tr);
-        refine_block_ls<IT>(C, CM_FOUR, tr, m, em, ls_passes);
+        const SelErr se = fs_any<IT>(k4, tr.lo, tr.hi);
+        tr.sel = se.sel;
+        tr.err = se.err;
+        tr.mode = CM_FOUR;
+        tr = refine_ls_any<IT>(k4, tr, ls_passes, 0);
         if (!needs_err || tr.err < res.err) {
             res = tr;
             orig = to;
         }
     }
     if (res.err > 0 && use_likely)
-        for (int it = 0; it < cf_passes; it++) refine_block_cf<IT>(C, CM_FOUR, res, m, p.error_mode, p.orderings4, p.exhaustive);
+        for (int it = 0; it < cf_passes; it++) res = refine_cf_any<IT>(kind_for(CM_FOUR, p.error_mode), res, p.orderings4, p.exhaustive, 0);
 
     if (res.err > 0 && (p.color_mode & CM_THREE)) {
         Res t = orig;
-        find_selectors_tp<IT>(C, CM_THREE, EM_FULL, t);
-        refine_block_ls<IT>(C, CM_THREE, t, m, EM_FULL, ls_passes);
+        const SelErr se = fs_tp<IT, K_T3>(t.lo, t.hi);
+        t.sel = se.sel;
+        t.err = se.err;
+        t.mode = CM_THREE;
+        t = refine_ls<IT, K_T3>(t, ls_passes, 0);
         if (t.err > 0 && use_likely)
-            for (int it = 0; it < cf_passes; it++) refine_block_cf<IT>(C, CM_THREE, t, m, EM_FULL, p.orderings3, p.exhaustive);
+            for (int it = 0; it < cf_passes; it++) t = refine_cf<IT, K_T3>(t, p.orderings3, p.exhaustive, 0);
         if (t.err < res.err) res = t;
     }
 
-    if (res.err > 0 && p.color_mode == CM_TB && m.has_black && !((m.mx[0] | m.mx[1] | m.mx[2]) < 4)) {
-        Res t = res_init();
-        const Metrics mnb = get_metrics(C, true);
-        find_endpoints<IT>(C, t, mnb, EP_PCA, true, (int)p.power_iterations);
-        find_selectors_tp<IT>(C, CM_TB, EM_FULL, t);
-        refine_block_ls<IT>(C, CM_TB, t, mnb, EM_FULL, ls_passes);
-        if (t.err < res.err) res = t;
+    if (res.err > 0 && p.color_mode == CM_TB && has_black) {
+        const int *M0 = s_met[G.g][0];
+        if (!((M0[MT_MX] | M0[MT_MX + 1] | M0[MT_MX + 2]) < 4)) {
+            get_metrics(1, true);
+            const int2 ep = find_endpoints(EP_PCA, true, (int)p.power_iterations, 1);
+            Res t = res_init();
+            t.lo = ep.x;
+            t.hi = ep.y;
+            const SelErr se = fs_tp<IT, K_TB>(t.lo, t.hi);
+            t.sel = se.sel;
+            t.err = se.err;
+            t.mode = CM_TB;
+            t = refine_ls<IT, K_TB>(t, ls_passes, 1);
+            if (t.err < res.err) res = t;
+        }
     }
 
-    if (res.err > 0 && p.search_rounds > 0) endpoint_search<IT>(C, res, p.error_mode, p.search_rounds);
+    if (res.err > 0 && p.search_rounds > 0) {
+        const int M = res.mode == CM_THREE ? CM_THREE : (res.mode == CM_TB ? CM_TB : CM_FOUR);
+        res = endpoint_search_any<IT>(kind_for(M, M == CM_FOUR ? p.error_mode : EM_FULL), res, p.search_rounds);
+    }
     return write_block(res);
 }
 
-// BC4Encoder::EncodeBlock (BC4Encoder.cpp:30-71) for one group; returns the 8 bytes
-__device__ __forceinline__ uint2 encode_bc4_group(const Ctx &C, int ch) {
-    const int v = ch == 0 ? C.pr : (ch == 1 ? C.pg : (ch == 2 ? C.pb : C.pa));
-    const int mn = (int)gmin(C.gm, (unsigned)v), mx = (int)gmax(C.gm, (unsigned)v);
+// BC4Encoder::EncodeBlock (BC4Encoder.cpp:30-71) for the group's block; returns the 8 bytes
+__device__ __forceinline__ uint2 encode_bc4_group(const Grp &G, int ch) {
+    const int v = (int)((s_px[G.g][G.lane] >> (8 * ch)) & 0xFF);
+    const int mn = (int)gmin(G.gm, (unsigned)v), mx = (int)gmax(G.gm, (unsigned)v);
     if (mn == mx) return make_uint2((uint32_t)mn | ((uint32_t)mn << 8), 0u);
     const int bias = 4 - mn * 14, delta = mx - mn, x = v * 14;
     int lvl = 0;
 #pragma unroll
     for (int c = 0; c < 7; c++) lvl += x >= delta * (1 + 2 * c) - bias;
     const uint32_t s = (kBC4Levels >> (3 * lvl)) & 7u;
-    const int bit = 3 * C.lane;
-    const uint32_t lo = gor(C.gm, bit < 32 ? s << bit : 0u);
-    const uint32_t hi = gor(C.gm, bit >= 32 ? s << (bit - 32) : (bit + 3 > 32 ? s >> (32 - bit) : 0u));
+    const int bit = 3 * G.lane;
+    const uint32_t lo = gor(G.gm, bit < 32 ? s << bit : 0u);
+    const uint32_t hi = gor(G.gm, bit >= 32 ? s << (bit - 32) : (bit + 3 > 32 ? s >> (32 - bit) : 0u));
     // bytes: a0=max, a1=min, then 48 selector bits little endian
     return make_uint2((uint32_t)mx | ((uint32_t)mn << 8) | (lo << 16), (lo >> 16) | (hi << 16));
 }
@@ -902,50 +1025,35 @@ __device__ __forceinline__ uint2 encode_bc4_group(const Ctx &C, int ch) {
 // BC1 / BC3 encode kernel: one block per 16-lane group, grid-stride
 // ---------------------------------------------------------------------------
 template <int IT>
-__global__ void __launch_bounds__(128) k_bc1_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long nblocks,
-                                                    qt_bc1_params p, uint8_t *__restrict__ out, int bc3) {
-    __shared__ float s_mid5[32], s_mid6[64];
-    __shared__ uint16_t s_vox[16];
-    __shared__ uint32_t s_px[kGroupsPerCta][16];
-    __shared__ int s_sum[kGroupsPerCta][51];
+__global__ void __launch_bounds__(128, 4) k_bc1_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long nblocks,
+                                                       qt_bc1_params p, uint8_t *__restrict__ out, int bc3) {
     for (int i = threadIdx.x; i < 64; i += blockDim.x) {
         if (i < 32) s_mid5[i] = c_mid5[i];
         s_mid6[i] = c_mid6[i];
         if (i < 16) s_vox[i] = c_voxels[i];
     }
     __syncthreads();
-
-    const int grp = threadIdx.x >> 4;
-    Ctx C;
-    C.lane = threadIdx.x & 15;
-    C.gm = 0xFFFFu << (threadIdx.x & 16);
-    C.spx = s_px[grp];
-    C.ssum = s_sum[grp];
-    C.mid5 = s_mid5;
-    C.mid6 = s_mid6;
-    C.vox = s_vox;
+    const Grp G = grp();
     if (bc3) p.color_mode = CM_FOUR;  // BC3Encoder.h:39-40
 
-    for (long b = (long)blockIdx.x * kGroupsPerCta + grp; b < nblocks; b += (long)gridDim.x * kGroupsPerCta) {
+    for (long b = (long)blockIdx.x * kGroupsPerCta + G.g; b < nblocks; b += (long)gridDim.x * kGroupsPerCta) {
         const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
-        int sx = bx * 4 + (C.lane & 3), sy = by * 4 + (C.lane >> 2);
+        int sx = bx * 4 + (G.lane & 3), sy = by * 4 + (G.lane >> 2);
         if (sx >= w) sx %= w;  // RawTexture::GetBlock wraps at the edges (Texture.h:105-108)
         if (sy >= h) sy %= h;
         const uint32_t v = *reinterpret_cast<const uint32_t *>(rgba + ((size_t)sy * w + sx) * 4);
-        C.spx[C.lane] = v;
-        C.pr = v & 0xFF;
-        C.pg = (v >> 8) & 0xFF;
-        C.pb = (v >> 16) & 0xFF;
-        C.pa = v >> 24;
-        __syncwarp(C.gm);
-        const uint2 blk = encode_bc1_group<IT>(C, p);
+        const float fr = (float)(v & 0xFF), fg = (float)((v >> 8) & 0xFF), fb = (float)((v >> 16) & 0xFF);
+        s_px[G.g][G.lane] = v;
+        s_pf[G.g][G.lane] = make_float4(fr, fg, fb, fr * fr + fg * fg + fb * fb);
+        __syncwarp(G.gm);
+        const uint2 blk = encode_bc1_group<IT>(G, p);
         if (bc3) {
-            const uint2 a = encode_bc4_group(C, 3);
-            if (C.lane == 0) reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
-        } else if (C.lane == 0) {
+            const uint2 a = encode_bc4_group(G, 3);
+            if (G.lane == 0) reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
+        } else if (G.lane == 0) {
             reinterpret_cast<uint2 *>(out)[b] = blk;
         }
-        __syncwarp(C.gm);
+        __syncwarp(G.gm);
     }
 }
 
