@@ -352,15 +352,21 @@ template <int IT, int K> __device__ __forceinline__ float block_err(const float4
         const float r2 = -2.0f * P.r2, g2 = -2.0f * P.g2, b2 = -2.0f * P.b2;
         const float r3 = -2.0f * P.r3, g3 = -2.0f * P.g3, b3 = -2.0f * P.b3;
         float t0 = 0.0f, t1 = 0.0f;  // two accumulators: shorter dependency chain, still exact
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const float4 p = pf[i];
+#pragma unroll 2
+        for (int i = 0; i < 16; i += 2) {
+            const float4 p = pf[i], q = pf[i + 1];
             float m = fmaf(p.z, b0, fmaf(p.y, g0, fmaf(p.x, r0, v0)));
+            float n = fmaf(q.z, b0, fmaf(q.y, g0, fmaf(q.x, r0, v0)));
             m = fminf(m, fmaf(p.z, b1, fmaf(p.y, g1, fmaf(p.x, r1, v1))));
+            n = fminf(n, fmaf(q.z, b1, fmaf(q.y, g1, fmaf(q.x, r1, v1))));
             m = fminf(m, fmaf(p.z, b2, fmaf(p.y, g2, fmaf(p.x, r2, v2))));
-            if (K != K_T3) m = fminf(m, fmaf(p.z, b3, fmaf(p.y, g3, fmaf(p.x, r3, v3))));
-            if (i & 1) t1 += p.w + m;
-            else t0 += p.w + m;
+            n = fminf(n, fmaf(q.z, b2, fmaf(q.y, g2, fmaf(q.x, r2, v2))));
+            if (K != K_T3) {
+                m = fminf(m, fmaf(p.z, b3, fmaf(p.y, g3, fmaf(p.x, r3, v3))));
+                n = fminf(n, fmaf(q.z, b3, fmaf(q.y, g3, fmaf(q.x, r3, v3))));
+            }
+            t0 += p.w + m;
+            t1 += q.w + n;
         }
         tot = t0 + t1;
     } else if (K == K_F4_FASTER) {
@@ -369,7 +375,7 @@ template <int IT, int K> __device__ __forceinline__ float block_err(const float4
         const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
         const float t0 = (float)(d0 + d1), t1 = (float)(d1 + d2), t2 = (float)(d2 + d3);
         const float a2r = 2.0f * ar, a2g = 2.0f * ag, a2b = 2.0f * ab;
-#pragma unroll
+#pragma unroll 4
         for (int i = 0; i < 16; i++) {
             const float4 p = pf[i];
             const float dot = fmaf(p.z, a2b, fmaf(p.y, a2g, p.x * a2r));
@@ -384,7 +390,7 @@ template <int IT, int K> __device__ __forceinline__ float block_err(const float4
         const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
         const float far_ = (float)ar, fag = (float)ag, fab = (float)ab;
         const float c0r = (float)P.r0, c0g = (float)P.g0, c0b = (float)P.b0;
-#pragma unroll
+#pragma unroll 4
         for (int i = 0; i < 16; i++) {
             const float4 p = pf[i];
             const float dd = fmaf(p.z - c0b, fab, fmaf(p.y - c0g, fag, (p.x - c0r) * far_));
@@ -706,7 +712,7 @@ template <int IT, int K> __device__ __noinline__ Res refine_cf(Res r, unsigned o
 #pragma unroll
     for (int i = 0; i < 16; i++) rank += __shfl_sync(G.gm, key, i, 16) < key;
     int sr = 0, sg = 0, sb = 0;  // sum of the texels ranked at or below this lane's position
-#pragma unroll
+#pragma unroll 4
     for (int j = 0; j < 16; j++) {
         if (__shfl_sync(G.gm, rank, j, 16) <= G.lane) {
             const uint32_t u = s_px[G.g][j];
@@ -1025,7 +1031,7 @@ __device__ __forceinline__ uint2 encode_bc4_group(const Grp &G, int ch) {
 // BC1 / BC3 encode kernel: one block per 16-lane group, grid-stride
 // ---------------------------------------------------------------------------
 template <int IT>
-__global__ void __launch_bounds__(128, 4) k_bc1_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long nblocks,
+__global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long nblocks,
                                                        qt_bc1_params p, uint8_t *__restrict__ out, int bc3) {
     for (int i = threadIdx.x; i < 64; i += blockDim.x) {
         if (i < 32) s_mid5[i] = c_mid5[i];
