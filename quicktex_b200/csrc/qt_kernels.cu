@@ -190,6 +190,7 @@ __shared__ float4 s_pf[kGroupsPerCta][16];        // (r, g, b, r^2+g^2+b^2) as e
 __shared__ int s_sum[kGroupsPerCta][17 * 3];       // cluster-fit prefix sums
 __shared__ uint16_t s_row[kGroupsPerCta][128];     // BestOrders row of the current cluster fit
 __shared__ int s_met[kGroupsPerCta][2][16];        // metrics: [0] all texels, [1] ignoring black
+__shared__ int s_pp[kGroupsPerCta];                // sum over the block of r^2 + g^2 + b^2
 
 // metric slots
 constexpr int MT_MN = 0, MT_MX = 3, MT_AV = 6, MT_SUM = 9, MT_GREY = 12, MT_BLACK = 13;
@@ -344,31 +345,30 @@ template <int IT, int K> __device__ __forceinline__ float block_err(const float4
     const Pal P = make_pal<IT>(lo, hi, kind_three(K));
     float tot = 0.0f;
     if (K == K_F4_FULL || K == K_T3 || K == K_TB) {
-        // sum_t min_j |p_t - c_j|^2 = sum_t (|p_t|^2 + min_j (|c_j|^2 - 2 p_t.c_j)); every term is an exact integer
-        const float v0 = (float)sq3(P.r0, P.g0, P.b0), v1 = (float)sq3(P.r1, P.g1, P.b1);
-        const float v2 = (float)sq3(P.r2, P.g2, P.b2), v3 = (float)sq3(P.r3, P.g3, P.b3);
-        const float r0 = -2.0f * P.r0, g0 = -2.0f * P.g0, b0 = -2.0f * P.b0;
-        const float r1 = -2.0f * P.r1, g1 = -2.0f * P.g1, b1 = -2.0f * P.b1;
-        const float r2 = -2.0f * P.r2, g2 = -2.0f * P.g2, b2 = -2.0f * P.b2;
-        const float r3 = -2.0f * P.r3, g3 = -2.0f * P.g3, b3 = -2.0f * P.b3;
-        float t0 = 0.0f, t1 = 0.0f;  // two accumulators: shorter dependency chain, still exact
+        // sum_t min_j |p_t - c_j|^2 = sum_t |p_t|^2 + sum_t min_j (|c_j|^2 - 2 p_t.c_j), in exact integers:
+        // p.c by one dp4a on the packed texel (the colour's alpha byte is 0), the first sum is per block
+        const uint32_t *px = s_px[grp().g];
+        const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
+        const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
+        const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
+        const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
+        int t0 = 0, t1 = 0;
 #pragma unroll 2
         for (int i = 0; i < 16; i += 2) {
-            const float4 p = pf[i], q = pf[i + 1];
-            float m = fmaf(p.z, b0, fmaf(p.y, g0, fmaf(p.x, r0, v0)));
-            float n = fmaf(q.z, b0, fmaf(q.y, g0, fmaf(q.x, r0, v0)));
-            m = fminf(m, fmaf(p.z, b1, fmaf(p.y, g1, fmaf(p.x, r1, v1))));
-            n = fminf(n, fmaf(q.z, b1, fmaf(q.y, g1, fmaf(q.x, r1, v1))));
-            m = fminf(m, fmaf(p.z, b2, fmaf(p.y, g2, fmaf(p.x, r2, v2))));
-            n = fminf(n, fmaf(q.z, b2, fmaf(q.y, g2, fmaf(q.x, r2, v2))));
+            const uint32_t u = px[i], q = px[i + 1];
+            int m = v0 - 2 * (int)__dp4a(u, c0, 0u), n = v0 - 2 * (int)__dp4a(q, c0, 0u);
+            m = min(m, v1 - 2 * (int)__dp4a(u, c1, 0u));
+            n = min(n, v1 - 2 * (int)__dp4a(q, c1, 0u));
+            m = min(m, v2 - 2 * (int)__dp4a(u, c2, 0u));
+            n = min(n, v2 - 2 * (int)__dp4a(q, c2, 0u));
             if (K != K_T3) {
-                m = fminf(m, fmaf(p.z, b3, fmaf(p.y, g3, fmaf(p.x, r3, v3))));
-                n = fminf(n, fmaf(q.z, b3, fmaf(q.y, g3, fmaf(q.x, r3, v3))));
+                m = min(m, v3 - 2 * (int)__dp4a(u, c3, 0u));
+                n = min(n, v3 - 2 * (int)__dp4a(q, c3, 0u));
             }
-            t0 += p.w + m;
-            t1 += q.w + n;
+            t0 += m;
+            t1 += n;
         }
-        tot = t0 + t1;
+        tot = (float)(s_pp[grp().g] + t0 + t1);
     } else if (K == K_F4_FASTER) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
         const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
@@ -1051,6 +1051,8 @@ __global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict
         const float fr = (float)(v & 0xFF), fg = (float)((v >> 8) & 0xFF), fb = (float)((v >> 16) & 0xFF);
         s_px[G.g][G.lane] = v;
         s_pf[G.g][G.lane] = make_float4(fr, fg, fb, fr * fr + fg * fg + fb * fb);
+        const unsigned pp = gsum(G.gm, sq3((int)(v & 0xFF), (int)((v >> 8) & 0xFF), (int)((v >> 16) & 0xFF)));
+        if (G.lane == 0) s_pp[G.g] = (int)pp;
         __syncwarp(G.gm);
         const uint2 blk = encode_bc1_group<IT>(G, p);
         if (bc3) {
