@@ -139,6 +139,52 @@ int qt_bc5_decode_host(const uint8_t *blocks, int width, int height, int chan0, 
 int qt_bc5_decode_device(const uint8_t *blocks, int width, int height, int chan0, int chan1, uint8_t *rgba,
                          void *stream);
 
+/* ---- batched persistent path (no reference counterpart: the reference runs one
+ * texture per Encode/Decode call, Encoder.h:36-56 / Decoder.h:36-54) ----
+ *
+ * Many textures of any size, format and level in one launch: every texture is
+ * cut into tiles of consecutive blocks (tile size per format/level from a tuning
+ * table), the tiles are queued heaviest-first in device memory, and one
+ * persistent kernel, replayed from a captured CUDA graph, pulls tiles until the
+ * queue is empty. Each texture's output is byte-identical to the single-texture
+ * entry points above. */
+#define QT_OP_ENCODE 0
+#define QT_OP_DECODE 1
+
+typedef struct qt_batch qt_batch;
+
+typedef struct qt_batch_item {
+    int32_t op;            /* QT_OP_ENCODE or QT_OP_DECODE */
+    int32_t format;        /* 1 = BC1, 3 = BC3, 4 = BC4, 5 = BC5 */
+    int32_t width, height; /* texture size in texels */
+    const uint8_t *src;    /* device: RGBA8 texels (encode) or blocks (decode) */
+    uint8_t *dst;          /* device: blocks (encode) or RGBA8 texels (decode) */
+    qt_bc1_params params;  /* BC1/BC3 encode settings */
+    int32_t chan0, chan1;  /* BC4 (chan0) / BC5 channels */
+    int32_t interpolator;  /* BC1/BC3 decode */
+    int32_t write_alpha;   /* BC1 decode */
+} qt_batch_item;
+
+/* Tuning rule: tiles of `tile_blocks` blocks and a relative cost per block for
+ * (op, format, level); level is ignored for BC4/BC5 and decodes (-1). */
+typedef struct qt_tile_rule {
+    int32_t op, format, level;
+    uint32_t tile_blocks;
+    float cost_per_block;
+} qt_tile_rule;
+
+int qt_batch_create(int device, qt_batch **out);
+int qt_batch_destroy(qt_batch *b);
+/* Replace the tuning rules (rules not given keep their defaults). */
+int qt_batch_set_rules(qt_batch *b, const qt_tile_rule *rules, size_t n);
+/* Persistent grid size in CTAs per SM (0 = the kernel's occupancy limit). */
+int qt_batch_set_grid(qt_batch *b, int ctas_per_sm);
+/* Enqueue one persistent launch over all items on `stream` (device buffers; the
+ * call returns once the work is queued). */
+int qt_batch_run(qt_batch *b, const qt_batch_item *items, size_t n, void *stream);
+/* Number of tiles the last qt_batch_run queued. */
+size_t qt_batch_last_tiles(const qt_batch *b);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,259 @@
+"""Batched persistent encode/decode (C-ABI ``qt_batch_*``).
+
+Many textures of uneven sizes, formats (BC1/BC3/BC4/BC5), operations
+(encode/decode) and levels run as ONE persistent kernel launch replayed from a
+CUDA graph: each texture is cut into tiles of consecutive blocks, the tiles are
+queued heaviest-first in device memory, and 16-lane groups pull tiles until the
+queue is empty. Tile sizes and per-block costs per (op, format, level) come from
+the tuning table written by ``quicktex_b200.autotune`` (``data/batch_tuning.json``).
+
+Every output is byte-identical to the single-texture entry points: the batch
+changes only the launch model.
+
+    jobs = [Job.encode("bc1", rgba, w, h, level=18), Job.decode("bc4", blocks, w, h, channel=0), ...]
+    outs = run_jobs(jobs)            # list of bytes, one per job
+"""
+
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import json
+import os
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import capi
+
+QT_OP_ENCODE, QT_OP_DECODE = 0, 1
+FORMATS = {"bc1": 1, "bc3": 3, "bc4": 4, "bc5": 5}
+BLOCK_BYTES = {1: 8, 3: 16, 4: 8, 5: 16}
+TUNING_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data", "batch_tuning.json")
+
+
+class BatchItem(ctypes.Structure):
+    """``qt_batch_item``."""
+
+    _fields_ = [
+        ("op", ctypes.c_int32), ("format", ctypes.c_int32), ("width", ctypes.c_int32), ("height", ctypes.c_int32),
+        ("src", ctypes.c_void_p), ("dst", ctypes.c_void_p), ("params", capi.BC1Params),
+        ("chan0", ctypes.c_int32), ("chan1", ctypes.c_int32), ("interpolator", ctypes.c_int32),
+        ("write_alpha", ctypes.c_int32),
+    ]
+
+
+class TileRule(ctypes.Structure):
+    """``qt_tile_rule``."""
+
+    _fields_ = [("op", ctypes.c_int32), ("format", ctypes.c_int32), ("level", ctypes.c_int32),
+                ("tile_blocks", ctypes.c_uint32), ("cost_per_block", ctypes.c_float)]
+
+
+_sigs_done = False
+
+
+def _lib():
+    global _sigs_done
+    L = capi.lib()
+    if not _sigs_done:
+        L.qt_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)]
+        L.qt_batch_destroy.argtypes = [ctypes.c_void_p]
+        L.qt_batch_set_rules.argtypes = [ctypes.c_void_p, ctypes.POINTER(TileRule), ctypes.c_size_t]
+        L.qt_batch_set_grid.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.qt_batch_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_size_t, ctypes.c_void_p]
+        L.qt_batch_last_tiles.argtypes = [ctypes.c_void_p]
+        L.qt_batch_last_tiles.restype = ctypes.c_size_t
+        for n in ("qt_batch_create", "qt_batch_destroy", "qt_batch_set_rules", "qt_batch_set_grid", "qt_batch_run"):
+            getattr(L, n).restype = ctypes.c_int
+        _sigs_done = True
+    return L
+
+
+def load_tuning(path: str = TUNING_PATH) -> Optional[dict]:
+    try:
+        with open(path) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return None
+
+
+class Batch:
+    """One batch queue (device buffers + captured graph) on one device."""
+
+    def __init__(self, device: int = 0, tuning: Optional[dict] = None, use_default_tuning: bool = True):
+        self.device = device
+        h = ctypes.c_void_p()
+        capi.check(_lib().qt_batch_create(device, ctypes.byref(h)))
+        self.handle = h
+        if tuning is None and use_default_tuning:
+            tuning = load_tuning()
+        if tuning:
+            self.apply_tuning(tuning)
+
+    def apply_tuning(self, tuning: dict) -> None:
+        rules = tuning.get("rules", [])
+        self.set_rules(rules)
+        if tuning.get("ctas_per_sm"):
+            self.set_grid(int(tuning["ctas_per_sm"]))
+
+    def set_rules(self, rules: Sequence[dict]) -> None:
+        arr = (TileRule * max(1, len(rules)))()
+        for i, r in enumerate(rules):
+            arr[i] = TileRule(r["op"], r["format"], r.get("level", -1), r["tile_blocks"], r["cost_per_block"])
+        capi.check(_lib().qt_batch_set_rules(self.handle, arr, len(rules)))
+
+    def set_grid(self, ctas_per_sm: int) -> None:
+        capi.check(_lib().qt_batch_set_grid(self.handle, ctas_per_sm))
+
+    def run(self, items: Sequence[BatchItem], stream: int = 0) -> None:
+        arr = (BatchItem * max(1, len(items)))(*items)
+        capi.check(_lib().qt_batch_run(self.handle, arr, len(items), ctypes.c_void_p(stream)))
+
+    def last_tiles(self) -> int:
+        return int(_lib().qt_batch_last_tiles(self.handle))
+
+    def close(self) -> None:
+        if self.handle:
+            _lib().qt_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclasses.dataclass
+class Job:
+    """One texture to encode or decode."""
+
+    op: int
+    fmt: int
+    width: int
+    height: int
+    data: np.ndarray  # RGBA8 texels (encode) or blocks (decode), uint8
+    params: Optional[capi.BC1Params] = None
+    chan0: int = 0
+    chan1: int = 1
+    interpolator: int = 0
+    write_alpha: bool = False
+
+    @staticmethod
+    def encode(fmt: str, rgba, width: int, height: int, level: int = 5, color_mode: int = capi.FOUR_COLOR,
+               interpolator: int = 0, channel: int = 3, chan0: int = 0, chan1: int = 1, params=None) -> "Job":
+        f = FORMATS[fmt]
+        if f in (1, 3) and params is None:
+            params = capi.params_for_level(level, color_mode if f == 1 else capi.FOUR_COLOR, interpolator)
+        c0, c1 = (channel, channel) if f == 4 else (chan0, chan1)
+        return Job(QT_OP_ENCODE, f, width, height, np.ascontiguousarray(rgba, np.uint8).reshape(-1), params, c0, c1)
+
+    @staticmethod
+    def decode(fmt: str, blocks, width: int, height: int, interpolator: int = 0, write_alpha: bool = False,
+               channel: int = 3, chan0: int = 0, chan1: int = 1) -> "Job":
+        f = FORMATS[fmt]
+        c0, c1 = (channel, channel) if f == 4 else (chan0, chan1)
+        data = np.frombuffer(bytes(blocks), np.uint8) if not isinstance(blocks, np.ndarray) else blocks.reshape(-1)
+        return Job(QT_OP_DECODE, f, width, height, data, None, c0, c1, interpolator, write_alpha)
+
+    @property
+    def nblocks(self) -> int:
+        return ((self.width + 3) // 4) * ((self.height + 3) // 4)
+
+    @property
+    def out_bytes(self) -> int:
+        return self.nblocks * BLOCK_BYTES[self.fmt] if self.op == QT_OP_ENCODE else self.width * self.height * 4
+
+    def item(self, src: int, dst: int) -> BatchItem:
+        it = BatchItem()
+        it.op, it.format, it.width, it.height = self.op, self.fmt, self.width, self.height
+        it.src, it.dst = src, dst
+        if self.params is not None:
+            it.params = self.params
+        it.chan0, it.chan1, it.interpolator, it.write_alpha = self.chan0, self.chan1, self.interpolator, int(self.write_alpha)
+        return it
+
+
+def _align(n: int, a: int = 256) -> int:
+    return (n + a - 1) // a * a
+
+
+class Arena:
+    """All jobs' inputs packed into one device buffer (and outputs into another),
+    filled from one pinned host buffer: one upload and one download per batch."""
+
+    def __init__(self, jobs: Sequence[Job], device: int = 0):
+        import torch
+
+        self.jobs = list(jobs)
+        self.in_off, self.out_off = [], []
+        ni = no = 0
+        for j in self.jobs:
+            self.in_off.append(ni)
+            self.out_off.append(no)
+            ni += _align(j.data.nbytes)
+            no += _align(j.out_bytes)
+        self.in_bytes, self.out_bytes = ni, no
+        dev = torch.device("cuda", device)
+        self.h_in = torch.empty(max(ni, 1), dtype=torch.uint8).pin_memory()
+        self.h_out = torch.empty(max(no, 1), dtype=torch.uint8).pin_memory()
+        hin = self.h_in.numpy()
+        for j, o in zip(self.jobs, self.in_off):
+            hin[o:o + j.data.nbytes] = j.data
+        self.d_in = torch.empty(max(ni, 1), dtype=torch.uint8, device=dev)
+        self.d_out = torch.empty(max(no, 1), dtype=torch.uint8, device=dev)
+
+    def upload(self, stream=None):
+        self.d_in.copy_(self.h_in, non_blocking=True)
+
+    def download(self):
+        self.h_out.copy_(self.d_out, non_blocking=True)
+
+    def items(self) -> list[BatchItem]:
+        bi, bo = self.d_in.data_ptr(), self.d_out.data_ptr()
+        return [j.item(bi + a, bo + b) for j, a, b in zip(self.jobs, self.in_off, self.out_off)]
+
+    def outputs(self) -> list[bytes]:
+        ho = self.h_out.numpy()
+        return [ho[o:o + j.out_bytes].tobytes() for j, o in zip(self.jobs, self.out_off)]
+
+
+def run_plain(items: Sequence[BatchItem], stream: int = 0) -> None:
+    """The same work with one launch per texture through the single-texture
+    device entry points (the launch model the batch replaces)."""
+    for it in items:
+        f, p = it.format, ctypes.byref(it.params)
+        src, dst, w, h, s = ctypes.c_void_p(it.src), ctypes.c_void_p(it.dst), it.width, it.height, ctypes.c_void_p(stream)
+        L = capi.lib()
+        if it.op == QT_OP_ENCODE:
+            rc = (L.qt_bc1_encode_device(src, w, h, p, dst, s) if f == 1 else
+                  L.qt_bc3_encode_device(src, w, h, p, dst, s) if f == 3 else
+                  L.qt_bc4_encode_device(src, w, h, it.chan0, dst, s) if f == 4 else
+                  L.qt_bc5_encode_device(src, w, h, it.chan0, it.chan1, dst, s))
+        else:
+            rc = (L.qt_bc1_decode_device(src, w, h, it.interpolator, it.write_alpha, dst, s) if f == 1 else
+                  L.qt_bc3_decode_device(src, w, h, it.interpolator, dst, s) if f == 3 else
+                  L.qt_bc4_decode_device(src, w, h, it.chan0, dst, s) if f == 4 else
+                  L.qt_bc5_decode_device(src, w, h, it.chan0, it.chan1, dst, s))
+        capi.check(rc)
+
+
+def run_jobs(jobs: Sequence[Job], device: int = 0, batch: Optional[Batch] = None) -> list[bytes]:
+    """Upload, one persistent launch, download; returns each job's output bytes."""
+    import torch
+
+    torch.cuda.set_device(device)
+    arena = Arena(jobs, device)
+    stream = torch.cuda.current_stream()
+    arena.upload()
+    own = batch is None
+    b = batch or Batch(device)
+    try:
+        b.run(arena.items(), stream.cuda_stream)
+        arena.download()
+        stream.synchronize()
+    finally:
+        if own:
+            b.close()
+    return arena.outputs()

@@ -342,6 +342,11 @@ const HostTables &host_tables() {
     static const HostTables *t = make_tables();
     return *t;
 }
+
+int set_error(int code, const char *msg) { return set_err(code, "%s", msg); }
+int cuda_error(int e, const char *what) { return cuda_err((cudaError_t)e, what); }
+int ensure_current_device(int *dev) { return ensure_device(dev); }
+int check_bc1_params(const qt_bc1_params *p, bool bc3) { return check_params(p, bc3); }
 }  // namespace qtk
 
 // ===========================================================================

@@ -23,9 +23,34 @@ struct alignas(16) HostTables {
     uint32_t match6[4][256];
 };
 
+// Device descriptor of one texture of a batch (built from qt_batch_item).
+struct BatchItemDev {
+    const uint8_t *src;
+    uint8_t *dst;
+    int32_t w, h, bw, bh;
+    int32_t op;           // QT_OP_ENCODE / QT_OP_DECODE
+    int32_t fmt;          // 1, 3, 4, 5
+    int32_t c0, c1;       // BC4/BC5 channels
+    int32_t interp;       // decode interpolator
+    int32_t write_alpha;  // BC1 decode
+    qt_bc1_params p;      // BC1/BC3 encode settings
+};
+
+// One unit of the device work queue: `count` consecutive blocks of item `item`.
+struct TileDev {
+    uint32_t item, start, count, pad;
+};
+
 // Builds the tables on the host (the factor matrices with the reference's
 // float operation order) from the embedded ordering-table blob.
 const HostTables &host_tables();
+
+// Shared host helpers (qt_capi.cpp): thread-local error message, status codes,
+// per-device table upload on the current device, argument checks.
+int set_error(int code, const char *msg);
+int cuda_error(int cuda_status, const char *what);
+int ensure_current_device(int *dev);
+int check_bc1_params(const qt_bc1_params *p, bool bc3);
 
 // Kernel-side entry points (qt_kernels.cu). Each returns a cudaError_t value
 // cast to int (0 on success). All pointers are device pointers.
@@ -37,5 +62,11 @@ int launch_bc4_encode(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc
 // fmt: 1 = BC1, 3 = BC3, 4 = BC4, 5 = BC5
 int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
                   uint8_t *rgba, void *stream);
+
+// Persistent batch kernel: groups pull tiles from tiles[0 .. ctl[1]) through the
+// counter ctl[0] until the queue is empty. grid = CTAs to launch (0 = one wave).
+int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, void *stream);
+int batch_ctas_per_sm();
+int batch_sms();
 
 }  // namespace qtk

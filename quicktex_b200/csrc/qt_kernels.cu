@@ -1232,18 +1232,129 @@ __global__ void __launch_bounds__(256) k_decode(const uint8_t *__restrict__ bloc
 }
 
 // ---------------------------------------------------------------------------
+// persistent batch kernel: many textures, any format / op / level, one launch
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ uint32_t bc4_texel(uint2 blk, int i) {
+    uint32_t v[8];
+    bc4_values(blk.x & 0xFF, (blk.x >> 8) & 0xFF, v);
+    const uint64_t bits = ((uint64_t)blk.y << 16) | (blk.x >> 16);
+    const uint32_t s = (uint32_t)(bits >> (3 * i)) & 7u;
+    uint32_t val = v[0];
+#pragma unroll
+    for (int k = 1; k < 8; k++) val = s == (uint32_t)k ? v[k] : val;
+    return val;
+}
+
+// texel `i` of block `b` of a BC1/BC3/BC4/BC5 texture (the decoders of k_decode, per texel)
+template <int IT>
+__device__ __forceinline__ uint32_t decode_texel(const uint8_t *blocks, int fmt, long b, int i, int write_alpha, int c0, int c1) {
+    if (fmt == 1 || fmt == 3) {
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(blocks) + (fmt == 1 ? 2 * b : 4 * b + 2);
+        const uint32_t x = __ldg(w), y = __ldg(w + 1);
+        uint32_t col[4];
+        bc1_palette<IT>(x & 0xFFFF, x >> 16, fmt == 1, fmt == 1 && write_alpha, col);
+        const uint32_t s = (y >> (2 * i)) & 3;
+        uint32_t px = s == 0 ? col[0] : (s == 1 ? col[1] : (s == 2 ? col[2] : col[3]));
+        if (fmt == 3) {
+            const uint32_t *a = reinterpret_cast<const uint32_t *>(blocks) + 4 * b;
+            px = (px & 0x00FFFFFFu) | (bc4_texel(make_uint2(__ldg(a), __ldg(a + 1)), i) << 24);
+        }
+        return px;
+    }
+    uint32_t px = 0xFF000000u;  // ColorBlock default texel (0, 0, 0, 255)
+    const uint32_t *w = reinterpret_cast<const uint32_t *>(blocks) + (fmt == 4 ? 2 * b : 4 * b);
+    px = (px & ~(0xFFu << (8 * c0))) | (bc4_texel(make_uint2(__ldg(w), __ldg(w + 1)), i) << (8 * c0));
+    if (fmt == 5) px = (px & ~(0xFFu << (8 * c1))) | (bc4_texel(make_uint2(__ldg(w + 2), __ldg(w + 3)), i) << (8 * c1));
+    return px;
+}
+
+__device__ __forceinline__ void batch_block(const Grp &G, const BatchItemDev &I, long b) {
+    const int by = (int)(b / I.bw), bx = (int)(b - (long)by * I.bw);
+    int sx = bx * 4 + (G.lane & 3), sy = by * 4 + (G.lane >> 2);
+    if (I.op == QT_OP_DECODE) {
+        uint32_t px;
+        switch (I.interp) {
+            case IT_IDEAL: px = decode_texel<IT_IDEAL>(I.src, I.fmt, b, G.lane, I.write_alpha, I.c0, I.c1); break;
+            case IT_ROUND: px = decode_texel<IT_ROUND>(I.src, I.fmt, b, G.lane, I.write_alpha, I.c0, I.c1); break;
+            case IT_NVIDIA: px = decode_texel<IT_NVIDIA>(I.src, I.fmt, b, G.lane, I.write_alpha, I.c0, I.c1); break;
+            default: px = decode_texel<IT_AMD>(I.src, I.fmt, b, G.lane, I.write_alpha, I.c0, I.c1); break;
+        }
+        if (sx + I.w >= 4 * I.bw && sy + I.h >= 4 * I.bh)  // the texel no later block overwrites (Texture.h:114-134)
+            *reinterpret_cast<uint32_t *>(I.dst + ((size_t)(sy % I.h) * I.w + (sx % I.w)) * 4) = px;
+        return;
+    }
+    if (sx >= I.w) sx %= I.w;
+    if (sy >= I.h) sy %= I.h;
+    const uint32_t v = *reinterpret_cast<const uint32_t *>(I.src + ((size_t)sy * I.w + sx) * 4);
+    const float fr = (float)(v & 0xFF), fg = (float)((v >> 8) & 0xFF), fb = (float)((v >> 16) & 0xFF);
+    s_px[G.g][G.lane] = v;
+    s_pf[G.g][G.lane] = make_float4(fr, fg, fb, fr * fr + fg * fg + fb * fb);
+    const unsigned pp = gsum(G.gm, sq3((int)(v & 0xFF), (int)((v >> 8) & 0xFF), (int)((v >> 16) & 0xFF)));
+    if (G.lane == 0) s_pp[G.g] = (int)pp;
+    __syncwarp(G.gm);
+    if (I.fmt == 1 || I.fmt == 3) {
+        qt_bc1_params p = I.p;
+        if (I.fmt == 3) p.color_mode = CM_FOUR;
+        uint2 blk;
+        switch (p.interpolator) {
+            case IT_IDEAL: blk = encode_bc1_group<IT_IDEAL>(G, p); break;
+            case IT_ROUND: blk = encode_bc1_group<IT_ROUND>(G, p); break;
+            case IT_NVIDIA: blk = encode_bc1_group<IT_NVIDIA>(G, p); break;
+            default: blk = encode_bc1_group<IT_AMD>(G, p); break;
+        }
+        if (I.fmt == 3) {
+            const uint2 a = encode_bc4_group(G, 3);
+            if (G.lane == 0) reinterpret_cast<uint4 *>(I.dst)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
+        } else if (G.lane == 0) {
+            reinterpret_cast<uint2 *>(I.dst)[b] = blk;
+        }
+    } else {
+        const uint2 a = encode_bc4_group(G, I.c0);
+        if (I.fmt == 5) {
+            const uint2 c = encode_bc4_group(G, I.c1);
+            if (G.lane == 0) reinterpret_cast<uint4 *>(I.dst)[b] = make_uint4(a.x, a.y, c.x, c.y);
+        } else if (G.lane == 0) {
+            reinterpret_cast<uint2 *>(I.dst)[b] = a;
+        }
+    }
+    __syncwarp(G.gm);
+}
+
+// ctl[0] is the queue head (atomically advanced by each group), ctl[1] the number of tiles.
+__global__ void __launch_bounds__(128, 6) k_batch(const BatchItemDev *__restrict__ items, const TileDev *__restrict__ tiles,
+                                                  uint32_t *__restrict__ ctl) {
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+        if (i < 32) s_mid5[i] = c_mid5[i];
+        s_mid6[i] = c_mid6[i];
+        if (i < 16) s_vox[i] = c_voxels[i];
+    }
+    __syncthreads();
+    const Grp G = grp();
+    const uint32_t ntiles = ctl[1];
+    while (true) {
+        uint32_t t = 0;
+        if (G.lane == 0) t = atomicAdd(&ctl[0], 1u);
+        t = __shfl_sync(G.gm, t, 0, 16);
+        if (t >= ntiles) break;
+        const TileDev T = tiles[t];
+        const BatchItemDev I = items[T.item];
+        for (uint32_t k = 0; k < T.count; k++) batch_block(G, I, (long)T.start + k);
+    }
+}
+
+// ---------------------------------------------------------------------------
 // host-side launchers
 // ---------------------------------------------------------------------------
+static int num_sms() {
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+    return sms;
+}
+
 static int grid_for(long work, int per_cta) {
-    static int sms = 0;
-    if (sms == 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-        if (sms <= 0) sms = 148;
-    }
-    long need = (work + per_cta - 1) / per_cta;
-    long cap = (long)sms * 64;
+    const long need = (work + per_cta - 1) / per_cta;
+    const long cap = (long)num_sms() * 64;
     return (int)(need < cap ? (need > 0 ? need : 1) : cap);
 }
 
@@ -1268,6 +1379,20 @@ int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p,
         case IT_NVIDIA: k_bc1_encode<IT_NVIDIA><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
         default: k_bc1_encode<IT_AMD><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
     }
+    return (int)cudaGetLastError();
+}
+
+int batch_sms() { return num_sms(); }
+
+int batch_ctas_per_sm() {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch, 128, 0) != cudaSuccess || n <= 0) n = 1;
+    return n;
+}
+
+int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, void *stream) {
+    if (grid <= 0) grid = num_sms() * batch_ctas_per_sm();
+    k_batch<<<grid, 128, 0, (cudaStream_t)stream>>>(items, tiles, ctl);
     return (int)cudaGetLastError();
 }
 
