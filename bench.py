@@ -315,12 +315,95 @@ def run_ours(args, world, rank, local):
         "gpu_launches": len(SETTINGS) * args.steps,
         "clocks": clk.summary(),
     }
+    if not args.no_batch:
+        line["batched"] = measure_batched(args, dev, world)
     if world == 1 and rank == 0 and not args.no_cpu:
         v, dt, cores, kind = cpu_reference_sample(img)
         line["cpu_baseline"] = {"value": v, "unit": "Mblocks/s", "cores": cores, "kind": kind,
                                 "sample": f"512x512 crop x 36 settings, as-shipped OpenMP encode, {dt:.1f} s"}
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+def measure_batched(args, dev, world):
+    """Mixed batch: 10,000 seeded textures (log-uniform sides 4..2048, 25% off the
+    4-texel grid; BC1:BC3:BC4:BC5 = 4:3:2:1; levels uniform in {0,5,10,18};
+    BC4 on channel 0, BC5 on channels 0,1) as one persistent CUDA-graph launch
+    versus one launch per texture, device-resident; plus the persistent path
+    with the upload and download of all textures inside the timed region."""
+    import torch
+
+    import quicktex_b200.synth as syn
+    from quicktex_b200.batch import Arena, Batch, Job, run_plain, run_plain_host
+
+    items = syn.mixed_batch(args.batch_count)
+    pools = syn.MixedBatchPools()
+    jobs = [Job.encode(i.fmt, pools.texture(i), i.width, i.height, level=i.level, channel=0, chan0=0, chan1=1)
+            for i in items]
+    del pools
+    nblocks = sum(j.nblocks for j in jobs)
+    arena = Arena(jobs, dev.index)
+    arena.upload()
+    stream = torch.cuda.current_stream(dev)
+    sptr = stream.cuda_stream
+    citems = arena.items()
+    batch = Batch(dev.index)
+
+    def timed(fn, reps):
+        ts = []
+        for _ in range(reps):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        return ts
+
+    for _ in range(args.warmup):
+        batch.run(citems, sptr)
+    torch.cuda.synchronize()
+    persistent = timed(lambda: batch.run(citems, sptr), args.steps)
+    arena.download()
+    torch.cuda.synchronize()
+    out_persistent = arena.h_out.clone()
+    arena.d_out.zero_()
+    run_plain(citems, sptr)
+    torch.cuda.synchronize()
+    plain = timed(lambda: run_plain(citems, sptr), max(1, args.steps // 2))
+    arena.download()
+    torch.cuda.synchronize()
+    identical = bool(torch.equal(out_persistent, arena.h_out))
+
+    def e2e():
+        arena.upload()
+        batch.run(citems, sptr)
+        arena.download()
+
+    e2e_ms = timed(e2e, max(1, args.steps // 2))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    run_plain_host(arena)
+    plain_e2e = (time.perf_counter() - t0) * 1e3
+    pm, qm, em = float(np.median(persistent)), float(np.median(plain)), float(np.median(e2e_ms))
+    ntiles = batch.last_tiles()
+    batch.close()
+    return {
+        "workload": f"{len(jobs)} textures, log-uniform 4..2048 sides (25% not multiples of 4), "
+                    "BC1:BC3:BC4:BC5 = 4:3:2:1, levels {0,5,10,18}, encode",
+        "blocks": nblocks,
+        "persistent_mblocks_s": world * nblocks / (pm / 1e3) / 1e6,
+        "plain_mblocks_s": world * nblocks / (qm / 1e3) / 1e6,
+        "persistent_over_plain": qm / pm,
+        "persistent_e2e_mblocks_s": world * nblocks / (em / 1e3) / 1e6,
+        "plain_e2e_mblocks_s": world * nblocks / (plain_e2e / 1e3) / 1e6,
+        "persistent_over_plain_e2e": plain_e2e / em,
+        "e2e_h2d_bytes": arena.in_bytes, "e2e_d2h_bytes": arena.out_bytes,
+        "ms": {"persistent": pm, "plain": qm, "persistent_e2e": em, "plain_e2e": plain_e2e},
+        "tiles": ntiles,
+        "launches_per_step": {"persistent": 1, "plain": len(jobs)},
+        "outputs_identical": identical,
+    }
 
 
 def main():
@@ -331,6 +414,8 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
+    ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain leg")
+    ap.add_argument("--batch-count", type=int, default=10000, help="textures in the batched leg")
     ap.add_argument("--size", type=int, default=4096, help="texture side (profiling variants only)")
     ap.add_argument("--levels", type=str, default="0,10,18", help="levels (profiling variants only)")
     args = ap.parse_args()

@@ -239,6 +239,27 @@ def run_plain(items: Sequence[BatchItem], stream: int = 0) -> None:
         capi.check(rc)
 
 
+def run_plain_host(arena: "Arena") -> None:
+    """Every texture through its own host-buffer C-ABI call (upload, launch,
+    download and wait per texture): the per-texture launch model end to end."""
+    L = capi.lib()
+    hi, ho = arena.h_in.data_ptr(), arena.h_out.data_ptr()
+    for j, a, b in zip(arena.jobs, arena.in_off, arena.out_off):
+        src, dst, w, h = ctypes.c_void_p(hi + a), ctypes.c_void_p(ho + b), j.width, j.height
+        if j.op == QT_OP_ENCODE:
+            p = ctypes.byref(j.params) if j.params is not None else None
+            rc = (L.qt_bc1_encode_host(src, w, h, p, dst) if j.fmt == 1 else
+                  L.qt_bc3_encode_host(src, w, h, p, dst) if j.fmt == 3 else
+                  L.qt_bc4_encode_host(src, w, h, j.chan0, dst) if j.fmt == 4 else
+                  L.qt_bc5_encode_host(src, w, h, j.chan0, j.chan1, dst))
+        else:
+            rc = (L.qt_bc1_decode_host(src, w, h, j.interpolator, int(j.write_alpha), dst) if j.fmt == 1 else
+                  L.qt_bc3_decode_host(src, w, h, j.interpolator, dst) if j.fmt == 3 else
+                  L.qt_bc4_decode_host(src, w, h, j.chan0, dst) if j.fmt == 4 else
+                  L.qt_bc5_decode_host(src, w, h, j.chan0, j.chan1, dst))
+        capi.check(rc)
+
+
 def run_jobs(jobs: Sequence[Job], device: int = 0, batch: Optional[Batch] = None) -> list[bytes]:
     """Upload, one persistent launch, download; returns each job's output bytes."""
     import torch

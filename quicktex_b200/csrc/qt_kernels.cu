@@ -938,15 +938,15 @@ __device__ __forceinline__ uint2 write_block(const Res &r) {
 // ---------------------------------------------------------------------------
 // BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342) for the group's block
 // ---------------------------------------------------------------------------
-template <int IT> __device__ __forceinline__ uint2 encode_bc1_group(const Grp &G, const qt_bc1_params &p) {
+template <int IT> __device__ __forceinline__ uint2 encode_bc1_group(const Grp &G, const qt_bc1_params &p, int color_mode) {
     if (__all_sync(G.gm, s_px[G.g][G.lane] == s_px[G.g][0])) return write_block_solid<IT>(s_px[G.g][0]);
 
     get_metrics(0, false);
     const bool has_black = s_met[G.g][0][MT_BLACK] != 0;
     const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
     bool needs_err = use_likely;
-    needs_err |= p.color_mode == CM_THREE;
-    needs_err |= (p.color_mode == CM_TB) && has_black;
+    needs_err |= color_mode == CM_THREE;
+    needs_err |= (color_mode == CM_TB) && has_black;
     needs_err |= p.error_mode != EM_NONE;
     needs_err |= p.search_rounds > 0;
     const int em = needs_err ? p.error_mode : EM_NONE;
@@ -974,7 +974,7 @@ template <int IT> __device__ __forceinline__ uint2 encode_bc1_group(const Grp &G
     if (res.err > 0 && use_likely)
         for (int it = 0; it < cf_passes; it++) res = refine_cf_any<IT>(kind_for(CM_FOUR, p.error_mode), res, p.orderings4, p.exhaustive, 0);
 
-    if (res.err > 0 && (p.color_mode & CM_THREE)) {
+    if (res.err > 0 && (color_mode & CM_THREE)) {
         Res t = orig;
         const SelErr se = fs_tp<IT, K_T3>(t.lo, t.hi);
         t.sel = se.sel;
@@ -986,7 +986,7 @@ template <int IT> __device__ __forceinline__ uint2 encode_bc1_group(const Grp &G
         if (t.err < res.err) res = t;
     }
 
-    if (res.err > 0 && p.color_mode == CM_TB && has_black) {
+    if (res.err > 0 && color_mode == CM_TB && has_black) {
         const int *M0 = s_met[G.g][0];
         if (!((M0[MT_MX] | M0[MT_MX + 1] | M0[MT_MX + 2]) < 4)) {
             get_metrics(1, true);
@@ -1040,7 +1040,7 @@ __global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict
     }
     __syncthreads();
     const Grp G = grp();
-    if (bc3) p.color_mode = CM_FOUR;  // BC3Encoder.h:39-40
+    const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
 
     for (long b = (long)blockIdx.x * kGroupsPerCta + G.g; b < nblocks; b += (long)gridDim.x * kGroupsPerCta) {
         const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
@@ -1054,7 +1054,7 @@ __global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict
         const unsigned pp = gsum(G.gm, sq3((int)(v & 0xFF), (int)((v >> 8) & 0xFF), (int)((v >> 16) & 0xFF)));
         if (G.lane == 0) s_pp[G.g] = (int)pp;
         __syncwarp(G.gm);
-        const uint2 blk = encode_bc1_group<IT>(G, p);
+        const uint2 blk = encode_bc1_group<IT>(G, p, color_mode);
         if (bc3) {
             const uint2 a = encode_bc4_group(G, 3);
             if (G.lane == 0) reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
@@ -1268,7 +1268,11 @@ __device__ __forceinline__ uint32_t decode_texel(const uint8_t *blocks, int fmt,
     return px;
 }
 
-__device__ __forceinline__ void batch_block(const Grp &G, const BatchItemDev &I, long b) {
+template <int IT> __device__ __noinline__ uint2 encode_bc1_batch(const qt_bc1_params *p, int color_mode) {
+    return encode_bc1_group<IT>(grp(), *p, color_mode);
+}
+
+__device__ __forceinline__ void batch_block(const Grp &G, const BatchItemDev &__restrict__ I, long b) {
     const int by = (int)(b / I.bw), bx = (int)(b - (long)by * I.bw);
     int sx = bx * 4 + (G.lane & 3), sy = by * 4 + (G.lane >> 2);
     if (I.op == QT_OP_DECODE) {
@@ -1293,14 +1297,13 @@ __device__ __forceinline__ void batch_block(const Grp &G, const BatchItemDev &I,
     if (G.lane == 0) s_pp[G.g] = (int)pp;
     __syncwarp(G.gm);
     if (I.fmt == 1 || I.fmt == 3) {
-        qt_bc1_params p = I.p;
-        if (I.fmt == 3) p.color_mode = CM_FOUR;
+        const int cm = I.fmt == 3 ? CM_FOUR : I.p.color_mode;  // BC3Encoder.h:39-40
         uint2 blk;
-        switch (p.interpolator) {
-            case IT_IDEAL: blk = encode_bc1_group<IT_IDEAL>(G, p); break;
-            case IT_ROUND: blk = encode_bc1_group<IT_ROUND>(G, p); break;
-            case IT_NVIDIA: blk = encode_bc1_group<IT_NVIDIA>(G, p); break;
-            default: blk = encode_bc1_group<IT_AMD>(G, p); break;
+        switch (I.p.interpolator) {
+            case IT_IDEAL: blk = encode_bc1_batch<IT_IDEAL>(&I.p, cm); break;
+            case IT_ROUND: blk = encode_bc1_batch<IT_ROUND>(&I.p, cm); break;
+            case IT_NVIDIA: blk = encode_bc1_batch<IT_NVIDIA>(&I.p, cm); break;
+            default: blk = encode_bc1_batch<IT_AMD>(&I.p, cm); break;
         }
         if (I.fmt == 3) {
             const uint2 a = encode_bc4_group(G, 3);
@@ -1337,7 +1340,8 @@ __global__ void __launch_bounds__(128, 6) k_batch(const BatchItemDev *__restrict
         t = __shfl_sync(G.gm, t, 0, 16);
         if (t >= ntiles) break;
         const TileDev T = tiles[t];
-        const BatchItemDev I = items[T.item];
+        // the descriptor stays in (L1-cached) global memory: copying it to registers spills
+        const BatchItemDev &I = items[T.item];
         for (uint32_t k = 0; k < T.count; k++) batch_block(G, I, (long)T.start + k);
     }
 }

@@ -196,3 +196,21 @@ def mixed_batch(count: int = 10000, workload: int = 4, max_side: int = 2048) -> 
                 h = h - 4 if h > max_side else h
         items.append(BatchItem(FORMATS[int(fmts[i])], LEVELS[int(levels[i])], w, h, i))
     return items
+
+
+class MixedBatchPools:
+    """Texel sources for the mixed batch: every texture is a window, at a seeded
+    offset, of one of two pre-generated 4096x4096 pools (block mix; block mix
+    with the alpha mix for BC3), so 10,000 textures cost two pool generations."""
+
+    def __init__(self, workload: int = 4, side: int = 4096):
+        self.side = side
+        self.rgb = block_mix(side, side, workload=workload, stream=1)
+        self.rgba = alpha_mix(side, side, workload=workload, stream=2)
+        self.rng = rng_for(workload, 3)
+
+    def texture(self, item: BatchItem) -> np.ndarray:
+        pool = self.rgba if item.fmt == "bc3" else self.rgb
+        y0 = int(self.rng.integers(0, self.side - item.height + 1))
+        x0 = int(self.rng.integers(0, self.side - item.width + 1))
+        return np.ascontiguousarray(pool[y0:y0 + item.height, x0:x0 + item.width])
