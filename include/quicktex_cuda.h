@@ -185,6 +185,27 @@ int qt_batch_run(qt_batch *b, const qt_batch_item *items, size_t n, void *stream
 /* Number of tiles the last qt_batch_run queued. */
 size_t qt_batch_last_tiles(const qt_batch *b);
 
+/* ---- the batched path without device allocation (no counterpart in the reference) ----
+ *
+ * For callers that may not allocate GPU memory when they encode: engines that
+ * reserve their whole device budget at start-up, latency-critical loops that
+ * cannot take the device-wide synchronisation cudaMalloc/cudaFree may cause,
+ * code running under a host allocator lock. Same work and same output bytes as
+ * qt_batch_run, but the work queue lives in a fixed array of
+ * QT_NOALLOC_SCRATCH_BYTES (384 KiB) inside the library, held on every GPU that
+ * loads it until the process exits; the call makes no cudaMalloc/cudaFree and
+ * creates no batch object. Inputs and outputs are the caller's device buffers.
+ *  - At most QT_NOALLOC_MAX_ITEMS textures per call; more -> QT_ERR_ARG.
+ *  - All calls share the one queue, which keeps the last call's contents (its
+ *    head is reset on every call): calls whose GPU work overlaps race, so issue
+ *    them on one stream or wait for the previous one.
+ *  - The first call on a device sets up the queue's device address (and the
+ *    constant tables); make it before any stream capture. */
+#define QT_NOALLOC_MAX_ITEMS 1024
+#define QT_NOALLOC_MAX_TILES 16384
+#define QT_NOALLOC_SCRATCH_BYTES (384 * 1024)
+int qt_batch_run_noalloc(const qt_batch_item *items, size_t n, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
