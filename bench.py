@@ -317,6 +317,8 @@ def run_ours(args, world, rank, local):
     }
     if not args.no_batch:
         line["batched"] = measure_batched(args, dev, world)
+    if not args.no_serve and world == 1:
+        line["serve"] = measure_serving(args, dev)
     if world == 1 and rank == 0 and not args.no_cpu:
         v, dt, cores, kind = cpu_reference_sample(img)
         line["cpu_baseline"] = {"value": v, "unit": "Mblocks/s", "cores": cores, "kind": kind,
@@ -406,6 +408,67 @@ def measure_batched(args, dev, world):
     }
 
 
+def measure_serving(args, dev):
+    """Open-loop Poisson arrivals of encode (70%) / decode (30%) requests, sizes,
+    formats and levels drawn as in the mixed batch, against the continuous-batching
+    server (16 GiB device budget); latency = arrival -> result bytes on the host."""
+    import torch
+
+    import quicktex_b200.synth as syn
+    from quicktex_b200.batch import Job, run_jobs
+    from quicktex_b200.serve import Server, latency_stats
+
+    items = syn.mixed_batch(args.serve_pool, workload=5)
+    pools = syn.MixedBatchPools(workload=5)
+    enc = [Job.encode(i.fmt, pools.texture(i), i.width, i.height, level=i.level, channel=0, chan0=0, chan1=1)
+           for i in items]
+    del pools
+    dec = [Job.decode({1: "bc1", 3: "bc3", 4: "bc4", 5: "bc5"}[j.fmt], np.frombuffer(o, np.uint8), j.width, j.height,
+                      channel=0, chan0=0, chan1=1) for j, o in zip(enc, run_jobs(enc, dev.index))]
+    # request payloads live in pinned host memory, as a serving front end would keep them
+    total = sum(j.data.nbytes for j in enc + dec)
+    pinned = torch.empty(total, dtype=torch.uint8).pin_memory().numpy()
+    o = 0
+    for j in enc + dec:
+        n = j.data.nbytes
+        pinned[o:o + n] = j.data
+        j.data = pinned[o:o + n]
+        o += n
+    srv = Server(dev.index, memory_budget=16 << 30, slots=3)
+    for f in [srv.submit(j) for j in enc[:8] + dec[:8]]:  # warm-up: graphs captured, tables resident
+        f.result()
+    loads = []
+    for rate, seconds in zip(args.serve_rates, args.serve_seconds):
+        rng = np.random.default_rng(int(rate))
+        n = max(1, int(rate * seconds))
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+        is_dec = rng.random(n) < 0.3
+        pick = rng.integers(0, len(enc), n)
+        blocks0, batches0 = srv.blocks_done, srv.batches
+        t0 = time.perf_counter() + 0.01
+        futs = []
+        for k in range(n):
+            t = t0 + arrivals[k]
+            while True:
+                d = t - time.perf_counter()
+                if d <= 0:
+                    break
+                if d > 2e-4:
+                    time.sleep(d - 1e-4)
+            futs.append(srv.submit(dec[pick[k]] if is_dec[k] else enc[pick[k]], t_arrival=t))
+        for f in futs:
+            f.result()
+        span = max(f.request.t_done for f in futs) - t0
+        st = latency_stats(futs)
+        st.update({"offered_rps": rate, "achieved_rps": n / span, "mblocks_s": (srv.blocks_done - blocks0) / span / 1e6,
+                   "batches": srv.batches - batches0, "seconds_offered": seconds})
+        loads.append(st)
+    srv.close()
+    return {"mix": "70% encode / 30% decode; sizes, formats and levels as the mixed batch; "
+                   f"{len(enc)} distinct payloads in pinned host memory",
+            "device_budget_gib": 16, "slots": 3, "max_inflight_seen": srv.max_inflight_seen, "loads": loads}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -416,6 +479,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer end-to-end leg")
     ap.add_argument("--no-batch", action="store_true", help="skip the batched-vs-plain leg")
     ap.add_argument("--batch-count", type=int, default=10000, help="textures in the batched leg")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
+    ap.add_argument("--serve-pool", type=int, default=256, help="distinct request payloads")
+    ap.add_argument("--serve-rates", type=float, nargs="+", default=[1000, 10000, 50000])
+    ap.add_argument("--serve-seconds", type=float, nargs="+", default=[2.0, 2.0, 1.0])
     ap.add_argument("--size", type=int, default=4096, help="texture side (profiling variants only)")
     ap.add_argument("--levels", type=str, default="0,10,18", help="levels (profiling variants only)")
     args = ap.parse_args()

@@ -1,0 +1,229 @@
+"""Serving: continuous batching of encode/decode requests on one GPU.
+
+A ``Server`` accepts requests at any time (``submit`` returns a future) and
+runs them through the batched persistent path:
+
+* **Admission by memory budget.** Input and output buffers come from one
+  pre-reserved device arena (``memory_budget`` bytes, first-fit free list). A
+  request is admitted into a batch only when its bytes fit; otherwise it waits
+  until a running batch returns its memory.
+* **Continuous batching.** ``slots`` batches can be in flight at once, each on
+  its own CUDA stream with its own ``qt_batch`` queue. Whenever a slot is free
+  the worker folds every waiting request that fits (up to ``max_batch_blocks``)
+  into the next persistent launch, so requests that arrive while others run on
+  the GPU are admitted as soon as a slot and memory free up, and their work
+  overlaps on the device with the batches still running.
+* **Resident buffers.** Nothing is allocated per request: device memory is
+  carved from the arena, host staging is pinned and reused.
+
+The integer block output does not depend on what else is in a batch: every
+request's bytes equal those of the single-texture call (tests check this).
+"""
+
+from __future__ import annotations
+
+import collections
+import concurrent.futures
+import threading
+import time
+from typing import Optional
+
+import numpy as np
+
+from .batch import Batch, BatchItem, Job
+
+
+class DeviceArena:
+    """First-fit free list over one device buffer (the memory budget)."""
+
+    ALIGN = 256
+
+    def __init__(self, nbytes: int, device: int):
+        import torch
+
+        self.buf = torch.empty(nbytes, dtype=torch.uint8, device=torch.device("cuda", device))
+        self.base = self.buf.data_ptr()
+        self.size = nbytes
+        self.free = [(0, nbytes)]  # sorted (offset, length)
+        self.in_use = 0
+
+    def alloc(self, n: int) -> Optional[int]:
+        n = (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN
+        for i, (off, ln) in enumerate(self.free):
+            if ln >= n:
+                if ln == n:
+                    self.free.pop(i)
+                else:
+                    self.free[i] = (off + n, ln - n)
+                self.in_use += n
+                return off
+        return None
+
+    def release(self, off: int, n: int) -> None:
+        n = (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN
+        self.in_use -= n
+        fl = self.free
+        fl.append((off, n))
+        fl.sort()
+        merged = []
+        for o, l in fl:
+            if merged and merged[-1][0] + merged[-1][1] == o:
+                merged[-1] = (merged[-1][0], merged[-1][1] + l)
+            else:
+                merged.append((o, l))
+        self.free = merged
+
+
+class Request:
+    __slots__ = ("job", "future", "t_arrival", "t_done", "in_off", "out_off", "nbytes")
+
+    def __init__(self, job: Job, t_arrival: float):
+        self.job = job
+        self.future = concurrent.futures.Future()
+        self.t_arrival = t_arrival
+        self.t_done = None
+
+
+class _Slot:
+    def __init__(self, device: int, tuning=None):
+        import torch
+
+        self.stream = torch.cuda.Stream(device=device)
+        self.batch = Batch(device, tuning=tuning)
+        self.event = None
+        self.reqs: list[Request] = []
+        self.region = None  # (offset, nbytes) in the arena
+        self.h_out = None
+
+
+class Server:
+    """Continuous-batching encode/decode server on one GPU."""
+
+    def __init__(self, device: int = 0, memory_budget: int = 16 << 30, slots: int = 3,
+                 max_batch_blocks: int = 1 << 22, tuning=None):
+        import torch
+
+        torch.cuda.set_device(device)
+        self.device = device
+        self.arena = DeviceArena(memory_budget, device)
+        self.slots = [_Slot(device, tuning) for _ in range(slots)]
+        self.max_batch_blocks = max_batch_blocks
+        self.pending: collections.deque[Request] = collections.deque()
+        self.cv = threading.Condition()
+        self.running = True
+        self.batches = 0
+        self.blocks_done = 0
+        self.max_inflight_seen = 0
+        self.worker = threading.Thread(target=self._loop, name="quicktex-serve", daemon=True)
+        self.worker.start()
+
+    # ---- client side --------------------------------------------------------
+    def submit(self, job: Job, t_arrival: Optional[float] = None) -> concurrent.futures.Future:
+        """Queue a request; the future resolves to its output bytes. ``t_arrival``
+        (perf_counter seconds) defaults to now; latency is measured from it."""
+        r = Request(job, time.perf_counter() if t_arrival is None else t_arrival)
+        r.future.request = r
+        with self.cv:
+            self.pending.append(r)
+            self.cv.notify()
+        return r.future
+
+    def close(self) -> None:
+        with self.cv:
+            self.running = False
+            self.cv.notify()
+        self.worker.join()
+        for s in self.slots:
+            s.batch.close()
+
+    # ---- worker ---------------------------------------------------------------
+    def _launch(self, slot: _Slot, reqs: list[Request]) -> None:
+        import torch
+
+        n_in = sum(DeviceArena.ALIGN * ((r.job.data.nbytes + 255) // 256) for r in reqs)
+        n_out = sum(DeviceArena.ALIGN * ((r.job.out_bytes + 255) // 256) for r in reqs)
+        off = self.arena.alloc(n_in + n_out)
+        assert off is not None  # reserved by the caller
+        base = self.arena.base + off
+        items = []
+        pi, po = 0, n_in
+        with torch.cuda.stream(slot.stream):
+            for r in reqs:
+                j = r.job
+                r.in_off, r.out_off = pi, po - n_in
+                src = self.arena.buf[off + pi: off + pi + j.data.nbytes]
+                src.copy_(torch.from_numpy(j.data), non_blocking=True)
+                items.append(j.item(base + pi, base + po))
+                pi += DeviceArena.ALIGN * ((j.data.nbytes + 255) // 256)
+                po += DeviceArena.ALIGN * ((j.out_bytes + 255) // 256)
+            slot.batch.run(items, slot.stream.cuda_stream)
+            if slot.h_out is None or slot.h_out.numel() < n_out:
+                slot.h_out = torch.empty(max(n_out, 1 << 20) * 2, dtype=torch.uint8).pin_memory()
+            slot.h_out[:n_out].copy_(self.arena.buf[off + n_in: off + n_in + n_out], non_blocking=True)
+            slot.event = torch.cuda.Event()
+            slot.event.record(slot.stream)
+        slot.reqs = reqs
+        slot.region = (off, n_in + n_out)
+        self.batches += 1
+
+    def _complete(self, slot: _Slot) -> None:
+        t = time.perf_counter()
+        host = slot.h_out.numpy()
+        for r in slot.reqs:
+            out = host[r.out_off: r.out_off + r.job.out_bytes].tobytes()
+            r.t_done = t
+            self.blocks_done += r.job.nblocks
+            r.future.set_result(out)
+        self.arena.release(*slot.region)
+        slot.reqs, slot.region, slot.event = [], None, None
+
+    def _take(self) -> list[Request]:
+        """Admit waiting requests, FIFO, while they fit in the free memory and the batch cap."""
+        reqs, nbytes, blocks = [], 0, 0
+        free = self.arena.size - self.arena.in_use
+        largest = max((l for _, l in self.arena.free), default=0)
+        while self.pending:
+            r = self.pending[0]
+            need = DeviceArena.ALIGN * ((r.job.data.nbytes + 255) // 256 + (r.job.out_bytes + 255) // 256)
+            if reqs and (blocks + r.job.nblocks > self.max_batch_blocks):
+                break
+            if nbytes + need > min(free, largest):
+                break
+            reqs.append(self.pending.popleft())
+            nbytes += need
+            blocks += r.job.nblocks
+        return reqs
+
+    def _loop(self) -> None:
+        import torch
+
+        torch.cuda.set_device(self.device)
+        while True:
+            busy = [s for s in self.slots if s.event is not None]
+            for s in busy:
+                if s.event.query():
+                    self._complete(s)
+            free_slots = [s for s in self.slots if s.event is None]
+            inflight = len(self.slots) - len(free_slots)
+            with self.cv:
+                if not self.running and not self.pending and inflight == 0:
+                    return
+                reqs = self._take() if (free_slots and self.pending) else []
+                if not reqs and inflight == 0:
+                    if self.pending and not self.arena.in_use:  # a request larger than the whole budget
+                        r = self.pending.popleft()
+                        r.future.set_exception(MemoryError("request exceeds the server's memory budget"))
+                        continue
+                    self.cv.wait(timeout=0.001)
+                    continue
+            if reqs:
+                self._launch(free_slots[0], reqs)
+                self.max_inflight_seen = max(self.max_inflight_seen, inflight + 1)
+            else:
+                time.sleep(20e-6)
+
+
+def latency_stats(futures) -> dict:
+    lat = np.array([(f.request.t_done - f.request.t_arrival) * 1e3 for f in futures])
+    return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "mean_ms": float(lat.mean()), "max_ms": float(lat.max()), "requests": int(len(lat))}

@@ -1,0 +1,73 @@
+"""GPU: the continuous-batching server. Every request's result is the same
+alone and in the mix; requests are folded into shared launches, batches
+overlap on the device, and the memory budget admits requests as memory frees."""
+
+import time
+
+import numpy as np
+import pytest
+
+import quicktex_b200.synth as syn
+from quicktex_b200.batch import Job, run_jobs
+from quicktex_b200.serve import Server, latency_stats
+
+pytestmark = pytest.mark.gpu
+
+
+def _jobs(seed, n, max_side=200):
+    rng = np.random.default_rng(seed)
+    pool = syn.alpha_mix(max_side, max_side, workload=9, stream=40 + seed)
+    jobs = []
+    for _ in range(n):
+        w, h = int(rng.integers(1, max_side)), int(rng.integers(1, max_side))
+        fmt = ["bc1", "bc3", "bc4", "bc5"][int(rng.integers(0, 4))]
+        img = np.ascontiguousarray(pool[:h, :w])
+        if rng.random() < 0.3:
+            nb = ((w + 3) // 4) * ((h + 3) // 4) * (16 if fmt in ("bc3", "bc5") else 8)
+            jobs.append(Job.decode(fmt, rng.integers(0, 256, nb, dtype=np.uint8), w, h, interpolator=int(rng.integers(0, 4))))
+        else:
+            jobs.append(Job.encode(fmt, img, w, h, level=int(rng.choice([0, 5, 10, 18])),
+                                   color_mode=int(rng.choice([4, 3, 0x13])), interpolator=int(rng.integers(0, 4)), channel=0))
+    return jobs
+
+
+def test_results_same_alone_and_in_the_mix():
+    jobs = _jobs(1, 120)
+    alone = [run_jobs([j])[0] for j in jobs]
+    srv = Server(memory_budget=8 << 20, slots=3, max_batch_blocks=4096)
+    futs = [srv.submit(j) for j in jobs]
+    outs = [f.result(timeout=120) for f in futs]
+    srv.close()
+    assert outs == alone
+    assert srv.batches < len(jobs)        # requests were folded into shared launches
+    assert srv.max_inflight_seen >= 2     # batches overlapped on the device
+    st = latency_stats(futs)
+    assert st["requests"] == len(jobs) and st["p99_ms"] >= st["p50_ms"] > 0
+
+
+def test_budget_admission_and_oversize_request():
+    jobs = _jobs(2, 40, max_side=128)
+    # a budget that holds only a few requests at a time: the rest wait for memory to free up
+    srv = Server(memory_budget=1 << 20, slots=2)
+    futs = [srv.submit(j) for j in jobs]
+    big = Job.encode("bc1", np.zeros((1024, 1024, 4), np.uint8), 1024, 1024)  # 4 MiB + blocks > 1 MiB budget
+    fbig = srv.submit(big)
+    outs = [f.result(timeout=120) for f in futs]
+    with pytest.raises(MemoryError):
+        fbig.result(timeout=120)
+    srv.close()
+    assert outs == run_jobs(jobs)
+
+
+def test_requests_arriving_while_busy_are_admitted():
+    jobs = _jobs(3, 60)
+    srv = Server(memory_budget=64 << 20, slots=2, max_batch_blocks=2048)
+    futs = []
+    for i, j in enumerate(jobs):  # a steady trickle while earlier batches run
+        futs.append(srv.submit(j))
+        if i % 10 == 9:
+            time.sleep(0.002)
+    outs = [f.result(timeout=120) for f in futs]
+    srv.close()
+    assert outs == run_jobs(jobs)
+    assert srv.batches >= 2
