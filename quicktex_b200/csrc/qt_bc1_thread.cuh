@@ -1,0 +1,641 @@
+// qt_bc1_thread.cuh — thread-per-block BC1/BC3 encoder (included by qt_kernels.cu).
+//
+// One thread encodes one 4x4 block, following BC1Encoder::EncodeBlock
+// (BC1Encoder.cpp:261-342) step by step, with no cross-lane work: no
+// replicated scalar code, no reductions, 32 blocks in flight per warp. The
+// block's texels, cluster-fit sort keys and prefix sums live in shared
+// memory in a transposed layout ([item][thread]), so every per-texel access of
+// a warp is one conflict-free shared load and the loops stay rolled (a small
+// instruction footprint). Float arithmetic uses the same round-to-nearest
+// intrinsics and operation order as the group kernel; every texel sum is an
+// exact integer.
+
+namespace tpb {
+
+constexpr int kThreads = 128;
+
+__shared__ uint32_t t_px[16][kThreads];     // texel i of the thread's block
+__shared__ uint32_t t_srg[17][kThreads];    // cluster-fit prefix sums: r | g << 16
+__shared__ uint16_t t_sb[17][kThreads];     //                          b
+__shared__ uint32_t t_key[16][kThreads];    // cluster-fit projection keys
+
+struct R {  // EncodeResults (BC1Encoder.h:147-153); endpoints packed 5:6:5
+    int lo, hi;
+    uint32_t sel;
+    int mode;
+    uint32_t err;
+};
+
+__device__ __forceinline__ R rinit() {
+    R r;
+    r.lo = r.hi = 0;
+    r.sel = 0;
+    r.mode = CM_INCOMPLETE;
+    r.err = UINT_MAX;
+    return r;
+}
+
+struct M {  // ColorBlock::Metrics (ColorBlock.h:88-117)
+    int mn[3], mx[3], av[3], sum[3];
+    bool grey, has_black;
+};
+
+__device__ __forceinline__ uint32_t px(int i) { return t_px[i][threadIdx.x]; }
+__device__ __forceinline__ int cr(uint32_t v) { return v & 0xFF; }
+__device__ __forceinline__ int cg(uint32_t v) { return (v >> 8) & 0xFF; }
+__device__ __forceinline__ int cb(uint32_t v) { return (v >> 16) & 0xFF; }
+__device__ __forceinline__ bool black(uint32_t v) { return (cr(v) | cg(v) | cb(v)) < 4; }
+
+__device__ __noinline__ M metrics(bool ignore_black) {
+    M m;
+    m.mn[0] = m.mn[1] = m.mn[2] = 255;
+    m.mx[0] = m.mx[1] = m.mx[2] = 0;
+    m.sum[0] = m.sum[1] = m.sum[2] = 0;
+    m.has_black = false;
+    m.grey = true;
+    int total = 0;
+#pragma unroll 4
+    for (int i = 0; i < 16; i++) {
+        const uint32_t v = px(i);
+        const bool b = black(v);
+        m.has_black |= b;
+        if (ignore_black && b) continue;
+        const int r = cr(v), g = cg(v), bl = cb(v);
+        m.grey &= (r == g) && (r == bl);
+        m.mn[0] = min(m.mn[0], r); m.mn[1] = min(m.mn[1], g); m.mn[2] = min(m.mn[2], bl);
+        m.mx[0] = max(m.mx[0], r); m.mx[1] = max(m.mx[1], g); m.mx[2] = max(m.mx[2], bl);
+        m.sum[0] += r; m.sum[1] += g; m.sum[2] += bl;
+        total++;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; c++) m.av[c] = total > 0 ? (m.sum[c] + total / 2) / total : 0;
+    return m;
+}
+
+// FindSelectors<M>(error_mode), BC1Encoder.cpp:679-779; K is one of the group kernel's kinds
+template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, int hi) {
+    const Pal P = make_pal<IT>(lo, hi, kind_three(K));
+    uint32_t sel = 0, tot = 0;
+    if (K == K_F4_NONE || K == K_F4_FASTER) {
+        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
+        const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
+        const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
+        const int t0 = d0 + d1, t1 = d1 + d2, t2 = d2 + d3;
+#pragma unroll 4
+        for (int i = 0; i < 16; i++) {
+            const uint32_t v = px(i);
+            const int pr = cr(v), pg = cg(v), pb = cb(v);
+            const int dot = 2 * ar * pr + 2 * ag * pg + 2 * ab * pb;
+            const int s = 3 - ((dot <= t0) + (dot < t1) + (dot < t2));
+            if (K == K_F4_FASTER)
+                tot += sq3(pr - sel4(P.r0, P.r1, P.r2, P.r3, s), pg - sel4(P.g0, P.g1, P.g2, P.g3, s),
+                           pb - sel4(P.b0, P.b1, P.b2, P.b3, s));
+            sel |= (uint32_t)s << (2 * i);
+        }
+    } else if (K == K_F4_CHECK2) {
+        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
+        const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
+#pragma unroll 4
+        for (int i = 0; i < 16; i++) {
+            const uint32_t v = px(i);
+            const int pr = cr(v), pg = cg(v), pb = cb(v);
+            const int dd = (pr - P.r0) * ar + (pg - P.g0) * ag + (pb - P.b0) * ab;
+            const float sf = __fadd_rn(__fmul_rn(__int2float_rn(dd), f), 0.5f);
+            const int sl = clampi(f2i_x86(sf), 1, 3);
+            const unsigned e0 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - pr, sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - pg,
+                                    sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - pb);
+            const unsigned e1 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl) - pr, sel4(P.g0, P.g1, P.g2, P.g3, sl) - pg,
+                                    sel4(P.b0, P.b1, P.b2, P.b3, sl) - pb);
+            int s = sl;
+            unsigned e = e1;
+            if (e0 == e1) {
+                if (s == 1) s = 0;
+            } else if (e0 < e) {
+                s = sl - 1;
+                e = e0;
+            }
+            tot += e;
+            sel |= (uint32_t)s << (2 * i);
+        }
+    } else {
+        const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
+        const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
+        const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
+        const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
+#pragma unroll 4
+        for (int i = 0; i < 16; i++) {
+            const uint32_t u = px(i) & 0x00FFFFFFu;
+            const int pp = (int)__dp4a(u, u, 0u);
+            // |p - c|^2 = |p|^2 + |c|^2 - 2 p.c, exact; ties keep the lower index except selector 3 (:762)
+            int e = v0 - 2 * (int)__dp4a(u, c0, 0u), s = 0;
+            const int e1 = v1 - 2 * (int)__dp4a(u, c1, 0u);
+            if (e1 < e) { e = e1; s = 1; }
+            const int e2 = v2 - 2 * (int)__dp4a(u, c2, 0u);
+            if (e2 < e) { e = e2; s = 2; }
+            if (K != K_T3) {
+                const int e3 = v3 - 2 * (int)__dp4a(u, c3, 0u);
+                if (e3 <= e) { e = e3; s = 3; }
+            }
+            tot += (uint32_t)(e + pp);
+            sel |= (uint32_t)s << (2 * i);
+        }
+    }
+    return make_uint2(sel, tot);
+}
+
+template <int IT> __device__ __forceinline__ uint2 fs_any(int K, int lo, int hi) {
+    switch (K) {
+        case K_F4_NONE: return find_selectors<IT, K_F4_NONE>(lo, hi);
+        case K_F4_FASTER: return find_selectors<IT, K_F4_FASTER>(lo, hi);
+        case K_F4_CHECK2: return find_selectors<IT, K_F4_CHECK2>(lo, hi);
+        case K_F4_FULL: return find_selectors<IT, K_F4_FULL>(lo, hi);
+        case K_T3: return find_selectors<IT, K_T3>(lo, hi);
+        default: return find_selectors<IT, K_TB>(lo, hi);
+    }
+}
+
+// error of the endpoints only (the cluster-fit and search trials); same as find_selectors' total
+template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo, int hi, int pp_sum) {
+    const Pal P = make_pal<IT>(lo, hi, kind_three(K));
+    if (K == K_F4_FULL || K == K_T3 || K == K_TB) {
+        const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
+        const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
+        const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
+        const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
+        int t0 = 0, t1 = 0;
+#pragma unroll 2
+        for (int i = 0; i < 16; i += 2) {
+            const uint32_t u = px(i), q = px(i + 1);
+            int m = v0 - 2 * (int)__dp4a(u, c0, 0u), n = v0 - 2 * (int)__dp4a(q, c0, 0u);
+            m = min(m, v1 - 2 * (int)__dp4a(u, c1, 0u));
+            n = min(n, v1 - 2 * (int)__dp4a(q, c1, 0u));
+            m = min(m, v2 - 2 * (int)__dp4a(u, c2, 0u));
+            n = min(n, v2 - 2 * (int)__dp4a(q, c2, 0u));
+            if (K != K_T3) {
+                m = min(m, v3 - 2 * (int)__dp4a(u, c3, 0u));
+                n = min(n, v3 - 2 * (int)__dp4a(q, c3, 0u));
+            }
+            t0 += m;
+            t1 += n;
+        }
+        return (uint32_t)(pp_sum + t0 + t1);
+    }
+    return find_selectors<IT, K>(lo, hi).y;
+}
+
+// FindEndpointsSingleColor(result, pixels, color, is_3color) (BC1Encoder.cpp:458-471)
+template <int IT> __device__ __noinline__ R single_color(int stale_lo, int stale_hi, int ar, int ag, int ab, bool is3) {
+    const Pal P = make_pal<IT>(stale_lo, stale_hi, is3);  // colors[2] is internal index 1
+    uint32_t e = 0;
+#pragma unroll 4
+    for (int i = 0; i < 16; i++) {
+        const uint32_t v = px(i);
+        const int dr = cr(v) - P.r1, dg = cg(v) - P.g1, db = cb(v) - P.b1, da = (int)(v >> 24) - 255;
+        e += (uint32_t)(dr * dr + dg * dg + db * db + da * da);
+    }
+    const uint32_t mr = g_tab.match5[IT][ar], mg = g_tab.match6[IT][ag], mb = g_tab.match5[IT][ab];
+    R r;
+    r.lo = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
+    r.hi = eppack(mr & 0xFF, mg & 0xFF, mb & 0xFF);
+    r.err = e;
+    r.sel = 0x55555555u;
+    r.mode = is3 ? CM_THREE : CM_FOUR;
+    return r;
+}
+
+// FindEndpoints (BC1Encoder.cpp:473-677)
+__device__ __noinline__ int2 find_endpoints(const M &m, int mode, bool ignore_black, int power_iters) {
+    int lo, hi;
+    if (m.grey) {
+        const int fr = cr(px(0));
+        if (m.mx[0] - m.mn[0] < 2) {
+            lo = hi = eppack(s8to5(fr), s8to6(fr), s8to5(fr));
+        } else {
+            lo = eppack(s8to5(m.mn[0]), s8to6(m.mn[0]), s8to5(m.mn[0]));
+            hi = eppack(s8to5(m.mx[0]), s8to6(m.mx[0]), s8to5(m.mx[0]));
+        }
+    } else if (mode == EP_LS) {
+        const int d0 = m.mx[0] - m.mn[0], d1 = m.mx[1] - m.mn[1], d2 = m.mx[2] - m.mn[2];
+        const int c0 = (d0 >= d1 && d0 >= d2) ? 0 : ((d1 >= d2 && d1 >= d0) ? 1 : 2);
+        unsigned sxy0 = 0, sxy1 = 0, sxy2 = 0;  // zero-initialised (:510 is not)
+        for (int i = 0; i < 16; i++) {
+            const uint32_t v = px(i);
+            const int p0 = c0 == 0 ? cr(v) : (c0 == 1 ? cg(v) : cb(v));
+            sxy0 += (unsigned)(p0 * cr(v));
+            sxy1 += (unsigned)(p0 * cg(v));
+            sxy2 += (unsigned)(p0 * cb(v));
+        }
+        const unsigned sxy[3] = {sxy0, sxy1, sxy2};
+        float l[3] = {0.f, 0.f, 0.f}, h[3] = {0.f, 0.f, 0.f};
+        const float mn0 = (float)m.mn[c0];
+        l[c0] = h[c0] = mn0;
+        const unsigned sum_x = (unsigned)m.sum[c0], sum_xx = sxy[c0];
+        const float den = __fsub_rn(__uint2float_rn(16u * sum_xx), __uint2float_rn(sum_x * sum_x));
+        if (fabsf(den) > 1e-8f) {
+            for (int i = 1; i < 3; i++) {
+                const int c = (c0 + i) % 3;
+                const unsigned sum_y = (unsigned)m.sum[c], sum_xy = sxy[c];
+                const float a = __fdiv_rn(__uint2float_rn((16u * sum_xy) - (sum_x * sum_y)), den);
+                const float b = __fdiv_rn(__uint2float_rn((sum_xx * sum_y) - (sum_xy * sum_x)), den);
+                l[c] = __fadd_rn(b, __fmul_rn(a, l[c0]));
+                h[c] = __fadd_rn(b, __fmul_rn(a, h[c0]));
+            }
+        }
+        for (int c = 0; c < 3; c++) {
+            const float inset = __fdiv_rn(__fsub_rn(h[c], l[c]), 16.0f);
+            l[c] = __fdiv_rn(__fadd_rn(l[c], inset), 255.0f);
+            h[c] = __fdiv_rn(__fsub_rn(h[c], inset), 255.0f);
+        }
+        lo = precise_round565(l[0], l[1], l[2], s_mid5, s_mid6);
+        hi = precise_round565(h[0], h[1], h[2], s_mid5, s_mid6);
+    } else if (mode == EP_BB || mode == EP_BBINT) {
+        int cxz = 0, cyz = 0;
+        for (int i = 0; i < 16; i++) {  // b * r - avg.r, as written (:572-573)
+            const uint32_t v = px(i);
+            const int b = cb(v) - m.av[2];
+            cxz += b * cr(v) - m.av[0];
+            cyz += b * cg(v) - m.av[1];
+        }
+        if (mode == EP_BB) {
+            const float bias = __fdiv_rn(8.0f, 255.0f);
+            float l[3], h[3];
+            for (int c = 0; c < 3; c++) {
+                l[c] = __fdiv_rn((float)m.mn[c], 255.0f);
+                h[c] = __fdiv_rn((float)m.mx[c], 255.0f);
+                const float inset = __fdiv_rn(__fsub_rn(__fsub_rn(h[c], l[c]), bias), 16.0f);
+                l[c] = __fadd_rn(l[c], inset);
+                h[c] = __fsub_rn(h[c], inset);
+            }
+            if (cxz < 0) { const float t = l[0]; l[0] = h[0]; h[0] = t; }
+            if (cyz < 0) { const float t = l[1]; l[1] = h[1]; h[1] = t; }
+            lo = precise_round565(l[0], l[1], l[2], s_mid5, s_mid6);
+            hi = precise_round565(h[0], h[1], h[2], s_mid5, s_mid6);
+        } else {
+            int a[3], z[3];
+            for (int c = 0; c < 3; c++) {
+                const int inset = ((m.mx[c] - m.mn[c]) - 8) >> 4;
+                a[c] = clamp255(m.mn[c] + inset);
+                z[c] = clamp255(m.mx[c] - inset);
+            }
+            if (cxz < 0) { const int t = a[0]; a[0] = z[0]; z[0] = t; }
+            if (cyz < 0) { const int t = a[1]; a[1] = z[1]; z[1] = t; }
+            lo = eppack(s8to5(a[0]), s8to6(a[1]), s8to5(a[2]));
+            hi = eppack(s8to5(z[0]), s8to6(z[1]), s8to5(z[2]));
+        }
+    } else {  // PCA
+        int s00 = 0, s01 = 0, s02 = 0, s11 = 0, s12 = 0, s22 = 0;
+        for (int i = 0; i < 16; i++) {
+            const uint32_t v = px(i);
+            if (ignore_black && black(v)) continue;
+            const int dr = cr(v) - m.av[0], dg = cg(v) - m.av[1], db = cb(v) - m.av[2];
+            s00 += dr * dr; s01 += dr * dg; s02 += dr * db; s11 += dg * dg; s12 += dg * db; s22 += db * db;
+        }
+        const float k255 = 255.0f;
+        const float c00 = __fdiv_rn((float)(1 + s00), k255), c01 = __fdiv_rn((float)s01, k255);
+        const float c02 = __fdiv_rn((float)s02, k255), c11 = __fdiv_rn((float)(1 + s11), k255);
+        const float c12 = __fdiv_rn((float)s12, k255), c22 = __fdiv_rn((float)(1 + s22), k255);
+        const float c33 = __fdiv_rn(1.0f, k255), z = __fdiv_rn(0.0f, k255);
+        float d0 = __fsub_rn((float)m.mx[0], (float)m.mn[0]);
+        float d1 = __fsub_rn((float)m.mx[1], (float)m.mn[1]);
+        float d2 = __fsub_rn((float)m.mx[2], (float)m.mn[2]);
+        float d3 = __fsub_rn(0.0f, 0.0f);
+        if (c02 < 0) d0 = -d0;
+        if (c12 < 0) d1 = -d1;
+        for (int it = 0; it < power_iters; it++) {
+            const float n0 = fdot4_rn(d0, d1, d2, d3, c00, c01, c02, z);
+            const float n1 = fdot4_rn(d0, d1, d2, d3, c01, c11, c12, z);
+            const float n2 = fdot4_rn(d0, d1, d2, d3, c02, c12, c22, z);
+            const float n3 = fdot4_rn(d0, d1, d2, d3, z, z, z, c33);
+            d0 = n0; d1 = n1; d2 = n2; d3 = n3;
+        }
+        float k = 0.0f;
+        if (fabsf(d0) > k) k = fabsf(d0);
+        if (fabsf(d1) > k) k = fabsf(d1);
+        if (fabsf(d2) > k) k = fabsf(d2);
+        float a0 = 306.0f, a1 = 601.0f, a2 = 117.0f, a3 = 0.0f;
+        if (k >= 2) {
+            const float s = __fdiv_rn(2048.0f, k);
+            a0 = __fmul_rn(d0, s); a1 = __fmul_rn(d1, s); a2 = __fmul_rn(d2, s); a3 = __fmul_rn(d3, s);
+        }
+        a0 = __fmul_rn(a0, 16.0f); a1 = __fmul_rn(a1, 16.0f); a2 = __fmul_rn(a2, 16.0f); a3 = __fmul_rn(a3, 16.0f);
+        float min_dot = INFINITY, max_dot = -INFINITY;
+        int min_i = 0, max_i = 0;
+        for (int i = 0; i < 16; i++) {
+            const uint32_t v = px(i);
+            if (ignore_black && black(v)) continue;
+            const float dot = fdot4_rn((float)cr(v), (float)cg(v), (float)cb(v), 0.0f, a0, a1, a2, a3);
+            if (dot > max_dot) { max_dot = dot; max_i = i; }
+            if (dot < min_dot) { min_dot = dot; min_i = i; }
+        }
+        const uint32_t pmin = px(min_i), pmax = px(max_i);
+        lo = eppack(s8to5(cr(pmin)), s8to6(cg(pmin)), s8to5(cb(pmin)));
+        hi = eppack(s8to5(cr(pmax)), s8to6(cg(pmax)), s8to5(cb(pmax)));
+    }
+    return make_int2(lo, hi);
+}
+
+// RefineBlockLS<M> with RefineEndpointsLS<FourColor>(pixels) (BC1Encoder.cpp:781-825, 852-875)
+template <int IT, int K> __device__ __noinline__ R refine_ls(R r, const M &m, int passes) {
+    for (int pass = 0; pass < passes; pass++) {
+        R t = r;
+        int q0r = 0, q0g = 0, q0b = 0, n1 = 0, n2 = 0, n3 = 0;
+        for (int i = 0; i < 16; i++) {
+            const uint32_t v = px(i);
+            const int s = (t.sel >> (2 * i)) & 3;
+            q0r += cr(v) * s; q0g += cg(v) * s; q0b += cb(v) * s;
+            n1 += s == 1; n2 += s == 2; n3 += s == 3;
+        }
+        const int n0 = 16 - n1 - n2 - n3;
+        float m0 = (float)(n1 + 4 * n2 + 9 * n3), m1 = (float)(2 * n1 + 2 * n2), m2 = m1, m3 = (float)(9 * n0 + 4 * n1 + n2);
+        const float det = __fsub_rn(__fmul_rn(m0, m3), __fmul_rn(m1, m2));
+        if (fabsf(det) < 1e-8f) {
+            t = single_color<IT>(t.lo, t.hi, m.av[0], m.av[1], m.av[2], kind_three(K));
+        } else {
+            const float tt = m0; m0 = m3; m3 = tt;
+            m1 = -m1;
+            m2 = -m2;
+            const float sc = __fdiv_rn(__fdiv_rn(3.0f, 255.0f), det);
+            m0 = __fmul_rn(m0, sc); m1 = __fmul_rn(m1, sc); m2 = __fmul_rn(m2, sc); m3 = __fmul_rn(m3, sc);
+            const float f0r = (float)q0r, f0g = (float)q0g, f0b = (float)q0b;
+            const float q10r = (float)(m.sum[0] * 3) - f0r, q10g = (float)(m.sum[1] * 3) - f0g, q10b = (float)(m.sum[2] * 3) - f0b;
+            t.lo = precise_round565(__fadd_rn(__fmul_rn(m0, f0r), __fmul_rn(m1, q10r)),
+                                    __fadd_rn(__fmul_rn(m0, f0g), __fmul_rn(m1, q10g)),
+                                    __fadd_rn(__fmul_rn(m0, f0b), __fmul_rn(m1, q10b)), s_mid5, s_mid6);
+            t.hi = precise_round565(__fadd_rn(__fmul_rn(m2, f0r), __fmul_rn(m3, q10r)),
+                                    __fadd_rn(__fmul_rn(m2, f0g), __fmul_rn(m3, q10g)),
+                                    __fadd_rn(__fmul_rn(m2, f0b), __fmul_rn(m3, q10b)), s_mid5, s_mid6);
+            const uint2 se = find_selectors<IT, K>(t.lo, t.hi);
+            t.sel = se.x;
+            t.err = se.y;
+            t.mode = kind_mode(K);
+        }
+        if (t.lo == r.lo && t.hi == r.hi) break;
+        if (K == K_F4_NONE || t.err < r.err) r = t;
+        else break;
+    }
+    return r;
+}
+
+template <int IT> __device__ __forceinline__ R refine_ls_any(int K, R r, const M &m, int passes) {
+    switch (K) {
+        case K_F4_NONE: return refine_ls<IT, K_F4_NONE>(r, m, passes);
+        case K_F4_FASTER: return refine_ls<IT, K_F4_FASTER>(r, m, passes);
+        case K_F4_CHECK2: return refine_ls<IT, K_F4_CHECK2>(r, m, passes);
+        case K_F4_FULL: return refine_ls<IT, K_F4_FULL>(r, m, passes);
+        case K_T3: return refine_ls<IT, K_T3>(r, m, passes);
+        default: return refine_ls<IT, K_TB>(r, m, passes);
+    }
+}
+
+// RefineBlockCF<M> (BC1Encoder.cpp:877-928): the reference's loop as written
+template <int IT, int K> __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool exhaustive, int pp_sum) {
+    constexpr bool four = !kind_three(K);
+    const int tid = threadIdx.x;
+    const R orig = r;
+    const uint32_t w = orig.sel;
+    const int n1 = __popc(w & ~(w >> 1) & 0x55555555u), n2 = __popc(~w & (w >> 1) & 0x55555555u);
+    const int n3 = __popc(w & (w >> 1) & 0x55555555u), n0 = 16 - n1 - n2 - n3;
+    int start;
+    if (four) start = n0 == 16 ? 15 : n1 == 16 ? 700 : n2 == 16 ? 753 : n3 == 16 ? 515 : (int)g_tab.hash4[n0 | (n1 << 4) | (n2 << 8)];
+    else start = n0 == 16 ? 12 : n1 == 16 ? 15 : n2 == 16 ? 89 : (int)g_tab.hash3[n0 | (n1 << 4)];
+    // projection keys, rank by counting (keys are distinct), prefix sums in rank order
+    const int axr = s5to8(epr(orig.hi)) - s5to8(epr(orig.lo));
+    const int axg = s6to8(epg(orig.hi)) - s6to8(epg(orig.lo));
+    const int axb = s5to8(epb(orig.hi)) - s5to8(epb(orig.lo));
+    for (int i = 0; i < 16; i++) {
+        const uint32_t v = px(i);
+        t_key[i][tid] = ((uint32_t)(0x1000000 + cr(v) * axr + cg(v) * axg + cb(v) * axb) << 4) | (uint32_t)i;
+    }
+    for (int i = 0; i < 16; i++) {  // t_srg/t_sb[k] first hold the colour of rank k-1
+        const uint32_t ki = t_key[i][tid];
+        int rank = 0;
+#pragma unroll 4
+        for (int j = 0; j < 16; j++) rank += t_key[j][tid] < ki;
+        const uint32_t v = px(i);
+        t_srg[rank + 1][tid] = (uint32_t)cr(v) | ((uint32_t)cg(v) << 16);
+        t_sb[rank + 1][tid] = (uint16_t)cb(v);
+    }
+    uint32_t arg = 0, ab = 0;
+    t_srg[0][tid] = 0;
+    t_sb[0][tid] = 0;
+    for (int k = 1; k <= 16; k++) {
+        arg += t_srg[k][tid];
+        ab += t_sb[k][tid];
+        t_srg[k][tid] = arg;
+        t_sb[k][tid] = (uint16_t)ab;
+    }
+    const float t16r = (float)(arg & 0xFFFF), t16g = (float)(arg >> 16), t16b = (float)ab;
+    const float denom = four ? 3.0f : 2.0f;
+    const unsigned total = exhaustive ? (four ? 969u : 153u) : orderings;
+    const uint16_t *row = four ? g_tab.best4 + start * 128 : g_tab.best3 + start * 32;
+    bool sc_done = false, from_ls = false;
+    R sc;
+    for (unsigned q = 0; q < total; q++) {
+        const int th = exhaustive ? (int)q : (int)row[q];
+        R t;
+        if (is_single_hash(four, th)) {
+            if (!sc_done) {  // the same trial for every single-colour ordering of this call
+                sc = single_color<IT>(orig.lo, orig.hi, m.av[0], m.av[1], m.av[2], !four);
+                sc.mode = kind_mode(K);
+                sc_done = true;
+            }
+            t = sc;
+        } else {
+            const float4 f = four ? g_tab.factors4[th] : g_tab.factors3[th];
+            const uint32_t o = four ? g_tab.orders4[th] : g_tab.orders3[th];
+            const int l1 = o & 0xFF, l2 = l1 + ((o >> 8) & 0xFF), l3 = l2 + ((o >> 16) & 0xFF);
+            uint32_t qrg = t_srg[l1][tid] + t_srg[l2][tid], qb = (uint32_t)t_sb[l1][tid] + t_sb[l2][tid];
+            if (four) {
+                qrg += t_srg[l3][tid];
+                qb += t_sb[l3][tid];
+            }
+            const float fr = (float)(qrg & 0xFFFF), fg = (float)(qrg >> 16), fb = (float)qb;
+            const float q0r = t16r * denom - fr, q0g = t16g * denom - fg, q0b = t16b * denom - fb;
+            t.lo = precise_round565(__fadd_rn(__fmul_rn(f.x, q0r), __fmul_rn(f.y, fr)),
+                                    __fadd_rn(__fmul_rn(f.x, q0g), __fmul_rn(f.y, fg)),
+                                    __fadd_rn(__fmul_rn(f.x, q0b), __fmul_rn(f.y, fb)), s_mid5, s_mid6);
+            t.hi = precise_round565(__fadd_rn(__fmul_rn(f.z, q0r), __fmul_rn(f.w, fr)),
+                                    __fadd_rn(__fmul_rn(f.z, q0g), __fmul_rn(f.w, fg)),
+                                    __fadd_rn(__fmul_rn(f.z, q0b), __fmul_rn(f.w, fb)), s_mid5, s_mid6);
+            t.err = block_error<IT, K>(t.lo, t.hi, pp_sum);
+            t.sel = 0;  // filled for the winner below
+            t.mode = kind_mode(K);
+        }
+        if (t.err < r.err) {
+            r = t;
+            from_ls = !is_single_hash(four, th);
+        }
+        if (t.err == 0) break;
+    }
+    if (from_ls) r.sel = find_selectors<IT, K>(r.lo, r.hi).x;  // selectors of the winning LS trial
+    return r;
+}
+
+// EndpointSearch (BC1Encoder.cpp:930-996): the reference's sequential loop
+template <int IT, int K> __device__ __noinline__ R endpoint_search(R r, unsigned rounds, int pp_sum) {
+    unsigned prev = 0;
+    int forbidden = -1;
+    bool moved = false;
+    for (unsigned i = 0; i < rounds; i++) {
+        if ((int)(i & 31) == forbidden) continue;
+        const uint16_t vx = s_vox[i & 15];
+        const int ddr = ((int)((unsigned)vx << 30)) >> 30, ddg = ((int)((unsigned)vx << 28)) >> 30;
+        const int ddb = ((int)((unsigned)vx << 26)) >> 30;
+        int lo = r.lo, hi = r.hi;
+        if (i & 16) lo = eppack(clampi(epr(lo) + ddr, 0, 31), clampi(epg(lo) + ddg, 0, 63), clampi(epb(lo) + ddb, 0, 31));
+        else hi = eppack(clampi(epr(hi) + ddr, 0, 31), clampi(epg(hi) + ddg, 0, 63), clampi(epb(hi) + ddb, 0, 31));
+        const uint32_t e = block_error<IT, K>(lo, hi, pp_sum);
+        if (e < r.err) {
+            r.lo = lo;
+            r.hi = hi;
+            r.err = e;
+            forbidden = (int)((vx >> 8) & 15) | (int)(i & 16);
+            prev = i;
+            moved = true;
+        }
+        if (i - prev > 32) break;
+    }
+    if (moved) r.sel = find_selectors<IT, K>(r.lo, r.hi).x;
+    return r;
+}
+
+template <int IT> __device__ __forceinline__ R refine_cf_any(int K, R r, const M &m, unsigned o, bool ex, int pp) {
+    switch (K) {
+        case K_F4_NONE: return refine_cf<IT, K_F4_NONE>(r, m, o, ex, pp);
+        case K_F4_FASTER: return refine_cf<IT, K_F4_FASTER>(r, m, o, ex, pp);
+        case K_F4_CHECK2: return refine_cf<IT, K_F4_CHECK2>(r, m, o, ex, pp);
+        case K_F4_FULL: return refine_cf<IT, K_F4_FULL>(r, m, o, ex, pp);
+        default: return refine_cf<IT, K_T3>(r, m, o, ex, pp);
+    }
+}
+
+template <int IT> __device__ __forceinline__ R search_any(int K, R r, unsigned rounds, int pp) {
+    switch (K) {
+        case K_F4_NONE: return endpoint_search<IT, K_F4_NONE>(r, rounds, pp);
+        case K_F4_FASTER: return endpoint_search<IT, K_F4_FASTER>(r, rounds, pp);
+        case K_F4_CHECK2: return endpoint_search<IT, K_F4_CHECK2>(r, rounds, pp);
+        case K_F4_FULL: return endpoint_search<IT, K_F4_FULL>(r, rounds, pp);
+        case K_T3: return endpoint_search<IT, K_T3>(r, rounds, pp);
+        default: return endpoint_search<IT, K_TB>(r, rounds, pp);
+    }
+}
+
+__device__ __forceinline__ uint2 write(const R &r) {
+    Res g;
+    g.lo = r.lo;
+    g.hi = r.hi;
+    g.sel = r.sel;
+    g.mode = r.mode;
+    g.err = r.err;
+    return write_block(g);
+}
+
+// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342), one thread
+template <int IT> __device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_mode, int pp_sum) {
+    const uint32_t c0 = px(0);
+    bool solid = true;
+    for (int i = 1; i < 16; i++) solid &= px(i) == c0;
+    if (solid) return write_block_solid<IT>(c0);
+
+    const M m = metrics(false);
+    const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
+    bool needs_err = use_likely;
+    needs_err |= color_mode == CM_THREE;
+    needs_err |= (color_mode == CM_TB) && m.has_black;
+    needs_err |= p.error_mode != EM_NONE;
+    needs_err |= p.search_rounds > 0;
+    const int em = needs_err ? p.error_mode : EM_NONE;
+    const int ls_passes = p.two_ls_passes ? 2 : 1, cf_passes = p.two_cf_passes ? 2 : 1;
+    const int ep_passes = (needs_err && p.two_ep_passes) ? 2 : 1;
+    const int k4 = kind_for(CM_FOUR, em);
+
+    R orig = rinit(), res = rinit();
+    for (int round = 0; round < ep_passes; round++) {
+        const int2 ep = find_endpoints(m, round == 1 ? EP_BB : p.endpoint_mode, false, (int)p.power_iterations);
+        R to = rinit();
+        to.lo = ep.x;
+        to.hi = ep.y;
+        R tr = to;
+        const uint2 se = fs_any<IT>(k4, tr.lo, tr.hi);
+        tr.sel = se.x;
+        tr.err = se.y;
+        tr.mode = CM_FOUR;
+        tr = refine_ls_any<IT>(k4, tr, m, ls_passes);
+        if (!needs_err || tr.err < res.err) {
+            res = tr;
+            orig = to;
+        }
+    }
+    if (res.err > 0 && use_likely)
+        for (int it = 0; it < cf_passes; it++)
+            res = refine_cf_any<IT>(kind_for(CM_FOUR, p.error_mode), res, m, p.orderings4, p.exhaustive, pp_sum);
+
+    if (res.err > 0 && (color_mode & CM_THREE)) {
+        R t = orig;
+        const uint2 se = find_selectors<IT, K_T3>(t.lo, t.hi);
+        t.sel = se.x;
+        t.err = se.y;
+        t.mode = CM_THREE;
+        t = refine_ls<IT, K_T3>(t, m, ls_passes);
+        if (t.err > 0 && use_likely)
+            for (int it = 0; it < cf_passes; it++) t = refine_cf<IT, K_T3>(t, m, p.orderings3, p.exhaustive, pp_sum);
+        if (t.err < res.err) res = t;
+    }
+
+    if (res.err > 0 && color_mode == CM_TB && m.has_black && !((m.mx[0] | m.mx[1] | m.mx[2]) < 4)) {
+        const M mnb = metrics(true);
+        const int2 ep = find_endpoints(mnb, EP_PCA, true, (int)p.power_iterations);
+        R t = rinit();
+        t.lo = ep.x;
+        t.hi = ep.y;
+        const uint2 se = find_selectors<IT, K_TB>(t.lo, t.hi);
+        t.sel = se.x;
+        t.err = se.y;
+        t.mode = CM_TB;
+        t = refine_ls<IT, K_TB>(t, mnb, ls_passes);
+        if (t.err < res.err) res = t;
+    }
+
+    if (res.err > 0 && p.search_rounds > 0) {
+        const int Md = res.mode == CM_THREE ? CM_THREE : (res.mode == CM_TB ? CM_TB : CM_FOUR);
+        res = search_any<IT>(kind_for(Md, Md == CM_FOUR ? p.error_mode : EM_FULL), res, p.search_rounds, pp_sum);
+    }
+    return write(res);
+}
+
+}  // namespace tpb
+
+// one block per thread; BC3 adds the BC4 alpha block on channel 3
+template <int IT>
+__global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_thread(const uint8_t *__restrict__ rgba, int w, int h, int bw,
+                                                                   long nblocks, qt_bc1_params p, uint8_t *__restrict__ out,
+                                                                   int bc3, int aligned) {
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+        if (i < 32) s_mid5[i] = c_mid5[i];
+        s_mid6[i] = c_mid6[i];
+        if (i < 16) s_vox[i] = c_voxels[i];
+    }
+    __syncthreads();
+    const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
+    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x) {
+        const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+        uint32_t v[16];
+        load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
+        int pp = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            tpb::t_px[i][threadIdx.x] = v[i];
+            const uint32_t u = v[i] & 0x00FFFFFFu;
+            pp += (int)__dp4a(u, u, 0u);
+        }
+        const uint2 blk = tpb::encode_block<IT>(p, color_mode, pp);
+        if (bc3) {
+#pragma unroll
+            for (int i = 0; i < 16; i++) v[i] = tpb::t_px[i][threadIdx.x];
+            const uint2 a = bc4_block_thread(v, 3);
+            reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
+        } else {
+            reinterpret_cast<uint2 *>(out)[b] = blk;
+        }
+    }
+}

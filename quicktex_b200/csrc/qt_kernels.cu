@@ -34,6 +34,7 @@
 #include <cfloat>
 #include <climits>
 #include <cstdint>
+#include <cstdlib>
 
 #include "qt_internal.h"
 
@@ -1231,6 +1232,8 @@ __global__ void __launch_bounds__(256) k_decode(const uint8_t *__restrict__ bloc
     }
 }
 
+#include "qt_bc1_thread.cuh"
+
 // ---------------------------------------------------------------------------
 // persistent batch kernel: many textures, any format / op / level, one launch
 // ---------------------------------------------------------------------------
@@ -1372,11 +1375,33 @@ int upload_tables(int device) {
     return (int)e;
 }
 
+// BC1 mapping: 0 = one block per thread, 1 = one block per 16-lane group.
+// QT_BC1_MAPPING=thread|group overrides the default for comparison runs.
+static int bc1_mapping() {
+    static int m = -1;
+    if (m < 0) {
+        const char *e = getenv("QT_BC1_MAPPING");
+        m = (e && e[0] == 'g') ? 1 : 0;
+    }
+    return m;
+}
+
 int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3, void *stream) {
     const int bw = (w + 3) / 4, bh = (h + 3) / 4;
     const long n = (long)bw * bh;
-    const int grid = grid_for(n, kGroupsPerCta);
     cudaStream_t s = (cudaStream_t)stream;
+    if (bc1_mapping() == 0) {
+        const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
+        const int g = grid_for(n, tpb::kThreads);
+        switch (p.interpolator) {
+            case IT_IDEAL: k_bc1_thread<IT_IDEAL><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, n, p, out, bc3, aligned); break;
+            case IT_ROUND: k_bc1_thread<IT_ROUND><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, n, p, out, bc3, aligned); break;
+            case IT_NVIDIA: k_bc1_thread<IT_NVIDIA><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, n, p, out, bc3, aligned); break;
+            default: k_bc1_thread<IT_AMD><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, n, p, out, bc3, aligned); break;
+        }
+        return (int)cudaGetLastError();
+    }
+    const int grid = grid_for(n, kGroupsPerCta);
     switch (p.interpolator) {
         case IT_IDEAL: k_bc1_encode<IT_IDEAL><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
         case IT_ROUND: k_bc1_encode<IT_ROUND><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
