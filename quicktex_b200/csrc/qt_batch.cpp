@@ -80,13 +80,14 @@ struct qt_batch {
             for (int f : {1, 3, 4, 5})
                 for (int l = 0; l < kLevels; l++) {
                     Rule &r = rules[rule_index(op, f, l)];
+                    // a warp takes one tile; tiles are multiples of its 32 lanes
                     if (op == QT_OP_DECODE) {
-                        r = {1024, 0.05f};
+                        r = {2048, 0.05f};
                     } else if (f == 4 || f == 5) {
-                        r = {1024, 0.1f};
+                        r = {2048, 0.1f};
                     } else {  // BC1 / BC3 encode: cost grows steeply with the level's cluster fit and search
                         const float c = l >= 17 ? 25.f : l >= 13 ? 15.f : l >= 9 ? 4.f : l >= 7 ? 2.f : l >= 1 ? 1.5f : 1.f;
-                        r = {l >= 13 ? 8u : l >= 7 ? 32u : 128u, c + (f == 3 ? 0.1f : 0.f)};
+                        r = {l >= 13 ? 32u : l >= 7 ? 64u : 256u, c + (f == 3 ? 0.1f : 0.f)};
                     }
                 }
     }

@@ -1183,169 +1183,146 @@ __device__ __forceinline__ void bc4_decode_into(uint2 blk, int ch, uint32_t px[1
 // same wrapped position: source (px, py) is final iff px + w >= 4*bw and
 // py + h >= 4*bh (RawTexture::SetBlock, Texture.h:114-134).
 template <int IT>
+__device__ __forceinline__ void decode_block(const uint8_t *__restrict__ blocks, int w, int h, int bw, int bh, long b,
+                                             int fmt, int write_alpha, int c0, int c1, int aligned,
+                                             uint8_t *__restrict__ rgba) {
+    const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+    uint32_t px[16];
+    if (fmt == 1 || fmt == 3) {
+        const uint2 cb = fmt == 1 ? __ldg(reinterpret_cast<const uint2 *>(blocks) + b)
+                                  : make_uint2(__ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 2),
+                                               __ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 3));
+        uint32_t col[4];
+        bc1_palette<IT>(cb.x & 0xFFFF, cb.x >> 16, fmt == 1, fmt == 1 && write_alpha, col);
+#pragma unroll
+        for (int i = 0; i < 16; i++) {
+            const uint32_t s = (cb.y >> (2 * i)) & 3;
+            px[i] = s == 0 ? col[0] : (s == 1 ? col[1] : (s == 2 ? col[2] : col[3]));
+        }
+        if (fmt == 3) bc4_decode_into(make_uint2(__ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b),
+                                                 __ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 1)), 3, px);
+    } else {
+#pragma unroll
+        for (int i = 0; i < 16; i++) px[i] = 0xFF000000u;  // ColorBlock default texel (0,0,0,255)
+        if (fmt == 4) {
+            bc4_decode_into(__ldg(reinterpret_cast<const uint2 *>(blocks) + b), c0, px);
+        } else {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(blocks) + b);
+            bc4_decode_into(make_uint2(q.x, q.y), c0, px);
+            bc4_decode_into(make_uint2(q.z, q.w), c1, px);
+        }
+    }
+    const bool interior = aligned && bx > 0 && by > 0 && bx * 4 + 4 <= w && by * 4 + 4 <= h;
+    if (interior) {
+#pragma unroll
+        for (int y = 0; y < 4; y++)
+            *reinterpret_cast<uint4 *>(rgba + ((size_t)(by * 4 + y) * w + bx * 4) * 4) =
+                make_uint4(px[4 * y], px[4 * y + 1], px[4 * y + 2], px[4 * y + 3]);
+    } else {
+#pragma unroll
+        for (int y = 0; y < 4; y++)
+#pragma unroll
+            for (int x = 0; x < 4; x++) {
+                const int sx = bx * 4 + x, sy = by * 4 + y;
+                if (sx + w >= 4 * bw && sy + h >= 4 * bh)
+                    *reinterpret_cast<uint32_t *>(rgba + ((size_t)(sy % h) * w + (sx % w)) * 4) = px[4 * y + x];
+            }
+    }
+}
+
+// Decode: every texel of every block is decoded, and a texel is stored only
+// if no later block (in the reference's by, bx, x, y write order) writes the
+// same wrapped position: source (px, py) is final iff px + w >= 4*bw and
+// py + h >= 4*bh (RawTexture::SetBlock, Texture.h:114-134).
+template <int IT>
 __global__ void __launch_bounds__(256) k_decode(const uint8_t *__restrict__ blocks, int w, int h, int bw, int bh,
                                                 long nblocks, int fmt, int write_alpha, int c0, int c1, int aligned,
                                                 uint8_t *__restrict__ rgba) {
-    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x) {
-        const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
-        uint32_t px[16];
-        if (fmt == 1 || fmt == 3) {
-            const uint2 cb = fmt == 1 ? __ldg(reinterpret_cast<const uint2 *>(blocks) + b)
-                                      : make_uint2(__ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 2),
-                                                   __ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 3));
-            uint32_t col[4];
-            bc1_palette<IT>(cb.x & 0xFFFF, cb.x >> 16, fmt == 1, fmt == 1 && write_alpha, col);
-#pragma unroll
-            for (int i = 0; i < 16; i++) {
-                const uint32_t s = (cb.y >> (2 * i)) & 3;
-                px[i] = s == 0 ? col[0] : (s == 1 ? col[1] : (s == 2 ? col[2] : col[3]));
-            }
-            if (fmt == 3) bc4_decode_into(make_uint2(__ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b),
-                                                     __ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 1)), 3, px);
-        } else {
-#pragma unroll
-            for (int i = 0; i < 16; i++) px[i] = 0xFF000000u;  // ColorBlock default texel (0,0,0,255)
-            if (fmt == 4) {
-                bc4_decode_into(__ldg(reinterpret_cast<const uint2 *>(blocks) + b), c0, px);
-            } else {
-                const uint4 q = __ldg(reinterpret_cast<const uint4 *>(blocks) + b);
-                bc4_decode_into(make_uint2(q.x, q.y), c0, px);
-                bc4_decode_into(make_uint2(q.z, q.w), c1, px);
-            }
-        }
-        const bool interior = aligned && bx > 0 && by > 0 && bx * 4 + 4 <= w && by * 4 + 4 <= h;
-        if (interior) {
-#pragma unroll
-            for (int y = 0; y < 4; y++)
-                *reinterpret_cast<uint4 *>(rgba + ((size_t)(by * 4 + y) * w + bx * 4) * 4) =
-                    make_uint4(px[4 * y], px[4 * y + 1], px[4 * y + 2], px[4 * y + 3]);
-        } else {
-#pragma unroll
-            for (int y = 0; y < 4; y++)
-#pragma unroll
-                for (int x = 0; x < 4; x++) {
-                    const int sx = bx * 4 + x, sy = by * 4 + y;
-                    if (sx + w >= 4 * bw && sy + h >= 4 * bh)
-                        *reinterpret_cast<uint32_t *>(rgba + ((size_t)(sy % h) * w + (sx % w)) * 4) = px[4 * y + x];
-                }
-        }
-    }
+    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x)
+        decode_block<IT>(blocks, w, h, bw, bh, b, fmt, write_alpha, c0, c1, aligned, rgba);
 }
 
 #include "qt_bc1_thread.cuh"
 
 // ---------------------------------------------------------------------------
-// persistent batch kernel: many textures, any format / op / level, one launch
+// persistent batch kernel: many textures, any format / op / level, one launch.
+// A warp claims one tile (consecutive blocks of one texture) at a time; its
+// lanes take the tile's blocks, one block per thread.
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ uint32_t bc4_texel(uint2 blk, int i) {
-    uint32_t v[8];
-    bc4_values(blk.x & 0xFF, (blk.x >> 8) & 0xFF, v);
-    const uint64_t bits = ((uint64_t)blk.y << 16) | (blk.x >> 16);
-    const uint32_t s = (uint32_t)(bits >> (3 * i)) & 7u;
-    uint32_t val = v[0];
-#pragma unroll
-    for (int k = 1; k < 8; k++) val = s == (uint32_t)k ? v[k] : val;
-    return val;
+template <int IT> __device__ __noinline__ uint2 encode_bc1_batch(const qt_bc1_params *p, int color_mode, int pp) {
+    return tpb::encode_block<IT>(*p, color_mode, pp);
 }
 
-// texel `i` of block `b` of a BC1/BC3/BC4/BC5 texture (the decoders of k_decode, per texel)
-template <int IT>
-__device__ __forceinline__ uint32_t decode_texel(const uint8_t *blocks, int fmt, long b, int i, int write_alpha, int c0, int c1) {
-    if (fmt == 1 || fmt == 3) {
-        const uint32_t *w = reinterpret_cast<const uint32_t *>(blocks) + (fmt == 1 ? 2 * b : 4 * b + 2);
-        const uint32_t x = __ldg(w), y = __ldg(w + 1);
-        uint32_t col[4];
-        bc1_palette<IT>(x & 0xFFFF, x >> 16, fmt == 1, fmt == 1 && write_alpha, col);
-        const uint32_t s = (y >> (2 * i)) & 3;
-        uint32_t px = s == 0 ? col[0] : (s == 1 ? col[1] : (s == 2 ? col[2] : col[3]));
-        if (fmt == 3) {
-            const uint32_t *a = reinterpret_cast<const uint32_t *>(blocks) + 4 * b;
-            px = (px & 0x00FFFFFFu) | (bc4_texel(make_uint2(__ldg(a), __ldg(a + 1)), i) << 24);
-        }
-        return px;
-    }
-    uint32_t px = 0xFF000000u;  // ColorBlock default texel (0, 0, 0, 255)
-    const uint32_t *w = reinterpret_cast<const uint32_t *>(blocks) + (fmt == 4 ? 2 * b : 4 * b);
-    px = (px & ~(0xFFu << (8 * c0))) | (bc4_texel(make_uint2(__ldg(w), __ldg(w + 1)), i) << (8 * c0));
-    if (fmt == 5) px = (px & ~(0xFFu << (8 * c1))) | (bc4_texel(make_uint2(__ldg(w + 2), __ldg(w + 3)), i) << (8 * c1));
-    return px;
-}
-
-template <int IT> __device__ __noinline__ uint2 encode_bc1_batch(const qt_bc1_params *p, int color_mode) {
-    return encode_bc1_group<IT>(grp(), *p, color_mode);
-}
-
-__device__ __forceinline__ void batch_block(const Grp &G, const BatchItemDev &__restrict__ I, long b) {
-    const int by = (int)(b / I.bw), bx = (int)(b - (long)by * I.bw);
-    int sx = bx * 4 + (G.lane & 3), sy = by * 4 + (G.lane >> 2);
+__device__ __forceinline__ void batch_block(const BatchItemDev &__restrict__ I, long b) {
+    const bool aligned = ((I.w & 3) == 0) && ((reinterpret_cast<uintptr_t>(I.op == QT_OP_ENCODE ? I.src : I.dst) & 15) == 0);
     if (I.op == QT_OP_DECODE) {
-        uint32_t px;
         switch (I.interp) {
-            case IT_IDEAL: px = decode_texel<IT_IDEAL>(I.src, I.fmt, b, G.lane, I.write_alpha, I.c0, I.c1); break;
-            case IT_ROUND: px = decode_texel<IT_ROUND>(I.src, I.fmt, b, G.lane, I.write_alpha, I.c0, I.c1); break;
-            case IT_NVIDIA: px = decode_texel<IT_NVIDIA>(I.src, I.fmt, b, G.lane, I.write_alpha, I.c0, I.c1); break;
-            default: px = decode_texel<IT_AMD>(I.src, I.fmt, b, G.lane, I.write_alpha, I.c0, I.c1); break;
+            case IT_IDEAL: decode_block<IT_IDEAL>(I.src, I.w, I.h, I.bw, I.bh, b, I.fmt, I.write_alpha, I.c0, I.c1, aligned, I.dst); break;
+            case IT_ROUND: decode_block<IT_ROUND>(I.src, I.w, I.h, I.bw, I.bh, b, I.fmt, I.write_alpha, I.c0, I.c1, aligned, I.dst); break;
+            case IT_NVIDIA: decode_block<IT_NVIDIA>(I.src, I.w, I.h, I.bw, I.bh, b, I.fmt, I.write_alpha, I.c0, I.c1, aligned, I.dst); break;
+            default: decode_block<IT_AMD>(I.src, I.w, I.h, I.bw, I.bh, b, I.fmt, I.write_alpha, I.c0, I.c1, aligned, I.dst); break;
         }
-        if (sx + I.w >= 4 * I.bw && sy + I.h >= 4 * I.bh)  // the texel no later block overwrites (Texture.h:114-134)
-            *reinterpret_cast<uint32_t *>(I.dst + ((size_t)(sy % I.h) * I.w + (sx % I.w)) * 4) = px;
         return;
     }
-    if (sx >= I.w) sx %= I.w;
-    if (sy >= I.h) sy %= I.h;
-    const uint32_t v = *reinterpret_cast<const uint32_t *>(I.src + ((size_t)sy * I.w + sx) * 4);
-    const float fr = (float)(v & 0xFF), fg = (float)((v >> 8) & 0xFF), fb = (float)((v >> 16) & 0xFF);
-    s_px[G.g][G.lane] = v;
-    s_pf[G.g][G.lane] = make_float4(fr, fg, fb, fr * fr + fg * fg + fb * fb);
-    const unsigned pp = gsum(G.gm, sq3((int)(v & 0xFF), (int)((v >> 8) & 0xFF), (int)((v >> 16) & 0xFF)));
-    if (G.lane == 0) s_pp[G.g] = (int)pp;
-    __syncwarp(G.gm);
-    if (I.fmt == 1 || I.fmt == 3) {
-        const int cm = I.fmt == 3 ? CM_FOUR : I.p.color_mode;  // BC3Encoder.h:39-40
-        uint2 blk;
-        switch (I.p.interpolator) {
-            case IT_IDEAL: blk = encode_bc1_batch<IT_IDEAL>(&I.p, cm); break;
-            case IT_ROUND: blk = encode_bc1_batch<IT_ROUND>(&I.p, cm); break;
-            case IT_NVIDIA: blk = encode_bc1_batch<IT_NVIDIA>(&I.p, cm); break;
-            default: blk = encode_bc1_batch<IT_AMD>(&I.p, cm); break;
-        }
-        if (I.fmt == 3) {
-            const uint2 a = encode_bc4_group(G, 3);
-            if (G.lane == 0) reinterpret_cast<uint4 *>(I.dst)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
-        } else if (G.lane == 0) {
-            reinterpret_cast<uint2 *>(I.dst)[b] = blk;
-        }
-    } else {
-        const uint2 a = encode_bc4_group(G, I.c0);
+    const int by = (int)(b / I.bw), bx = (int)(b - (long)by * I.bw);
+    uint32_t v[16];
+    load_block_thread(I.src, I.w, I.h, bx, by, aligned && (bx * 4 + 4 <= I.w) && (by * 4 + 4 <= I.h), v);
+    if (I.fmt == 4 || I.fmt == 5) {
+        const uint2 a = bc4_block_thread(v, I.c0);
         if (I.fmt == 5) {
-            const uint2 c = encode_bc4_group(G, I.c1);
-            if (G.lane == 0) reinterpret_cast<uint4 *>(I.dst)[b] = make_uint4(a.x, a.y, c.x, c.y);
-        } else if (G.lane == 0) {
+            const uint2 c = bc4_block_thread(v, I.c1);
+            reinterpret_cast<uint4 *>(I.dst)[b] = make_uint4(a.x, a.y, c.x, c.y);
+        } else {
             reinterpret_cast<uint2 *>(I.dst)[b] = a;
         }
+        return;
     }
-    __syncwarp(G.gm);
+    int pp = 0;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        tpb::t_px[i][threadIdx.x] = v[i];
+        const uint32_t u = v[i] & 0x00FFFFFFu;
+        pp += (int)__dp4a(u, u, 0u);
+    }
+    const int cm = I.fmt == 3 ? CM_FOUR : I.p.color_mode;  // BC3Encoder.h:39-40
+    uint2 blk;
+    switch (I.p.interpolator) {
+        case IT_IDEAL: blk = encode_bc1_batch<IT_IDEAL>(&I.p, cm, pp); break;
+        case IT_ROUND: blk = encode_bc1_batch<IT_ROUND>(&I.p, cm, pp); break;
+        case IT_NVIDIA: blk = encode_bc1_batch<IT_NVIDIA>(&I.p, cm, pp); break;
+        default: blk = encode_bc1_batch<IT_AMD>(&I.p, cm, pp); break;
+    }
+    if (I.fmt == 3) {
+#pragma unroll
+        for (int i = 0; i < 16; i++) v[i] = tpb::t_px[i][threadIdx.x];
+        const uint2 a = bc4_block_thread(v, 3);
+        reinterpret_cast<uint4 *>(I.dst)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
+    } else {
+        reinterpret_cast<uint2 *>(I.dst)[b] = blk;
+    }
 }
 
-// ctl[0] is the queue head (atomically advanced by each group), ctl[1] the number of tiles.
-__global__ void __launch_bounds__(128, 6) k_batch(const BatchItemDev *__restrict__ items, const TileDev *__restrict__ tiles,
-                                                  uint32_t *__restrict__ ctl) {
+// ctl[0] is the queue head (atomically advanced by each warp), ctl[1] the number of tiles.
+__global__ void __launch_bounds__(tpb::kThreads, 4) k_batch(const BatchItemDev *__restrict__ items,
+                                                            const TileDev *__restrict__ tiles, uint32_t *__restrict__ ctl) {
     for (int i = threadIdx.x; i < 64; i += blockDim.x) {
         if (i < 32) s_mid5[i] = c_mid5[i];
         s_mid6[i] = c_mid6[i];
         if (i < 16) s_vox[i] = c_voxels[i];
     }
     __syncthreads();
-    const Grp G = grp();
+    const int lane = threadIdx.x & 31;
     const uint32_t ntiles = ctl[1];
     while (true) {
         uint32_t t = 0;
-        if (G.lane == 0) t = atomicAdd(&ctl[0], 1u);
-        t = __shfl_sync(G.gm, t, 0, 16);
+        if (lane == 0) t = atomicAdd(&ctl[0], 1u);
+        t = __shfl_sync(0xFFFFFFFFu, t, 0);
         if (t >= ntiles) break;
         const TileDev T = tiles[t];
         // the descriptor stays in (L1-cached) global memory: copying it to registers spills
         const BatchItemDev &I = items[T.item];
-        for (uint32_t k = 0; k < T.count; k++) batch_block(G, I, (long)T.start + k);
+        for (uint32_t k = lane; k < T.count; k += 32) batch_block(I, (long)T.start + k);
+        __syncwarp();
     }
 }
 
@@ -1415,13 +1392,13 @@ int batch_sms() { return num_sms(); }
 
 int batch_ctas_per_sm() {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch, 128, 0) != cudaSuccess || n <= 0) n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch, tpb::kThreads, 0) != cudaSuccess || n <= 0) n = 1;
     return n;
 }
 
 int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, void *stream) {
     if (grid <= 0) grid = num_sms() * batch_ctas_per_sm();
-    k_batch<<<grid, 128, 0, (cudaStream_t)stream>>>(items, tiles, ctl);
+    k_batch<<<grid, tpb::kThreads, 0, (cudaStream_t)stream>>>(items, tiles, ctl);
     return (int)cudaGetLastError();
 }
 

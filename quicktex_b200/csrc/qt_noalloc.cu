@@ -53,7 +53,7 @@ uint32_t h_ctl[2];
 // tile size and relative per-block cost of an item, from the work its settings imply
 void tile_rule(const qt_batch_item &it, uint32_t *tile_blocks, float *cost) {
     if (it.op != QT_OP_ENCODE || it.format == 4 || it.format == 5) {
-        *tile_blocks = 1024;
+        *tile_blocks = 2048;
         *cost = it.op == QT_OP_ENCODE ? 0.1f : 0.05f;
         return;
     }
@@ -64,7 +64,7 @@ void tile_rule(const qt_batch_item &it, uint32_t *tile_blocks, float *cost) {
     else if (p.orderings4 >= 9) c = 4.f;
     else if (p.orderings4 >= 4) c = 2.f;
     *cost = c;
-    *tile_blocks = c >= 15.f ? 8u : c >= 2.f ? 32u : 128u;
+    *tile_blocks = c >= 15.f ? 32u : c >= 2.f ? 64u : 256u;
 }
 
 int check_item(const qt_batch_item &it) {
