@@ -72,6 +72,50 @@ CONFIG = {
 }
 
 
+# DRAM bytes per block of the BC1 kernel, from the ncu capture summarised in
+# profiles/k_bc1_thread_L18_1024sq_full.md (dram__bytes_read.sum + dram__bytes_write.sum
+# = 4,691,456 B for 65,536 blocks); a full 4096^2 launch is that times 1,048,576 blocks.
+BC1_DRAM_BYTES_PER_BLOCK = (4662272 + 29184) / 65536
+
+
+def measure_hbm_paths(dev, stream):
+    """The bandwidth-bound kernels on 16384^2 textures (1 GiB of texels, far larger than L2):
+    BC4 and BC5 encode, BC1 and BC4 decode; achieved = algorithmic bytes / CUDA-event time."""
+    import torch
+
+    from quicktex_b200 import capi
+
+    side = 16384
+    nb = (side // 4) ** 2
+    rng = np.random.default_rng(7)
+    tex = torch.from_numpy(rng.integers(0, 256, side * side * 4, dtype=np.uint8)).to(dev)
+    blocks16 = torch.empty(nb * 16, dtype=torch.uint8, device=dev)
+    out = torch.empty(side * side * 4, dtype=torch.uint8, device=dev)
+    sptr = stream.cuda_stream
+    L = capi.lib()
+    cases = {
+        "bc4_encode": (lambda: capi.check(L.qt_bc4_encode_device(capi._vp(tex.data_ptr()), side, side, 0, capi._vp(blocks16.data_ptr()), capi._vp(sptr))), nb * (64 + 8)),
+        "bc5_encode": (lambda: capi.check(L.qt_bc5_encode_device(capi._vp(tex.data_ptr()), side, side, 0, 1, capi._vp(blocks16.data_ptr()), capi._vp(sptr))), nb * (64 + 16)),
+        "bc1_decode": (lambda: capi.check(L.qt_bc1_decode_device(capi._vp(blocks16.data_ptr()), side, side, 0, 0, capi._vp(out.data_ptr()), capi._vp(sptr))), nb * (8 + 64)),
+        "bc4_decode": (lambda: capi.check(L.qt_bc4_decode_device(capi._vp(blocks16.data_ptr()), side, side, 0, capi._vp(out.data_ptr()), capi._vp(sptr))), nb * (8 + 64)),
+    }
+    res = {}
+    for name, (fn, nbytes) in cases.items():
+        fn()
+        fn()
+        ts = []
+        for _ in range(5):
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            fn()
+            b.record(stream)
+            b.synchronize()
+            ts.append(a.elapsed_time(b))
+        ms = float(np.median(ts))
+        res[name] = {"ms": ms, "gb_s": nbytes / (ms / 1e3) / 1e9, "mblocks_s": nb / (ms / 1e3) / 1e6}
+    return res
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -304,7 +348,8 @@ def run_ours(args, world, rank, local):
         "dtype": "u8", "data": "synthetic (seeded PCG64 block mix; no public corpus exists)", "config": CONFIG,
         "roofline": {
             "bound": "fp32_issue", "achieved": achieved, "peak": peak_tops, "unit": "Tlane-op/s",
-            "frac": achieved / peak_tops, "traffic": None,
+            "frac": achieved / peak_tops, "traffic": BC1_DRAM_BYTES_PER_BLOCK * NB,
+            "traffic_source": "ncu dram bytes of a 1024^2 L18 launch, scaled to this launch's blocks",
             "kernel": "qtk::k_bc1_encode (all 36 settings)",
             "work": "10 lane-ops x oracle-counted candidate evaluations per block",
             "peak_source": f"{sms} SMs x 128 lanes x sm_max_mhz ({peaks_kind})",
@@ -315,6 +360,10 @@ def run_ours(args, world, rank, local):
         "gpu_launches": len(SETTINGS) * args.steps,
         "clocks": clk.summary(),
     }
+    peaks_hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm = measure_hbm_paths(dev, stream)
+    line["hbm_paths"] = {k: dict(v, frac_of_hbm=v["gb_s"] / peaks_hbm) for k, v in hbm.items()}
+    line["hbm_paths"]["peak_gb_s"] = peaks_hbm
     if not args.no_batch:
         line["batched"] = measure_batched(args, dev, world)
     if not args.no_serve and world == 1:
