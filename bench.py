@@ -190,14 +190,9 @@ def dist_init(args):
 
 
 def reduce_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from quicktex_b200.shard import max_over_ranks
 
-    t = torch.tensor([x], device="cuda", dtype=torch.float64)
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return max_over_ranks(x) if world > 1 else x
 
 
 def barrier(world: int):
@@ -387,10 +382,16 @@ def measure_batched(args, dev, world):
     import quicktex_b200.synth as syn
     from quicktex_b200.batch import Arena, Batch, Job, run_plain, run_plain_host
 
+    from quicktex_b200.shard import block_cost, max_over_ranks, shard
+
     items = syn.mixed_batch(args.batch_count)
+    all_blocks = sum(((i.width + 3) // 4) * ((i.height + 3) // 4) for i in items)
     pools = syn.MixedBatchPools()
     jobs = [Job.encode(i.fmt, pools.texture(i), i.width, i.height, level=i.level, channel=0, chan0=0, chan1=1)
             for i in items]
+    if world > 1:  # each rank encodes its cost-balanced share of the same batch
+        rank = int(os.environ.get("RANK", "0"))
+        jobs = [jobs[k] for k in shard(items, world, rank, lambda i: block_cost(i.width, i.height, i.fmt, i.level))]
     del pools
     nblocks = sum(j.nblocks for j in jobs)
     arena = Arena(jobs, dev.index)
@@ -436,18 +437,20 @@ def measure_batched(args, dev, world):
     t0 = time.perf_counter()
     run_plain_host(arena)
     plain_e2e = (time.perf_counter() - t0) * 1e3
-    pm, qm, em = float(np.median(persistent)), float(np.median(plain)), float(np.median(e2e_ms))
+    pm, qm, em = (max_over_ranks(float(np.median(x))) for x in (persistent, plain, e2e_ms))
+    plain_e2e = max_over_ranks(plain_e2e)
     ntiles = batch.last_tiles()
     batch.close()
     return {
         "workload": f"{len(jobs)} textures, log-uniform 4..2048 sides (25% not multiples of 4), "
                     "BC1:BC3:BC4:BC5 = 4:3:2:1, levels {0,5,10,18}, encode",
-        "blocks": nblocks,
-        "persistent_mblocks_s": world * nblocks / (pm / 1e3) / 1e6,
-        "plain_mblocks_s": world * nblocks / (qm / 1e3) / 1e6,
+        "blocks": all_blocks,
+        "scaling": "strong (the batch is sharded across ranks)" if world > 1 else "single GPU",
+        "persistent_mblocks_s": all_blocks / (pm / 1e3) / 1e6,
+        "plain_mblocks_s": all_blocks / (qm / 1e3) / 1e6,
         "persistent_over_plain": qm / pm,
-        "persistent_e2e_mblocks_s": world * nblocks / (em / 1e3) / 1e6,
-        "plain_e2e_mblocks_s": world * nblocks / (plain_e2e / 1e3) / 1e6,
+        "persistent_e2e_mblocks_s": all_blocks / (em / 1e3) / 1e6,
+        "plain_e2e_mblocks_s": all_blocks / (plain_e2e / 1e3) / 1e6,
         "persistent_over_plain_e2e": plain_e2e / em,
         "e2e_h2d_bytes": arena.in_bytes, "e2e_d2h_bytes": arena.out_bytes,
         "ms": {"persistent": pm, "plain": qm, "persistent_e2e": em, "plain_e2e": plain_e2e},
