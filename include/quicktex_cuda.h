@@ -184,6 +184,21 @@ int qt_batch_set_grid(qt_batch *b, int ctas_per_sm);
 int qt_batch_run(qt_batch *b, const qt_batch_item *items, size_t n, void *stream);
 /* Number of tiles the last qt_batch_run queued. */
 size_t qt_batch_last_tiles(const qt_batch *b);
+/* Size the queue for up to `items` textures and `tiles` tiles now, so that later
+ * runs within those limits never reallocate it (a reallocation waits for the
+ * device and re-captures the graph). Never shrinks the queue. */
+int qt_batch_reserve(qt_batch *b, size_t items, size_t tiles);
+
+/* Many copies in one call (serving front ends staging request payloads): one
+ * cudaMemcpyAsync per entry on `stream`, direction taken from the pointers
+ * (cudaMemcpyDefault). Host memory should be pinned for the copies to be
+ * asynchronous. No counterpart in the reference. */
+typedef struct qt_copy {
+    void *dst;
+    const void *src;
+    size_t bytes;
+} qt_copy;
+int qt_copy_async(const qt_copy *copies, size_t n, void *stream);
 
 /* ---- the batched path without device allocation (no counterpart in the reference) ----
  *

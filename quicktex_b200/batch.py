@@ -3,8 +3,8 @@
 Many textures of uneven sizes, formats (BC1/BC3/BC4/BC5), operations
 (encode/decode) and levels run as ONE persistent kernel launch replayed from a
 CUDA graph: each texture is cut into tiles of consecutive blocks, the tiles are
-queued heaviest-first in device memory, and 16-lane groups pull tiles until the
-queue is empty. Tile sizes and per-block costs per (op, format, level) come from
+queued heaviest-first in device memory, and warps pull tiles (one block per
+lane) until the queue is empty. Tile sizes and per-block costs per (op, format, level) come from
 the tuning table written by ``quicktex_b200.autotune`` (``data/batch_tuning.json``).
 
 Every output is byte-identical to the single-texture entry points: the batch
@@ -43,6 +43,9 @@ class BatchItem(ctypes.Structure):
     ]
 
 
+ITEM_DTYPE = np.dtype(BatchItem)  # the same layout as a numpy record
+
+
 class TileRule(ctypes.Structure):
     """``qt_tile_rule``."""
 
@@ -64,7 +67,10 @@ def _lib():
         L.qt_batch_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_size_t, ctypes.c_void_p]
         L.qt_batch_last_tiles.argtypes = [ctypes.c_void_p]
         L.qt_batch_last_tiles.restype = ctypes.c_size_t
-        for n in ("qt_batch_create", "qt_batch_destroy", "qt_batch_set_rules", "qt_batch_set_grid", "qt_batch_run"):
+        L.qt_batch_reserve.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
+        L.qt_copy_async.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        for n in ("qt_batch_create", "qt_batch_destroy", "qt_batch_set_rules", "qt_batch_set_grid", "qt_batch_run",
+                  "qt_batch_reserve", "qt_copy_async"):
             getattr(L, n).restype = ctypes.c_int
         _sigs_done = True
     return L
@@ -106,8 +112,17 @@ class Batch:
     def set_grid(self, ctas_per_sm: int) -> None:
         capi.check(_lib().qt_batch_set_grid(self.handle, ctas_per_sm))
 
-    def run(self, items: Sequence[BatchItem], stream: int = 0) -> None:
-        arr = (BatchItem * max(1, len(items)))(*items)
+    def reserve(self, items: int, tiles: int) -> None:
+        """Size the queue now so runs within these limits never reallocate it."""
+        capi.check(_lib().qt_batch_reserve(self.handle, items, tiles))
+
+    def run(self, items, stream: int = 0) -> None:
+        """``items``: a sequence of ``BatchItem`` or an ``ITEM_DTYPE`` array."""
+        if isinstance(items, np.ndarray):
+            assert items.dtype == ITEM_DTYPE and items.flags.c_contiguous
+            arr = ctypes.cast(ctypes.c_void_p(items.ctypes.data), ctypes.POINTER(BatchItem))
+        else:
+            arr = (BatchItem * max(1, len(items)))(*items)
         capi.check(_lib().qt_batch_run(self.handle, arr, len(items), ctypes.c_void_p(stream)))
 
     def last_tiles(self) -> int:
@@ -173,6 +188,32 @@ class Job:
             it.params = self.params
         it.chan0, it.chan1, it.interpolator, it.write_alpha = self.chan0, self.chan1, self.interpolator, int(self.write_alpha)
         return it
+
+    def record(self) -> np.void:
+        """This job's ``qt_batch_item`` as an ``ITEM_DTYPE`` record with NULL buffers (cached)."""
+        r = self.__dict__.get("_record")
+        if r is None:
+            r = np.frombuffer(bytes(self.item(0, 0)), ITEM_DTYPE)[0]
+            self.__dict__["_record"] = r
+        return r
+
+
+def items_array(jobs: Sequence[Job], src, dst) -> np.ndarray:
+    """``qt_batch_item`` array for ``jobs`` with buffer addresses ``src``/``dst`` (sequences of ints)."""
+    arr = np.empty(len(jobs), ITEM_DTYPE)
+    for k, j in enumerate(jobs):
+        arr[k] = j.record()
+    arr["src"] = src
+    arr["dst"] = dst
+    return arr
+
+
+def copy_async(copies: np.ndarray, stream: int = 0) -> None:
+    """``copies``: uint64 array of shape (n, 3) rows (dst, src, bytes); one
+    cudaMemcpyAsync per row on ``stream`` (``qt_copy_async``)."""
+    c = np.ascontiguousarray(copies, np.uint64)
+    assert c.ndim == 2 and c.shape[1] == 3
+    capi.check(_lib().qt_copy_async(ctypes.c_void_p(c.ctypes.data), len(c), ctypes.c_void_p(stream)))
 
 
 def _align(n: int, a: int = 256) -> int:

@@ -224,6 +224,27 @@ int qt_batch_set_grid(qt_batch *b, int ctas_per_sm) {
 
 size_t qt_batch_last_tiles(const qt_batch *b) { return b ? b->last_tiles : 0; }
 
+int qt_copy_async(const qt_copy *copies, size_t n, void *stream) {
+    if (n && !copies) return qtk::set_error(QT_ERR_ARG, "copies is NULL");
+    for (size_t i = 0; i < n; i++) {
+        if (!copies[i].bytes) continue;
+        if (!copies[i].dst || !copies[i].src) return qtk::set_error(QT_ERR_ARG, "qt_copy_async: NULL buffer");
+        const cudaError_t e = cudaMemcpyAsync(copies[i].dst, copies[i].src, copies[i].bytes, cudaMemcpyDefault,
+                                              (cudaStream_t)stream);
+        if (e != cudaSuccess) return qtk::cuda_error((int)e, "qt_copy_async");
+    }
+    return QT_OK;
+}
+
+int qt_batch_reserve(qt_batch *b, size_t items, size_t tiles) {
+    if (!b) return qtk::set_error(QT_ERR_ARG, "NULL argument");
+    std::lock_guard<std::mutex> lk(b->mu);
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cur != b->device) return qtk::set_error(QT_ERR_STATE, "qt_batch_reserve: the batch belongs to another device");
+    return grow(b, std::max<size_t>(items, b->cap_items), std::max<size_t>(tiles, b->cap_tiles));
+}
+
 int qt_batch_run(qt_batch *b, const qt_batch_item *items, size_t n, void *stream) {
     if (!b || (n && !items)) return qtk::set_error(QT_ERR_ARG, "NULL argument");
     std::lock_guard<std::mutex> lk(b->mu);

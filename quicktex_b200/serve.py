@@ -14,7 +14,10 @@ runs them through the batched persistent path:
   the GPU are admitted as soon as a slot and memory free up, and their work
   overlaps on the device with the batches still running.
 * **Resident buffers.** Nothing is allocated per request: device memory is
-  carved from the arena, host staging is pinned and reused.
+  carved from the arena, each slot's queue is sized for the largest batch at
+  start-up (``qt_batch_reserve``), and the download buffer is pinned and reused.
+  Request payloads are copied straight from the caller's buffers (pinned for
+  asynchronous copies) by ``qt_copy_async``, one call per batch.
 
 The integer block output does not depend on what else is in a batch: every
 request's bytes equal those of the single-texture call (tests check this).
@@ -30,7 +33,15 @@ from typing import Optional
 
 import numpy as np
 
-from .batch import Batch, BatchItem, Job
+from .batch import Batch, Job, copy_async, items_array
+
+
+def _event(stream):
+    import torch
+
+    e = torch.cuda.Event()
+    e.record(stream)
+    return e
 
 
 class DeviceArena:
@@ -93,21 +104,33 @@ class _Slot:
         self.event = None
         self.reqs: list[Request] = []
         self.region = None  # (offset, nbytes) in the arena
-        self.h_out = None
+        self.h_out = None  # pinned download buffer, reused
+        self.h_out_np = None
+
+    def host_out(self, n: int) -> np.ndarray:
+        import torch
+
+        if self.h_out is None or self.h_out.numel() < n:
+            self.h_out = torch.empty(max(n, 1 << 20) * 2, dtype=torch.uint8).pin_memory()
+            self.h_out_np = self.h_out.numpy()
+        return self.h_out_np
 
 
 class Server:
     """Continuous-batching encode/decode server on one GPU."""
 
     def __init__(self, device: int = 0, memory_budget: int = 16 << 30, slots: int = 3,
-                 max_batch_blocks: int = 1 << 22, tuning=None):
+                 max_batch_blocks: int = 1 << 22, max_batch_requests: int = 8192, tuning=None):
         import torch
 
         torch.cuda.set_device(device)
         self.device = device
         self.arena = DeviceArena(memory_budget, device)
         self.slots = [_Slot(device, tuning) for _ in range(slots)]
+        for s in self.slots:  # queues sized for the largest batch up front: no reallocation while serving
+            s.batch.reserve(max_batch_requests, max_batch_blocks // 32 + max_batch_requests)
         self.max_batch_blocks = max_batch_blocks
+        self.max_batch_requests = max_batch_requests
         self.pending: collections.deque[Request] = collections.deque()
         self.cv = threading.Condition()
         self.running = True
@@ -128,6 +151,16 @@ class Server:
             self.cv.notify()
         return r.future
 
+    def submit_many(self, jobs, t_arrivals) -> list:
+        """``submit`` for several requests under one lock."""
+        reqs = [Request(j, t) for j, t in zip(jobs, t_arrivals)]
+        for r in reqs:
+            r.future.request = r
+        with self.cv:
+            self.pending.extend(reqs)
+            self.cv.notify()
+        return [r.future for r in reqs]
+
     def close(self) -> None:
         with self.cv:
             self.running = False
@@ -138,37 +171,40 @@ class Server:
 
     # ---- worker ---------------------------------------------------------------
     def _launch(self, slot: _Slot, reqs: list[Request]) -> None:
-        import torch
-
-        n_in = sum(DeviceArena.ALIGN * ((r.job.data.nbytes + 255) // 256) for r in reqs)
-        n_out = sum(DeviceArena.ALIGN * ((r.job.out_bytes + 255) // 256) for r in reqs)
+        """One batch on ``slot``'s stream: payload uploads (one copy per request,
+        issued from C), one persistent launch, one download of all outputs."""
+        n = len(reqs)
+        jobs = [r.job for r in reqs]
+        in_b = np.fromiter((j.data.nbytes for j in jobs), np.int64, n)
+        out_b = np.fromiter((j.out_bytes for j in jobs), np.int64, n)
+        a = DeviceArena.ALIGN
+        in_al, out_al = (in_b + a - 1) // a * a, (out_b + a - 1) // a * a
+        in_off, out_off = np.cumsum(in_al) - in_al, np.cumsum(out_al) - out_al
+        n_in, n_out = int(in_al.sum()), int(out_al.sum())
         off = self.arena.alloc(n_in + n_out)
         assert off is not None  # reserved by the caller
         base = self.arena.base + off
-        items = []
-        pi, po = 0, n_in
-        with torch.cuda.stream(slot.stream):
-            for r in reqs:
-                j = r.job
-                r.in_off, r.out_off = pi, po - n_in
-                src = self.arena.buf[off + pi: off + pi + j.data.nbytes]
-                src.copy_(torch.from_numpy(j.data), non_blocking=True)
-                items.append(j.item(base + pi, base + po))
-                pi += DeviceArena.ALIGN * ((j.data.nbytes + 255) // 256)
-                po += DeviceArena.ALIGN * ((j.out_bytes + 255) // 256)
-            slot.batch.run(items, slot.stream.cuda_stream)
-            if slot.h_out is None or slot.h_out.numel() < n_out:
-                slot.h_out = torch.empty(max(n_out, 1 << 20) * 2, dtype=torch.uint8).pin_memory()
-            slot.h_out[:n_out].copy_(self.arena.buf[off + n_in: off + n_in + n_out], non_blocking=True)
-            slot.event = torch.cuda.Event()
-            slot.event.record(slot.stream)
+        src = (base + in_off).astype(np.uint64)
+        dst = (base + n_in + out_off).astype(np.uint64)
+        copies = np.empty((n, 3), np.uint64)
+        copies[:, 0] = src
+        copies[:, 1] = np.fromiter((j.data.ctypes.data for j in jobs), np.uint64, n)
+        copies[:, 2] = in_b
+        host = slot.host_out(n_out)
+        stream = slot.stream.cuda_stream
+        copy_async(copies, stream)
+        slot.batch.run(items_array(jobs, src, dst), stream)
+        copy_async(np.array([[host.ctypes.data, base + n_in, n_out]], np.uint64), stream)
+        slot.event = _event(slot.stream)
+        for r, o in zip(reqs, out_off.tolist()):
+            r.out_off = o
         slot.reqs = reqs
         slot.region = (off, n_in + n_out)
         self.batches += 1
 
     def _complete(self, slot: _Slot) -> None:
         t = time.perf_counter()
-        host = slot.h_out.numpy()
+        host = slot.h_out_np
         for r in slot.reqs:
             out = host[r.out_off: r.out_off + r.job.out_bytes].tobytes()
             r.t_done = t
@@ -185,7 +221,7 @@ class Server:
         while self.pending:
             r = self.pending[0]
             need = DeviceArena.ALIGN * ((r.job.data.nbytes + 255) // 256 + (r.job.out_bytes + 255) // 256)
-            if reqs and (blocks + r.job.nblocks > self.max_batch_blocks):
+            if reqs and (blocks + r.job.nblocks > self.max_batch_blocks or len(reqs) >= self.max_batch_requests):
                 break
             if nbytes + need > min(free, largest):
                 break

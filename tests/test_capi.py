@@ -71,6 +71,16 @@ def test_argument_errors():
     assert lib.qt_bc1_encode_device(None, 4, 4, ctypes.byref(good), None, None) == capi.QT_ERR_ARG
     # misaligned device pointers are rejected before any launch
     assert lib.qt_bc1_encode_device(ctypes.c_void_p(4096 + 2), 4, 4, ctypes.byref(good), ctypes.c_void_p(8192), None) == capi.QT_ERR_ARG
+    # batch helpers check their arguments before touching a device
+    from quicktex_b200 import batch
+
+    L = batch._lib()
+    assert L.qt_batch_reserve(None, 1, 1) == capi.QT_ERR_ARG
+    assert L.qt_copy_async(None, 1, None) == capi.QT_ERR_ARG
+    assert L.qt_copy_async(None, 0, None) == capi.QT_OK
+    rows = np.array([[0, 4096, 16]], np.uint64)
+    assert L.qt_copy_async(ctypes.c_void_p(rows.ctypes.data), 1, None) == capi.QT_ERR_ARG
+    assert b"NULL" in lib.qt_last_error()
 
 
 def test_error_message_is_thread_local():

@@ -111,3 +111,48 @@ def test_batch_rejects_bad_items():
     with pytest.raises(capi.QtError):
         b.run([it])
     b.close()
+
+
+def test_reserve_and_record_arrays():
+    """A reserved queue runs batches within its size without reallocating, and
+    items given as an ITEM_DTYPE array run exactly like BatchItem lists."""
+    import torch
+
+    from quicktex_b200.batch import items_array
+
+    jobs, refs = make_jobs(7, 60)
+    b = Batch(0)
+    b.reserve(4096, 1 << 16)
+    b.reserve(16, 16)  # never shrinks
+    arena = Arena(jobs)
+    arena.upload()
+    s = torch.cuda.current_stream()
+    arr = items_array(jobs, [it.src for it in arena.items()], [it.dst for it in arena.items()])
+    b.run(arr, s.cuda_stream)
+    arena.download()
+    s.synchronize()
+    for o, r in zip(arena.outputs(), refs):
+        assert o == single(r)
+    b.close()
+
+
+def test_copy_async_round_trip():
+    import torch
+
+    from quicktex_b200.batch import copy_async
+
+    rng = np.random.default_rng(11)
+    sizes = [1, 7, 256, 4096, 100_003, 0]
+    h_in = torch.empty(sum(sizes) + 4096, dtype=torch.uint8).pin_memory()
+    h_out = torch.zeros_like(h_in).pin_memory()
+    h_in.numpy()[:] = rng.integers(0, 256, h_in.numel(), dtype=np.uint8)
+    d = torch.empty(h_in.numel(), dtype=torch.uint8, device="cuda")
+    s = torch.cuda.current_stream()
+    rows, o = [], 0
+    for n in sizes:
+        rows.append([d.data_ptr() + o, h_in.data_ptr() + o, n])
+        o += n
+    copy_async(np.array(rows, np.uint64), s.cuda_stream)
+    copy_async(np.array([[h_out.data_ptr(), d.data_ptr(), o]], np.uint64), s.cuda_stream)
+    s.synchronize()
+    assert np.array_equal(h_out.numpy()[:o], h_in.numpy()[:o])
