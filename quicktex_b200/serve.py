@@ -86,13 +86,17 @@ class DeviceArena:
 
 
 class Request:
-    __slots__ = ("job", "future", "t_arrival", "t_done", "in_off", "out_off", "nbytes")
+    __slots__ = ("job", "future", "t_arrival", "t_done", "out", "out_off")
 
-    def __init__(self, job: Job, t_arrival: float):
+    def __init__(self, job: Job, t_arrival: float, out: Optional[np.ndarray] = None):
+        if out is not None and (out.dtype != np.uint8 or out.nbytes < job.out_bytes or not out.flags.c_contiguous):
+            raise ValueError(f"out must be a contiguous uint8 array of at least {job.out_bytes} bytes")
         self.job = job
         self.future = concurrent.futures.Future()
         self.t_arrival = t_arrival
         self.t_done = None
+        self.out = out
+        self.out_off = 0
 
 
 class _Slot:
@@ -141,19 +145,23 @@ class Server:
         self.worker.start()
 
     # ---- client side --------------------------------------------------------
-    def submit(self, job: Job, t_arrival: Optional[float] = None) -> concurrent.futures.Future:
-        """Queue a request; the future resolves to its output bytes. ``t_arrival``
-        (perf_counter seconds) defaults to now; latency is measured from it."""
-        r = Request(job, time.perf_counter() if t_arrival is None else t_arrival)
+    def submit(self, job: Job, t_arrival: Optional[float] = None, out: Optional[np.ndarray] = None
+               ) -> concurrent.futures.Future:
+        """Queue a request. ``t_arrival`` (perf_counter seconds) defaults to now;
+        latency is measured from it. Without ``out`` the future resolves to the
+        output as ``bytes``; with ``out`` (a uint8 array, pinned for an
+        asynchronous copy) the result is copied from the device straight into it
+        and the future resolves to ``out[:job.out_bytes]``."""
+        r = Request(job, time.perf_counter() if t_arrival is None else t_arrival, out)
         r.future.request = r
         with self.cv:
             self.pending.append(r)
             self.cv.notify()
         return r.future
 
-    def submit_many(self, jobs, t_arrivals) -> list:
+    def submit_many(self, jobs, t_arrivals, outs=None) -> list:
         """``submit`` for several requests under one lock."""
-        reqs = [Request(j, t) for j, t in zip(jobs, t_arrivals)]
+        reqs = [Request(j, t, o) for j, t, o in zip(jobs, t_arrivals, outs if outs is not None else [None] * len(jobs))]
         for r in reqs:
             r.future.request = r
         with self.cv:
@@ -171,8 +179,8 @@ class Server:
 
     # ---- worker ---------------------------------------------------------------
     def _launch(self, slot: _Slot, reqs: list[Request]) -> None:
-        """One batch on ``slot``'s stream: payload uploads (one copy per request,
-        issued from C), one persistent launch, one download of all outputs."""
+        """One batch on ``slot``'s stream: payload uploads and result downloads
+        (one copy per request each, issued from C), one persistent launch."""
         n = len(reqs)
         jobs = [r.job for r in reqs]
         in_b = np.fromiter((j.data.nbytes for j in jobs), np.int64, n)
@@ -190,14 +198,19 @@ class Server:
         copies[:, 0] = src
         copies[:, 1] = np.fromiter((j.data.ctypes.data for j in jobs), np.uint64, n)
         copies[:, 2] = in_b
-        host = slot.host_out(n_out)
         stream = slot.stream.cuda_stream
         copy_async(copies, stream)
         slot.batch.run(items_array(jobs, src, dst), stream)
-        copy_async(np.array([[host.ctypes.data, base + n_in, n_out]], np.uint64), stream)
-        slot.event = _event(slot.stream)
-        for r, o in zip(reqs, out_off.tolist()):
+        # results: into the request's own buffer, else into the slot's pinned buffer
+        host = slot.host_out(n_out)
+        hbase = host.ctypes.data
+        copies[:, 1] = dst
+        copies[:, 2] = out_b
+        for k, (r, o) in enumerate(zip(reqs, out_off.tolist())):
             r.out_off = o
+            copies[k, 0] = hbase + o if r.out is None else r.out.ctypes.data
+        copy_async(copies, stream)
+        slot.event = _event(slot.stream)
         slot.reqs = reqs
         slot.region = (off, n_in + n_out)
         self.batches += 1
@@ -206,7 +219,8 @@ class Server:
         t = time.perf_counter()
         host = slot.h_out_np
         for r in slot.reqs:
-            out = host[r.out_off: r.out_off + r.job.out_bytes].tobytes()
+            n = r.job.out_bytes
+            out = host[r.out_off: r.out_off + n].tobytes() if r.out is None else r.out[:n]
             r.t_done = t
             self.blocks_done += r.job.nblocks
             r.future.set_result(out)

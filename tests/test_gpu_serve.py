@@ -71,3 +71,34 @@ def test_requests_arriving_while_busy_are_admitted():
     srv.close()
     assert outs == run_jobs(jobs)
     assert srv.batches >= 2
+
+
+def test_results_into_caller_buffers():
+    """Requests with a response buffer (pinned or pageable) get the same bytes
+    written straight into it; requests without one still get bytes."""
+    import torch
+
+    jobs = _jobs(4, 50)
+    ref = run_jobs(jobs)
+    pinned = torch.empty(sum(j.out_bytes + 256 for j in jobs), dtype=torch.uint8).pin_memory().numpy()
+    outs, o = [], 0
+    for k, j in enumerate(jobs):
+        if k % 3 == 0:
+            outs.append(None)
+        elif k % 3 == 1:
+            outs.append(pinned[o:o + j.out_bytes + 256])
+            o += j.out_bytes + 256
+        else:
+            outs.append(np.empty(j.out_bytes, np.uint8))
+    srv = Server(memory_budget=64 << 20, slots=2, max_batch_blocks=8192)
+    futs = srv.submit_many(jobs, [time.perf_counter()] * len(jobs), outs)
+    got = [f.result(timeout=120) for f in futs]
+    srv.close()
+    for g, r, out in zip(got, ref, outs):
+        if out is None:
+            assert isinstance(g, bytes) and g == r
+        else:
+            assert g.base is out or g is out or np.shares_memory(g, out)
+            assert g.tobytes() == r
+    with pytest.raises(ValueError):
+        Server.submit(srv, jobs[0], out=np.empty(1, np.uint8))
