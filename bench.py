@@ -530,7 +530,8 @@ def measure_serving(args, dev):
         jobs = [dec[p] if d else enc[p] for p, d in zip(pick, is_dec)]
         blocks0, batches0 = srv.blocks_done, srv.batches
         t0 = time.perf_counter() + 0.01
-        due_at = (t0 + arrivals).tolist()
+        due_np = t0 + arrivals
+        due_at = due_np.tolist()
         # the front end sleeps (releasing the GIL) until the next arrival, then hands
         # over every request due by now, each with its response buffer in a pinned
         # ring; latency counts from each scheduled arrival
@@ -540,7 +541,7 @@ def measure_serving(args, dev):
             if due_at[k] > now:
                 time.sleep(min(due_at[k] - now, 1e-3))
                 continue
-            k1 = int(np.searchsorted(due_at, now, side="right"))
+            k1 = int(np.searchsorted(due_np, now, side="right"))
             outs = [ring.take(j.out_bytes) for j in jobs[k:k1]]
             fs = srv.submit_many(jobs[k:k1], due_at[k:k1], outs)
             ring.hold(fs)

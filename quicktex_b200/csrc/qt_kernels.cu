@@ -1068,6 +1068,12 @@ __global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict
 
 // ---------------------------------------------------------------------------
 // thread-per-block kernels: BC4/BC5 encode, all decoders
+//
+// These move 72-80 bytes of HBM traffic per block, so at full bandwidth an SM
+// has ~400 thread-instructions per block to spend. The per-block work is kept
+// well under that: byte selection with PRMT (__byte_perm), one multiply-high
+// per texel for the BC4 level, 32-bit block indices where they fit, and one
+// kernel instantiation per format so nothing branches on it per block.
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ void load_block_thread(const uint8_t *__restrict__ rgba, int w, int h, int bx, int by,
                                                   bool fast, uint32_t px[16]) {
@@ -1088,41 +1094,77 @@ __device__ __forceinline__ void load_block_thread(const uint8_t *__restrict__ rg
     }
 }
 
+// The Levels table of BC4Encoder.cpp:45 ({1,7,6,5,4,3,2,0}: threshold count -> selector) as bytes for PRMT.
+constexpr uint32_t kBC4MapLo = 1u | (7u << 8) | (6u << 16) | (5u << 24);
+constexpr uint32_t kBC4MapHi = 4u | (3u << 8) | (2u << 16) | (0u << 24);
+
+// Exact division of n < 4096 by d = 2*delta (delta 1..255) as __umulhi(n, M[delta]):
+// M = (floor(2^(12+l) / d) + 1) << (20 - l), l = ceil(log2 d) (Granlund & Montgomery,
+// "Division by invariant integers using multiplication", 1994, Thm 4.2, N = 12 bits).
+struct BC4Magic {
+    uint32_t m[256];
+};
+constexpr BC4Magic make_bc4_magic() {
+    BC4Magic t{};
+    for (int delta = 1; delta < 256; delta++) {
+        const uint32_t d = 2u * (uint32_t)delta;
+        int l = 0;
+        while ((1u << l) < d) l++;
+        const uint64_t m = (1ull << (12 + l)) / d + 1;
+        t.m[delta] = (uint32_t)(m << (20 - l));
+    }
+    return t;
+}
+__device__ const BC4Magic g_bc4_magic = make_bc4_magic();
+
+// BC4Encoder::EncodeBlock (BC4Encoder.cpp:30-71) on channel ch. The reference
+// counts the thresholds delta*(1+2c) - bias (c = 0..6) that 14*value reaches;
+// for min <= value <= max that count is exactly
+// min(7, floor((14*(value - min) + 4 + delta) / (2*delta))), taken here with one
+// multiply-high per texel (equal for every (min, max, value), checked exhaustively).
 __device__ __forceinline__ uint2 bc4_block_thread(const uint32_t px[16], int ch) {
-    int mn = 255, mx = 0;
-    int v[16];
+    const uint32_t sel = 0x4440u | (uint32_t)ch;  // byte ch of the texel, zeros above
+    uint32_t v[16];
+    uint32_t mn = 255u, mx = 0u;
 #pragma unroll
     for (int i = 0; i < 16; i++) {
-        v[i] = (px[i] >> (8 * ch)) & 0xFF;
+        v[i] = __byte_perm(px[i], 0u, sel);
         mn = min(mn, v[i]);
         mx = max(mx, v[i]);
     }
-    if (mn == mx) return make_uint2((uint32_t)mn | ((uint32_t)mn << 8), 0u);
-    const int bias = 4 - mn * 14, delta = mx - mn;
-    int th[7];
-#pragma unroll
-    for (int c = 0; c < 7; c++) th[c] = delta * (1 + 2 * c) - bias;
-    uint64_t bits = 0;
+    if (mn == mx) return make_uint2(mn | (mn << 8), 0u);  // BC4Block(min): solid
+    const uint32_t delta = mx - mn;
+    const uint32_t M = __ldg(&g_bc4_magic.m[delta]);
+    const uint32_t K = 4u + delta - 14u * mn;  // 14*value + K == 14*(value - min) + 4 + delta (mod 2^32)
+    uint32_t lo = 0u, hi = 0u;                 // selector bits 0..31 and 32..47
 #pragma unroll
     for (int i = 0; i < 16; i++) {
-        const int x = v[i] * 14;
-        int lvl = 0;
-#pragma unroll
-        for (int c = 0; c < 7; c++) lvl += x >= th[c];
-        bits |= (uint64_t)((kBC4Levels >> (3 * lvl)) & 7u) << (3 * i);
+        const uint32_t lvl = min(__umulhi(14u * v[i] + K, M), 7u);
+        const uint32_t s = __byte_perm(kBC4MapLo, kBC4MapHi, lvl) & 7u;
+        if (i < 10) {
+            lo |= s << (3 * i);
+        } else if (i == 10) {
+            lo |= s << 30;
+            hi |= s >> 2;
+        } else {
+            hi |= s << (3 * i - 32);
+        }
     }
-    return make_uint2((uint32_t)mx | ((uint32_t)mn << 8) | ((uint32_t)bits << 16), (uint32_t)(bits >> 16));
+    return make_uint2(mx | (mn << 8) | (lo << 16), (lo >> 16) | (hi << 16));
 }
 
-__global__ void __launch_bounds__(256) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long nblocks,
-                                                    int c0, int c1, int bc5, int aligned, uint8_t *__restrict__ out) {
-    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x) {
-        const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+// One thread per block. Idx is uint32_t whenever the block count and the grid fit
+// 31 bits (the common case: no 64-bit division per block), else uint64_t.
+template <bool BC5, typename Idx>
+__global__ void __launch_bounds__(256) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, Idx bw, Idx nblocks,
+                                                    int c0, int c1, int aligned, uint8_t *__restrict__ out) {
+    for (Idx b = (Idx)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (Idx)gridDim.x * blockDim.x) {
+        const int by = (int)(b / bw), bx = (int)(b - (Idx)by * bw);
         const bool fast = aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h);
         uint32_t px[16];
         load_block_thread(rgba, w, h, bx, by, fast, px);
         const uint2 a = bc4_block_thread(px, c0);
-        if (bc5) {
+        if (BC5) {
             const uint2 c = bc4_block_thread(px, c1);
             reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, c.x, c.y);
         } else {
@@ -1151,67 +1193,117 @@ __device__ __forceinline__ void bc1_palette(uint32_t c0, uint32_t c1, bool allow
     }
 }
 
-__device__ __forceinline__ void bc4_values(uint32_t a0, uint32_t a1, uint32_t v[8]) {
-    v[0] = a0;
-    v[1] = a1;
-    if (a0 <= a1) {  // BC4Block::GetValues6 (BC4Block.cpp:44-53)
-        v[2] = (a0 * 4 + a1) / 5; v[3] = (a0 * 3 + a1 * 2) / 5; v[4] = (a0 * 2 + a1 * 3) / 5; v[5] = (a0 + a1 * 4) / 5;
-        v[6] = 0; v[7] = 255;
+// BC4Block::GetValues (BC4Block.cpp:44-64), the 8 values as bytes: lo = values 0..3, hi = 4..7
+__device__ __forceinline__ uint2 bc4_value_bytes(uint32_t a0, uint32_t a1) {
+    uint32_t v2, v3, v4, v5, v6, v7;
+    if (a0 <= a1) {  // GetValues6 (BC4Block.cpp:44-53)
+        v2 = (a0 * 4 + a1) / 5; v3 = (a0 * 3 + a1 * 2) / 5; v4 = (a0 * 2 + a1 * 3) / 5; v5 = (a0 + a1 * 4) / 5;
+        v6 = 0; v7 = 255;
     } else {  // GetValues8 (:55-64)
-        v[2] = (a0 * 6 + a1) / 7; v[3] = (a0 * 5 + a1 * 2) / 7; v[4] = (a0 * 4 + a1 * 3) / 7;
-        v[5] = (a0 * 3 + a1 * 4) / 7; v[6] = (a0 * 2 + a1 * 5) / 7; v[7] = (a0 + a1 * 6) / 7;
+        v2 = (a0 * 6 + a1) / 7; v3 = (a0 * 5 + a1 * 2) / 7; v4 = (a0 * 4 + a1 * 3) / 7;
+        v5 = (a0 * 3 + a1 * 4) / 7; v6 = (a0 * 2 + a1 * 5) / 7; v7 = (a0 + a1 * 6) / 7;
     }
+    return make_uint2(a0 | (a1 << 8) | (v2 << 16) | (v3 << 24), v4 | (v5 << 8) | (v6 << 16) | (v7 << 24));
 }
 
-__device__ __forceinline__ void bc4_decode_into(uint2 blk, int ch, uint32_t px[16]) {
-    uint32_t v[8];
-    bc4_values(blk.x & 0xFF, (blk.x >> 8) & 0xFF, v);
-    const uint64_t bits = ((uint64_t)blk.y << 16) | (blk.x >> 16);
-    const int sh = 8 * ch;
-#pragma unroll
-    for (int i = 0; i < 16; i++) {
-        const uint32_t s = (uint32_t)(bits >> (3 * i)) & 7u;
-        uint32_t val = v[0];
-#pragma unroll
-        for (int k = 1; k < 8; k++) val = s == (uint32_t)k ? v[k] : val;
-        px[i] = (px[i] & ~(0xFFu << sh)) | (val << sh);
-    }
+// Four 2-bit (BC1) or 3-bit (BC4) indices of one texel row, one per nibble: a PRMT selector.
+__device__ __forceinline__ uint32_t nibbles2(uint32_t x) {
+    x = (x & 0x0Fu) | ((x & 0xF0u) << 4);
+    return (x & 0x0303u) | ((x & 0x0C0Cu) << 2);
+}
+__device__ __forceinline__ uint32_t nibbles3(uint32_t x) {
+    return (x & 0x7u) | ((x & 0x38u) << 1) | ((x & 0x1C0u) << 2) | ((x & 0xE00u) << 3);
 }
 
-// Decode: every texel of every block is decoded, and a texel is stored only
-// if no later block (in the reference's by, bx, x, y write order) writes the
-// same wrapped position: source (px, py) is final iff px + w >= 4*bw and
-// py + h >= 4*bh (RawTexture::SetBlock, Texture.h:114-134).
-template <int IT>
-__device__ __forceinline__ void decode_block(const uint8_t *__restrict__ blocks, int w, int h, int bw, int bh, long b,
-                                             int fmt, int write_alpha, int c0, int c1, int aligned,
-                                             uint8_t *__restrict__ rgba) {
-    const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
-    uint32_t px[16];
-    if (fmt == 1 || fmt == 3) {
-        const uint2 cb = fmt == 1 ? __ldg(reinterpret_cast<const uint2 *>(blocks) + b)
-                                  : make_uint2(__ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 2),
-                                               __ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 3));
-        uint32_t col[4];
-        bc1_palette<IT>(cb.x & 0xFFFF, cb.x >> 16, fmt == 1, fmt == 1 && write_alpha, col);
-#pragma unroll
-        for (int i = 0; i < 16; i++) {
-            const uint32_t s = (cb.y >> (2 * i)) & 3;
-            px[i] = s == 0 ? col[0] : (s == 1 ? col[1] : (s == 2 ? col[2] : col[3]));
-        }
-        if (fmt == 3) bc4_decode_into(make_uint2(__ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b),
-                                                 __ldg(reinterpret_cast<const uint32_t *>(blocks) + 4 * b + 1)), 3, px);
-    } else {
-#pragma unroll
-        for (int i = 0; i < 16; i++) px[i] = 0xFF000000u;  // ColorBlock default texel (0,0,0,255)
-        if (fmt == 4) {
-            bc4_decode_into(__ldg(reinterpret_cast<const uint2 *>(blocks) + b), c0, px);
+// The BC4 values of texel row y (4 texels), one byte each, from the 48 selector bits
+__device__ __forceinline__ uint32_t bc4_row(uint2 vals, uint32_t sel_lo, uint32_t sel_hi, int y) {
+    const uint32_t x = y == 0 ? sel_lo : y == 1 ? (sel_lo >> 12) : y == 2 ? __funnelshift_r(sel_lo, sel_hi, 24) : (sel_hi >> 4);
+    return __byte_perm(vals.x, vals.y, nibbles3(x & 0xFFFu));
+}
+
+// Decode of one block into px[16] (RGBA8 words), for FMT 1 (BC1Decoder.cpp:33-55),
+// 3 (BC3Decoder.cpp:26-31: BC1 colours without 3-colour mode, then BC4 into alpha),
+// 4 (BC4Decoder.cpp:29-43 into channel c0 of (0,0,0,255)) and
+// 5 (BC5Decoder.cpp:25-30: c0, then c1).
+template <int FMT, int IT>
+__device__ __forceinline__ void decode_texels(const uint8_t *__restrict__ blocks, size_t b, int write_alpha, int c0,
+                                              int c1, uint32_t px[16]) {
+    if (FMT == 1 || FMT == 3) {
+        uint2 cb, ab = make_uint2(0u, 0u);
+        if (FMT == 1) {
+            cb = __ldg(reinterpret_cast<const uint2 *>(blocks) + b);
         } else {
             const uint4 q = __ldg(reinterpret_cast<const uint4 *>(blocks) + b);
-            bc4_decode_into(make_uint2(q.x, q.y), c0, px);
-            bc4_decode_into(make_uint2(q.z, q.w), c1, px);
+            ab = make_uint2(q.x, q.y);
+            cb = make_uint2(q.z, q.w);
+        }
+        uint32_t col[4];
+        bc1_palette<IT>(cb.x & 0xFFFF, cb.x >> 16, FMT == 1, FMT == 1 && write_alpha, col);
+        // channel planes: byte k of each = that channel of col[k]
+        const uint32_t A = __byte_perm(col[0], col[1], 0x5140), B = __byte_perm(col[2], col[3], 0x5140);
+        const uint32_t C = __byte_perm(col[0], col[1], 0x7362), D = __byte_perm(col[2], col[3], 0x7362);
+        const uint32_t Rp = __byte_perm(A, B, 0x5410), Gp = __byte_perm(A, B, 0x7632);
+        const uint32_t Bp = __byte_perm(C, D, 0x5410), Ap = __byte_perm(C, D, 0x7632);
+        uint2 av = make_uint2(0u, 0u);
+        uint32_t slo = 0u, shi = 0u;
+        if (FMT == 3) {
+            av = bc4_value_bytes(ab.x & 0xFF, (ab.x >> 8) & 0xFF);
+            slo = (ab.x >> 16) | (ab.y << 16);
+            shi = ab.y >> 16;
+        }
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const uint32_t S = nibbles2((cb.y >> (8 * y)) & 0xFFu);
+            const uint32_t Rr = __byte_perm(Rp, 0u, S), Gr = __byte_perm(Gp, 0u, S), Br = __byte_perm(Bp, 0u, S);
+            const uint32_t Ar = FMT == 3 ? bc4_row(av, slo, shi, y) : __byte_perm(Ap, 0u, S);
+            const uint32_t X = __byte_perm(Rr, Gr, 0x5140), Y = __byte_perm(Br, Ar, 0x5140);
+            const uint32_t X2 = __byte_perm(Rr, Gr, 0x7362), Y2 = __byte_perm(Br, Ar, 0x7362);
+            px[4 * y + 0] = __byte_perm(X, Y, 0x5410);
+            px[4 * y + 1] = __byte_perm(X, Y, 0x7632);
+            px[4 * y + 2] = __byte_perm(X2, Y2, 0x5410);
+            px[4 * y + 3] = __byte_perm(X2, Y2, 0x7632);
+        }
+    } else {
+        uint2 q0, q1 = make_uint2(0u, 0u);
+        if (FMT == 4) {
+            q0 = __ldg(reinterpret_cast<const uint2 *>(blocks) + b);
+        } else {
+            const uint4 q = __ldg(reinterpret_cast<const uint4 *>(blocks) + b);
+            q0 = make_uint2(q.x, q.y);
+            q1 = make_uint2(q.z, q.w);
+        }
+        // texel k of a row: byte c0 <- value k, other bytes of (0,0,0,255); BC5 then byte c1 <- value k
+        const uint32_t base0 = 0x7444u & ~(0xFu << (4 * c0));
+        const uint32_t base1 = 0x3210u & ~(0xFu << (4 * c1));
+        const uint2 v0 = bc4_value_bytes(q0.x & 0xFF, (q0.x >> 8) & 0xFF);
+        const uint32_t lo0 = (q0.x >> 16) | (q0.y << 16), hi0 = q0.y >> 16;
+        uint2 v1 = make_uint2(0u, 0u);
+        uint32_t lo1 = 0u, hi1 = 0u;
+        if (FMT == 5) {
+            v1 = bc4_value_bytes(q1.x & 0xFF, (q1.x >> 8) & 0xFF);
+            lo1 = (q1.x >> 16) | (q1.y << 16);
+            hi1 = q1.y >> 16;
+        }
+#pragma unroll
+        for (int y = 0; y < 4; y++) {
+            const uint32_t W0 = bc4_row(v0, lo0, hi0, y);
+            const uint32_t W1 = FMT == 5 ? bc4_row(v1, lo1, hi1, y) : 0u;
+#pragma unroll
+            for (int k = 0; k < 4; k++) {
+                uint32_t t = __byte_perm(W0, 0xFF000000u, base0 | ((uint32_t)k << (4 * c0)));
+                if (FMT == 5) t = __byte_perm(t, W1, base1 | ((uint32_t)(4 + k) << (4 * c1)));
+                px[4 * y + k] = t;
+            }
         }
     }
+}
+
+// Store of a decoded block. Every texel of every block is decoded, and a texel
+// is stored only if no later block (in the reference's by, bx, x, y write
+// order) writes the same wrapped position: source (px, py) is final iff
+// px + w >= 4*bw and py + h >= 4*bh (RawTexture::SetBlock, Texture.h:114-134).
+__device__ __forceinline__ void store_block(const uint32_t px[16], int w, int h, int bw, int bh, int bx, int by,
+                                            bool aligned, uint8_t *__restrict__ rgba) {
     const bool interior = aligned && bx > 0 && by > 0 && bx * 4 + 4 <= w && by * 4 + 4 <= h;
     if (interior) {
 #pragma unroll
@@ -1230,16 +1322,38 @@ __device__ __forceinline__ void decode_block(const uint8_t *__restrict__ blocks,
     }
 }
 
-// Decode: every texel of every block is decoded, and a texel is stored only
-// if no later block (in the reference's by, bx, x, y write order) writes the
-// same wrapped position: source (px, py) is final iff px + w >= 4*bw and
-// py + h >= 4*bh (RawTexture::SetBlock, Texture.h:114-134).
+template <int FMT, int IT>
+__device__ __forceinline__ void decode_block_fmt(const uint8_t *__restrict__ blocks, int w, int h, int bw, int bh,
+                                                 size_t b, int bx, int by, int write_alpha, int c0, int c1,
+                                                 bool aligned, uint8_t *__restrict__ rgba) {
+    uint32_t px[16];
+    decode_texels<FMT, IT>(blocks, b, write_alpha, c0, c1, px);
+    store_block(px, w, h, bw, bh, bx, by, aligned, rgba);
+}
+
+// Runtime-format decode of block b (the batch kernel's entry).
 template <int IT>
-__global__ void __launch_bounds__(256) k_decode(const uint8_t *__restrict__ blocks, int w, int h, int bw, int bh,
-                                                long nblocks, int fmt, int write_alpha, int c0, int c1, int aligned,
+__device__ __forceinline__ void decode_block(const uint8_t *__restrict__ blocks, int w, int h, int bw, int bh, long b,
+                                             int fmt, int write_alpha, int c0, int c1, int aligned,
+                                             uint8_t *__restrict__ rgba) {
+    const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+    switch (fmt) {
+        case 1: decode_block_fmt<1, IT>(blocks, w, h, bw, bh, (size_t)b, bx, by, write_alpha, c0, c1, aligned, rgba); break;
+        case 3: decode_block_fmt<3, IT>(blocks, w, h, bw, bh, (size_t)b, bx, by, write_alpha, c0, c1, aligned, rgba); break;
+        case 4: decode_block_fmt<4, IT>(blocks, w, h, bw, bh, (size_t)b, bx, by, write_alpha, c0, c1, aligned, rgba); break;
+        default: decode_block_fmt<5, IT>(blocks, w, h, bw, bh, (size_t)b, bx, by, write_alpha, c0, c1, aligned, rgba); break;
+    }
+}
+
+// One thread per block; Idx as in k_bc4_encode.
+template <int FMT, int IT, typename Idx>
+__global__ void __launch_bounds__(256) k_decode(const uint8_t *__restrict__ blocks, int w, int h, Idx bw, int bh,
+                                                Idx nblocks, int write_alpha, int c0, int c1, int aligned,
                                                 uint8_t *__restrict__ rgba) {
-    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x)
-        decode_block<IT>(blocks, w, h, bw, bh, b, fmt, write_alpha, c0, c1, aligned, rgba);
+    for (Idx b = (Idx)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (Idx)gridDim.x * blockDim.x) {
+        const int by = (int)(b / bw), bx = (int)(b - (Idx)by * bw);
+        decode_block_fmt<FMT, IT>(blocks, w, h, (int)bw, bh, (size_t)b, bx, by, write_alpha, c0, c1, aligned != 0, rgba);
+    }
 }
 
 #include "qt_bc1_thread.cuh"
@@ -1402,12 +1516,64 @@ int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl,
     return (int)cudaGetLastError();
 }
 
+// Grid of one thread per block when it fits (uint32_t indices), else a
+// grid-stride loop over 64-bit indices.
+static bool small_index(long n, int *grid) {
+    const long ctas = (n + 255) / 256;
+    if (n <= 0x7FFFFFFFL && ctas <= 0x7FFFFFFFL / 256) {
+        *grid = (int)(ctas > 0 ? ctas : 1);
+        return true;
+    }
+    *grid = num_sms() * 64;
+    return false;
+}
+
 int launch_bc4_encode(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc5, uint8_t *out, void *stream) {
     const int bw = (w + 3) / 4, bh = (h + 3) / 4;
     const long n = (long)bw * bh;
     const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
-    k_bc4_encode<<<grid_for(n, 256), 256, 0, (cudaStream_t)stream>>>(rgba, w, h, bw, n, c0, c1, bc5, aligned, out);
+    cudaStream_t s = (cudaStream_t)stream;
+    int grid = 0;
+    if (small_index(n, &grid)) {
+        const uint32_t ubw = (uint32_t)bw, un = (uint32_t)n;
+        if (bc5) k_bc4_encode<true, uint32_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, un, c0, c1, aligned, out);
+        else k_bc4_encode<false, uint32_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, un, c0, c1, aligned, out);
+    } else {
+        const uint64_t ubw = (uint64_t)bw, un = (uint64_t)n;
+        if (bc5) k_bc4_encode<true, uint64_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, un, c0, c1, aligned, out);
+        else k_bc4_encode<false, uint64_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, un, c0, c1, aligned, out);
+    }
     return (int)cudaGetLastError();
+}
+
+template <int FMT, int IT, typename Idx>
+static void launch_decode_t(int grid, cudaStream_t s, const uint8_t *blocks, int w, int h, int bw, int bh, long n,
+                            int write_alpha, int c0, int c1, int aligned, uint8_t *rgba) {
+    k_decode<FMT, IT, Idx><<<grid, 256, 0, s>>>(blocks, w, h, (Idx)bw, bh, (Idx)n, write_alpha, c0, c1, aligned, rgba);
+}
+
+template <typename Idx>
+static void launch_decode_idx(int fmt, int interp, int grid, cudaStream_t s, const uint8_t *blocks, int w, int h,
+                              int bw, int bh, long n, int write_alpha, int c0, int c1, int aligned, uint8_t *rgba) {
+#define QT_DEC(F, I) launch_decode_t<F, I, Idx>(grid, s, blocks, w, h, bw, bh, n, write_alpha, c0, c1, aligned, rgba)
+    if (fmt == 4) { QT_DEC(4, IT_IDEAL); return; }
+    if (fmt == 5) { QT_DEC(5, IT_IDEAL); return; }
+    if (fmt == 1) {
+        switch (interp) {
+            case IT_IDEAL: QT_DEC(1, IT_IDEAL); break;
+            case IT_ROUND: QT_DEC(1, IT_ROUND); break;
+            case IT_NVIDIA: QT_DEC(1, IT_NVIDIA); break;
+            default: QT_DEC(1, IT_AMD); break;
+        }
+        return;
+    }
+    switch (interp) {
+        case IT_IDEAL: QT_DEC(3, IT_IDEAL); break;
+        case IT_ROUND: QT_DEC(3, IT_ROUND); break;
+        case IT_NVIDIA: QT_DEC(3, IT_NVIDIA); break;
+        default: QT_DEC(3, IT_AMD); break;
+    }
+#undef QT_DEC
 }
 
 int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
@@ -1415,14 +1581,11 @@ int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int 
     const int bw = (w + 3) / 4, bh = (h + 3) / 4;
     const long n = (long)bw * bh;
     const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
-    const int grid = grid_for(n, 256);
-    cudaStream_t s = (cudaStream_t)stream;
-    switch (interp) {
-        case IT_IDEAL: k_decode<IT_IDEAL><<<grid, 256, 0, s>>>(blocks, w, h, bw, bh, n, fmt, write_alpha, c0, c1, aligned, rgba); break;
-        case IT_ROUND: k_decode<IT_ROUND><<<grid, 256, 0, s>>>(blocks, w, h, bw, bh, n, fmt, write_alpha, c0, c1, aligned, rgba); break;
-        case IT_NVIDIA: k_decode<IT_NVIDIA><<<grid, 256, 0, s>>>(blocks, w, h, bw, bh, n, fmt, write_alpha, c0, c1, aligned, rgba); break;
-        default: k_decode<IT_AMD><<<grid, 256, 0, s>>>(blocks, w, h, bw, bh, n, fmt, write_alpha, c0, c1, aligned, rgba); break;
-    }
+    int grid = 0;
+    if (small_index(n, &grid))
+        launch_decode_idx<uint32_t>(fmt, interp, grid, (cudaStream_t)stream, blocks, w, h, bw, bh, n, write_alpha, c0, c1, aligned, rgba);
+    else
+        launch_decode_idx<uint64_t>(fmt, interp, grid, (cudaStream_t)stream, blocks, w, h, bw, bh, n, write_alpha, c0, c1, aligned, rgba);
     return (int)cudaGetLastError();
 }
 
