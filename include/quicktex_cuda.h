@@ -200,6 +200,45 @@ typedef struct qt_copy {
 } qt_copy;
 int qt_copy_async(const qt_copy *copies, size_t n, void *stream);
 
+/* ---- serving: continuous batching on one GPU (no counterpart in the reference) ----
+ *
+ * A qt_server owns a device arena of `memory_budget` bytes, `slots` batch
+ * queues with a stream each, and a worker thread. qt_server_submit queues
+ * requests and returns at once: each is a qt_batch_item whose src and dst are
+ * HOST buffers (the payload and the response buffer; pinned memory makes the
+ * copies asynchronous), kept valid by the caller until the request completes.
+ * Whenever a slot is free the worker folds the waiting requests, in arrival
+ * order, that fit the largest free range of the arena and the batch caps into
+ * one persistent launch on that slot's stream: payload uploads, qt_batch_run,
+ * response downloads. Batches on different slots overlap on the device.
+ * Finished requests are reported by qt_server_poll with their tag, status and
+ * completion time. A request needing more than the whole budget completes at
+ * once with QT_ERR_RANGE. Response bytes equal those of the single-texture
+ * entry points. */
+typedef struct qt_server qt_server;
+typedef struct qt_server_stats {
+    uint64_t batches, requests_done, blocks_done;
+    uint32_t max_inflight, pending, inflight, slots;
+} qt_server_stats;
+int qt_server_create(int device, size_t memory_budget, int slots, size_t max_batch_blocks, size_t max_batch_requests,
+                     qt_server **out);
+/* Runs every request already submitted to completion, then frees the server. */
+int qt_server_destroy(qt_server *s);
+/* Tuning rules / grid of every slot's queue (as qt_batch_set_rules / qt_batch_set_grid). */
+int qt_server_set_rules(qt_server *s, const qt_tile_rule *rules, size_t n);
+int qt_server_set_grid(qt_server *s, int ctas_per_sm);
+/* Queue n requests; tags[i] is reported with request i's completion. All or
+ * nothing: an invalid request -> QT_ERR_ARG and none is queued. */
+int qt_server_submit(qt_server *s, const qt_batch_item *items, const uint64_t *tags, size_t n);
+/* Up to `cap` completions: tag, status (QT_OK or an error code) and completion
+ * time (seconds of qt_server_clock). Waits up to timeout_us (0: no wait) for
+ * the first one; *n receives the count. */
+int qt_server_poll(qt_server *s, uint64_t *tags, int32_t *status, double *t_done, size_t cap, int64_t timeout_us,
+                   size_t *n);
+int qt_server_get_stats(qt_server *s, qt_server_stats *out);
+/* CLOCK_MONOTONIC in seconds: the clock of the completion times. */
+double qt_server_clock(void);
+
 /* ---- the batched path without device allocation (no counterpart in the reference) ----
  *
  * For callers that may not allocate GPU memory when they encode: engines that

@@ -33,7 +33,7 @@ EXT = os.path.join(HERE, "_quicktex" + sysconfig.get_config_var("EXT_SUFFIX"))
 BLOB = os.path.join(HERE, "data", "bc1_order_tables.bin")
 
 KERNEL_SRCS = ["qt_kernels.cu", "qt_noalloc.cu"]
-HOST_SRCS = ["qt_capi.cpp", "qt_batch.cpp"]
+HOST_SRCS = ["qt_capi.cpp", "qt_batch.cpp", "qt_server.cpp"]
 HEADERS = [os.path.join(CSRC, "qt_internal.h"), os.path.join(INCLUDE, "quicktex_cuda.h")]
 
 

@@ -131,23 +131,28 @@ int grow(qt_batch *b, size_t items, size_t tiles) {
 }
 
 int check_item(const qt_batch_item &it) {
-    if (it.op != QT_OP_ENCODE && it.op != QT_OP_DECODE) return qtk::set_error(QT_ERR_ARG, "batch item: invalid op");
-    if (fmt_index(it.format) < 0) return qtk::set_error(QT_ERR_ARG, "batch item: format must be 1, 3, 4 or 5");
-    if (it.width <= 0) return qtk::set_error(QT_ERR_ARG, "Texture width must be greater than 0");
-    if (it.height <= 0) return qtk::set_error(QT_ERR_ARG, "Texture height must be greater than 0");
+    if (int rc = qtk::check_item_fields(it)) return rc;
     if (!it.src || !it.dst) return qtk::set_error(QT_ERR_ARG, "batch item: NULL buffer");
     const size_t bsz = (it.format == 3 || it.format == 5) ? 16 : 8;
     const size_t a_src = it.op == QT_OP_ENCODE ? 4 : bsz, a_dst = it.op == QT_OP_ENCODE ? bsz : 4;
     if (reinterpret_cast<uintptr_t>(it.src) % a_src || reinterpret_cast<uintptr_t>(it.dst) % a_dst)
         return qtk::set_error(QT_ERR_ARG, "batch item: misaligned buffer");
+    return QT_OK;
+}
+
+}  // namespace
+
+int qtk::check_item_fields(const qt_batch_item &it) {
+    if (it.op != QT_OP_ENCODE && it.op != QT_OP_DECODE) return qtk::set_error(QT_ERR_ARG, "batch item: invalid op");
+    if (fmt_index(it.format) < 0) return qtk::set_error(QT_ERR_ARG, "batch item: format must be 1, 3, 4 or 5");
+    if (it.width <= 0) return qtk::set_error(QT_ERR_ARG, "Texture width must be greater than 0");
+    if (it.height <= 0) return qtk::set_error(QT_ERR_ARG, "Texture height must be greater than 0");
     if (it.chan0 < 0 || it.chan0 > 3 || it.chan1 < 0 || it.chan1 > 3) return qtk::set_error(QT_ERR_ARG, "Channel out of range");
     if (it.op == QT_OP_DECODE && (it.interpolator < 0 || it.interpolator > 3))
         return qtk::set_error(QT_ERR_ARG, "Invalid interpolator type");
     if (it.op == QT_OP_ENCODE && (it.format == 1 || it.format == 3)) return qtk::check_bc1_params(&it.params, it.format == 3);
     return QT_OK;
 }
-
-}  // namespace
 
 extern "C" {
 

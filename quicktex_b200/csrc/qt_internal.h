@@ -51,6 +51,9 @@ int set_error(int code, const char *msg);
 int cuda_error(int cuda_status, const char *what);
 int ensure_current_device(int *dev);
 int check_bc1_params(const qt_bc1_params *p, bool bc3);
+// Checks of a qt_batch_item other than its buffers: op, format, size, channels,
+// interpolator and BC1 settings (qt_batch.cpp).
+int check_item_fields(const qt_batch_item &it);
 
 // Kernel-side entry points (qt_kernels.cu). Each returns a cudaError_t value
 // cast to int (0 on success). All pointers are device pointers.

@@ -1,23 +1,25 @@
 """Serving: continuous batching of encode/decode requests on one GPU.
 
-A ``Server`` accepts requests at any time (``submit`` returns a future) and
-runs them through the batched persistent path:
+``Server`` is the Python face of the native serving loop ``qt_server_*``
+(csrc/qt_server.cpp); the loop itself runs on a C++ worker thread, outside the
+interpreter lock:
 
-* **Admission by memory budget.** Input and output buffers come from one
-  pre-reserved device arena (``memory_budget`` bytes, first-fit free list). A
-  request is admitted into a batch only when its bytes fit; otherwise it waits
-  until a running batch returns its memory.
+* **Admission by memory budget.** Request payloads and results live in one
+  device arena of ``memory_budget`` bytes (first fit). A waiting request joins
+  a batch only when its bytes fit the largest free range; otherwise it waits
+  until a running batch returns its memory. A request larger than the whole
+  budget fails at once with ``MemoryError``.
 * **Continuous batching.** ``slots`` batches can be in flight at once, each on
-  its own CUDA stream with its own ``qt_batch`` queue. Whenever a slot is free
-  the worker folds every waiting request that fits (up to ``max_batch_blocks``)
-  into the next persistent launch, so requests that arrive while others run on
-  the GPU are admitted as soon as a slot and memory free up, and their work
+  its own CUDA stream with its own ``qt_batch`` queue (sized up front for
+  ``max_batch_blocks`` / ``max_batch_requests``, so it never reallocates).
+  Whenever a slot is free the worker folds the waiting requests, in arrival
+  order, into the next persistent launch: requests that arrive while others
+  run are admitted as soon as a slot and memory free up, and their work
   overlaps on the device with the batches still running.
-* **Resident buffers.** Nothing is allocated per request: device memory is
-  carved from the arena, each slot's queue is sized for the largest batch at
-  start-up (``qt_batch_reserve``), and the download buffer is pinned and reused.
-  Request payloads are copied straight from the caller's buffers (pinned for
-  asynchronous copies) by ``qt_copy_async``, one call per batch.
+* **Copies.** Each payload is uploaded from, and each result downloaded into,
+  host memory by one asynchronous copy on the batch's stream. Give a request a
+  pinned response buffer (``out=``) and its result lands there with no further
+  copy; without one, the future resolves to ``bytes``.
 
 The integer block output does not depend on what else is in a batch: every
 request's bytes equal those of the single-texture call (tests check this).
@@ -25,124 +27,146 @@ request's bytes equal those of the single-texture call (tests check this).
 
 from __future__ import annotations
 
-import collections
 import concurrent.futures
+import ctypes
 import threading
 import time
-from typing import Optional
+from typing import Optional, Sequence
 
 import numpy as np
 
-from .batch import Batch, Job, copy_async, items_array
+from . import capi
+from .batch import BatchItem, Job, TileRule, items_array, load_tuning
 
 
-def _event(stream):
-    import torch
+class _Stats(ctypes.Structure):
+    """``qt_server_stats``."""
 
-    e = torch.cuda.Event()
-    e.record(stream)
-    return e
+    _fields_ = [("batches", ctypes.c_uint64), ("requests_done", ctypes.c_uint64), ("blocks_done", ctypes.c_uint64),
+                ("max_inflight", ctypes.c_uint32), ("pending", ctypes.c_uint32), ("inflight", ctypes.c_uint32),
+                ("slots", ctypes.c_uint32)]
 
 
-class DeviceArena:
-    """First-fit free list over one device buffer (the memory budget)."""
+_sigs_done = False
+
+
+def _lib():
+    global _sigs_done
+    L = capi.lib()
+    if not _sigs_done:
+        vp, sz = ctypes.c_void_p, ctypes.c_size_t
+        L.qt_server_create.argtypes = [ctypes.c_int, sz, ctypes.c_int, sz, sz, ctypes.POINTER(vp)]
+        L.qt_server_destroy.argtypes = [vp]
+        L.qt_server_set_rules.argtypes = [vp, ctypes.POINTER(TileRule), sz]
+        L.qt_server_set_grid.argtypes = [vp, ctypes.c_int]
+        L.qt_server_submit.argtypes = [vp, ctypes.POINTER(BatchItem), vp, sz]
+        L.qt_server_poll.argtypes = [vp, vp, vp, vp, sz, ctypes.c_int64, ctypes.POINTER(sz)]
+        L.qt_server_get_stats.argtypes = [vp, ctypes.POINTER(_Stats)]
+        L.qt_server_clock.argtypes = []
+        L.qt_server_clock.restype = ctypes.c_double
+        for n in ("qt_server_create", "qt_server_destroy", "qt_server_set_rules", "qt_server_set_grid",
+                  "qt_server_submit", "qt_server_poll", "qt_server_get_stats"):
+            getattr(L, n).restype = ctypes.c_int
+        _sigs_done = True
+    return L
+
+
+class _PinnedPool:
+    """First-fit allocator over one pinned host buffer: the response buffers of
+    requests submitted without ``out`` (a download into pageable memory would
+    make the batch's copies synchronous)."""
 
     ALIGN = 256
 
-    def __init__(self, nbytes: int, device: int):
+    def __init__(self, nbytes: int):
         import torch
 
-        self.buf = torch.empty(nbytes, dtype=torch.uint8, device=torch.device("cuda", device))
-        self.base = self.buf.data_ptr()
-        self.size = nbytes
+        self.buf = torch.empty(nbytes, dtype=torch.uint8).pin_memory()
+        self.np = self.buf.numpy()
         self.free = [(0, nbytes)]  # sorted (offset, length)
-        self.in_use = 0
+        self.lock = threading.Lock()
 
-    def alloc(self, n: int) -> Optional[int]:
+    def take(self, n: int):
         n = (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN
-        for i, (off, ln) in enumerate(self.free):
-            if ln >= n:
-                if ln == n:
-                    self.free.pop(i)
-                else:
-                    self.free[i] = (off + n, ln - n)
-                self.in_use += n
-                return off
+        with self.lock:
+            for i, (off, ln) in enumerate(self.free):
+                if ln >= n:
+                    self.free[i:i + 1] = [] if ln == n else [(off + n, ln - n)]
+                    return off, n
         return None
 
-    def release(self, off: int, n: int) -> None:
-        n = (n + self.ALIGN - 1) // self.ALIGN * self.ALIGN
-        self.in_use -= n
-        fl = self.free
-        fl.append((off, n))
-        fl.sort()
-        merged = []
-        for o, l in fl:
-            if merged and merged[-1][0] + merged[-1][1] == o:
-                merged[-1] = (merged[-1][0], merged[-1][1] + l)
-            else:
-                merged.append((o, l))
-        self.free = merged
+    def give(self, off: int, n: int) -> None:
+        with self.lock:
+            fl = sorted(self.free + [(off, n)])
+            merged = [fl[0]]
+            for o, ln in fl[1:]:
+                if merged[-1][0] + merged[-1][1] == o:
+                    merged[-1] = (merged[-1][0], merged[-1][1] + ln)
+                else:
+                    merged.append((o, ln))
+            self.free = merged
 
 
 class Request:
-    __slots__ = ("job", "future", "t_arrival", "t_done", "out", "out_off")
+    __slots__ = ("job", "future", "t_arrival", "t_done", "out", "buf", "pooled")
 
-    def __init__(self, job: Job, t_arrival: float, out: Optional[np.ndarray] = None):
-        if out is not None and (out.dtype != np.uint8 or out.nbytes < job.out_bytes or not out.flags.c_contiguous):
-            raise ValueError(f"out must be a contiguous uint8 array of at least {job.out_bytes} bytes")
+    def __init__(self, job: Job, t_arrival: float, out: Optional[np.ndarray] = None, pool: Optional[_PinnedPool] = None):
+        if out is not None and (out.dtype != np.uint8 or out.nbytes < job.out_bytes or not out.flags.c_contiguous
+                                or not out.flags.writeable):
+            raise ValueError(f"out must be a writable contiguous uint8 array of at least {job.out_bytes} bytes")
         self.job = job
         self.future = concurrent.futures.Future()
+        self.future.request = self
         self.t_arrival = t_arrival
         self.t_done = None
         self.out = out
-        self.out_off = 0
+        self.pooled = None
+        if out is not None:
+            self.buf = out
+        else:
+            got = pool.take(job.out_bytes) if pool is not None else None
+            if got is not None:
+                self.pooled = got
+                self.buf = pool.np[got[0]: got[0] + job.out_bytes]
+            else:  # pool full: a pageable buffer (correct, but its download is synchronous)
+                self.buf = np.empty(job.out_bytes, np.uint8)
 
-
-class _Slot:
-    def __init__(self, device: int, tuning=None):
-        import torch
-
-        self.stream = torch.cuda.Stream(device=device)
-        self.batch = Batch(device, tuning=tuning)
-        self.event = None
-        self.reqs: list[Request] = []
-        self.region = None  # (offset, nbytes) in the arena
-        self.h_out = None  # pinned download buffer, reused
-        self.h_out_np = None
-
-    def host_out(self, n: int) -> np.ndarray:
-        import torch
-
-        if self.h_out is None or self.h_out.numel() < n:
-            self.h_out = torch.empty(max(n, 1 << 20) * 2, dtype=torch.uint8).pin_memory()
-            self.h_out_np = self.h_out.numpy()
-        return self.h_out_np
+    def result(self):
+        n = self.job.out_bytes
+        return self.buf[:n].tobytes() if self.out is None else self.out[:n]
 
 
 class Server:
     """Continuous-batching encode/decode server on one GPU."""
 
     def __init__(self, device: int = 0, memory_budget: int = 16 << 30, slots: int = 3,
-                 max_batch_blocks: int = 1 << 22, max_batch_requests: int = 8192, tuning=None):
-        import torch
-
-        torch.cuda.set_device(device)
+                 max_batch_blocks: int = 1 << 22, max_batch_requests: int = 8192, tuning=None,
+                 response_pool_bytes: int = 256 << 20):
+        L = _lib()
+        self._pool_bytes = response_pool_bytes
+        self._pool: Optional[_PinnedPool] = None  # pinned on first use
+        h = ctypes.c_void_p()
+        capi.check(L.qt_server_create(device, memory_budget, slots, max_batch_blocks, max_batch_requests,
+                                      ctypes.byref(h)))
+        self.handle = h
         self.device = device
-        self.arena = DeviceArena(memory_budget, device)
-        self.slots = [_Slot(device, tuning) for _ in range(slots)]
-        for s in self.slots:  # queues sized for the largest batch up front: no reallocation while serving
-            s.batch.reserve(max_batch_requests, max_batch_blocks // 32 + max_batch_requests)
-        self.max_batch_blocks = max_batch_blocks
-        self.max_batch_requests = max_batch_requests
-        self.pending: collections.deque[Request] = collections.deque()
-        self.cv = threading.Condition()
-        self.running = True
-        self.batches = 0
-        self.blocks_done = 0
-        self.max_inflight_seen = 0
-        self.worker = threading.Thread(target=self._loop, name="quicktex-serve", daemon=True)
-        self.worker.start()
+        tuning = load_tuning() if tuning is None else tuning
+        if tuning:
+            rules = tuning.get("rules", [])
+            arr = (TileRule * max(1, len(rules)))()
+            for i, r in enumerate(rules):
+                arr[i] = TileRule(r["op"], r["format"], r.get("level", -1), r["tile_blocks"], r["cost_per_block"])
+            capi.check(L.qt_server_set_rules(h, arr, len(rules)))
+            if tuning.get("ctas_per_sm"):
+                capi.check(L.qt_server_set_grid(h, int(tuning["ctas_per_sm"])))
+        # completion times come on CLOCK_MONOTONIC; latencies are measured against time.perf_counter
+        self._clock_offset = time.perf_counter() - L.qt_server_clock()
+        self._lock = threading.Lock()
+        self._inflight: dict[int, Request] = {}
+        self._next_tag = 1
+        self._closing = False
+        self._poller = threading.Thread(target=self._poll_loop, name="quicktex-serve-poll", daemon=True)
+        self._poller.start()
 
     # ---- client side --------------------------------------------------------
     def submit(self, job: Job, t_arrival: Optional[float] = None, out: Optional[np.ndarray] = None
@@ -151,126 +175,107 @@ class Server:
         latency is measured from it. Without ``out`` the future resolves to the
         output as ``bytes``; with ``out`` (a uint8 array, pinned for an
         asynchronous copy) the result is copied from the device straight into it
-        and the future resolves to ``out[:job.out_bytes]``."""
-        r = Request(job, time.perf_counter() if t_arrival is None else t_arrival, out)
-        r.future.request = r
-        with self.cv:
-            self.pending.append(r)
-            self.cv.notify()
-        return r.future
+        and the future resolves to ``out[:job.out_bytes]``. The job's payload and
+        ``out`` must not change until the future is done."""
+        return self.submit_many([job], [t_arrival], [out])[0]
 
-    def submit_many(self, jobs, t_arrivals, outs=None) -> list:
-        """``submit`` for several requests under one lock."""
-        reqs = [Request(j, t, o) for j, t, o in zip(jobs, t_arrivals, outs if outs is not None else [None] * len(jobs))]
-        for r in reqs:
-            r.future.request = r
-        with self.cv:
-            self.pending.extend(reqs)
-            self.cv.notify()
+    def submit_many(self, jobs: Sequence[Job], t_arrivals=None, outs=None) -> list:
+        """``submit`` for several requests in one native call."""
+        n = len(jobs)
+        if n == 0:
+            return []
+        now = time.perf_counter()
+        t_arrivals = [now] * n if t_arrivals is None else [now if t is None else t for t in t_arrivals]
+        outs = [None] * n if outs is None else outs
+        if self._pool is None and self._pool_bytes > 0 and any(o is None for o in outs):
+            self._pool = _PinnedPool(self._pool_bytes)
+        reqs = [Request(j, t, o, self._pool) for j, t, o in zip(jobs, t_arrivals, outs)]
+        items = items_array(jobs, [j.data.ctypes.data for j in jobs], [r.buf.ctypes.data for r in reqs])
+        with self._lock:
+            if self._closing:
+                raise RuntimeError("the server is closed")
+            t0 = self._next_tag
+            self._next_tag += n
+            for k, r in enumerate(reqs):
+                self._inflight[t0 + k] = r
+        tags = np.arange(t0, t0 + n, dtype=np.uint64)
+        rc = _lib().qt_server_submit(self.handle, ctypes.cast(items.ctypes.data, ctypes.POINTER(BatchItem)),
+                                     tags.ctypes.data, n)
+        if rc:
+            with self._lock:
+                for k in range(n):
+                    self._inflight.pop(t0 + k, None)
+            capi.check(rc)
         return [r.future for r in reqs]
 
     def close(self) -> None:
-        with self.cv:
-            self.running = False
-            self.cv.notify()
-        self.worker.join()
-        for s in self.slots:
-            s.batch.close()
+        """Finish every submitted request, then release the server."""
+        if self.handle is None:
+            return
+        with self._lock:
+            self._closing = True
+        self._poller.join()
+        self._final_stats = self.stats()
+        _lib().qt_server_destroy(self.handle)
+        self.handle = None
 
-    # ---- worker ---------------------------------------------------------------
-    def _launch(self, slot: _Slot, reqs: list[Request]) -> None:
-        """One batch on ``slot``'s stream: payload uploads and result downloads
-        (one copy per request each, issued from C), one persistent launch."""
-        n = len(reqs)
-        jobs = [r.job for r in reqs]
-        in_b = np.fromiter((j.data.nbytes for j in jobs), np.int64, n)
-        out_b = np.fromiter((j.out_bytes for j in jobs), np.int64, n)
-        a = DeviceArena.ALIGN
-        in_al, out_al = (in_b + a - 1) // a * a, (out_b + a - 1) // a * a
-        in_off, out_off = np.cumsum(in_al) - in_al, np.cumsum(out_al) - out_al
-        n_in, n_out = int(in_al.sum()), int(out_al.sum())
-        off = self.arena.alloc(n_in + n_out)
-        assert off is not None  # reserved by the caller
-        base = self.arena.base + off
-        src = (base + in_off).astype(np.uint64)
-        dst = (base + n_in + out_off).astype(np.uint64)
-        copies = np.empty((n, 3), np.uint64)
-        copies[:, 0] = src
-        copies[:, 1] = np.fromiter((j.data.ctypes.data for j in jobs), np.uint64, n)
-        copies[:, 2] = in_b
-        stream = slot.stream.cuda_stream
-        copy_async(copies, stream)
-        slot.batch.run(items_array(jobs, src, dst), stream)
-        # results: into the request's own buffer, else into the slot's pinned buffer
-        host = slot.host_out(n_out)
-        hbase = host.ctypes.data
-        copies[:, 1] = dst
-        copies[:, 2] = out_b
-        for k, (r, o) in enumerate(zip(reqs, out_off.tolist())):
-            r.out_off = o
-            copies[k, 0] = hbase + o if r.out is None else r.out.ctypes.data
-        copy_async(copies, stream)
-        slot.event = _event(slot.stream)
-        slot.reqs = reqs
-        slot.region = (off, n_in + n_out)
-        self.batches += 1
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
-    def _complete(self, slot: _Slot) -> None:
-        t = time.perf_counter()
-        host = slot.h_out_np
-        for r in slot.reqs:
-            n = r.job.out_bytes
-            out = host[r.out_off: r.out_off + n].tobytes() if r.out is None else r.out[:n]
-            r.t_done = t
-            self.blocks_done += r.job.nblocks
-            r.future.set_result(out)
-        self.arena.release(*slot.region)
-        slot.reqs, slot.region, slot.event = [], None, None
+    # ---- statistics -------------------------------------------------------------
+    def stats(self) -> dict:
+        """Batches launched, requests and blocks done, most batches in flight at once, ... (kept after close)."""
+        if self.handle is None:
+            return dict(self._final_stats)
+        s = _Stats()
+        capi.check(_lib().qt_server_get_stats(self.handle, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in _Stats._fields_}
 
-    def _take(self) -> list[Request]:
-        """Admit waiting requests, FIFO, while they fit in the free memory and the batch cap."""
-        reqs, nbytes, blocks = [], 0, 0
-        free = self.arena.size - self.arena.in_use
-        largest = max((l for _, l in self.arena.free), default=0)
-        while self.pending:
-            r = self.pending[0]
-            need = DeviceArena.ALIGN * ((r.job.data.nbytes + 255) // 256 + (r.job.out_bytes + 255) // 256)
-            if reqs and (blocks + r.job.nblocks > self.max_batch_blocks or len(reqs) >= self.max_batch_requests):
-                break
-            if nbytes + need > min(free, largest):
-                break
-            reqs.append(self.pending.popleft())
-            nbytes += need
-            blocks += r.job.nblocks
-        return reqs
+    @property
+    def batches(self) -> int:
+        return self.stats()["batches"]
 
-    def _loop(self) -> None:
-        import torch
+    @property
+    def blocks_done(self) -> int:
+        return self.stats()["blocks_done"]
 
-        torch.cuda.set_device(self.device)
+    @property
+    def max_inflight_seen(self) -> int:
+        return self.stats()["max_inflight"]
+
+    # ---- completions ----------------------------------------------------------------
+    def _poll_loop(self) -> None:
+        L = _lib()
+        cap = 4096
+        tags, status, t_done = np.empty(cap, np.uint64), np.empty(cap, np.int32), np.empty(cap, np.float64)
+        got = ctypes.c_size_t()
         while True:
-            busy = [s for s in self.slots if s.event is not None]
-            for s in busy:
-                if s.event.query():
-                    self._complete(s)
-            free_slots = [s for s in self.slots if s.event is None]
-            inflight = len(self.slots) - len(free_slots)
-            with self.cv:
-                if not self.running and not self.pending and inflight == 0:
-                    return
-                reqs = self._take() if (free_slots and self.pending) else []
-                if not reqs and inflight == 0:
-                    if self.pending and not self.arena.in_use:  # a request larger than the whole budget
-                        r = self.pending.popleft()
+            capi.check(L.qt_server_poll(self.handle, tags.ctypes.data, status.ctypes.data, t_done.ctypes.data, cap,
+                                        20_000, ctypes.byref(got)))
+            k = got.value
+            if k:
+                tl, sl, dl = tags[:k].tolist(), status[:k].tolist(), t_done[:k].tolist()
+                with self._lock:
+                    rs = [self._inflight.pop(t) for t in tl]
+                for r, s, t in zip(rs, sl, dl):
+                    r.t_done = t + self._clock_offset
+                    res = r.result() if s == capi.QT_OK else None
+                    if r.pooled is not None:  # result copied out (or failed): the pinned range is free again
+                        self._pool.give(*r.pooled)
+                        r.pooled, r.buf = None, None
+                    if s == capi.QT_OK:
+                        r.future.set_result(res)
+                    elif s == capi.QT_ERR_RANGE:
                         r.future.set_exception(MemoryError("request exceeds the server's memory budget"))
-                        continue
-                    self.cv.wait(timeout=0.001)
-                    continue
-            if reqs:
-                self._launch(free_slots[0], reqs)
-                self.max_inflight_seen = max(self.max_inflight_seen, inflight + 1)
-            else:
-                time.sleep(20e-6)
+                    else:
+                        r.future.set_exception(capi.QtError(s, "request failed on the device"))
+                continue
+            with self._lock:
+                if self._closing and not self._inflight:
+                    return
 
 
 def latency_stats(futures) -> dict:

@@ -99,3 +99,22 @@ def test_error_message_is_thread_local():
     th.join()
     assert b"Level" in lib.qt_last_error()
     assert seen["t"] != lib.qt_last_error()
+
+
+def test_server_argument_errors():
+    """The serving entry points check their arguments before touching a device."""
+    from quicktex_b200 import serve
+
+    L = serve._lib()
+    h = ctypes.c_void_p()
+    assert L.qt_server_create(0, 1 << 20, 0, 1024, 64, ctypes.byref(h)) == capi.QT_ERR_ARG  # no slots
+    assert L.qt_server_create(0, 0, 2, 1024, 64, ctypes.byref(h)) == capi.QT_ERR_ARG        # no budget
+    assert L.qt_server_create(0, 1 << 20, 2, 1024, 64, None) == capi.QT_ERR_ARG
+    n = ctypes.c_size_t()
+    assert L.qt_server_submit(None, None, None, 1) == capi.QT_ERR_ARG
+    assert L.qt_server_poll(None, None, None, None, 0, 0, ctypes.byref(n)) == capi.QT_ERR_ARG
+    assert L.qt_server_get_stats(None, None) == capi.QT_ERR_ARG
+    assert L.qt_server_destroy(None) == capi.QT_OK
+    import time
+
+    assert abs(L.qt_server_clock() - time.monotonic()) < 1.0

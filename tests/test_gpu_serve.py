@@ -35,7 +35,8 @@ def test_results_same_alone_and_in_the_mix():
     jobs = _jobs(1, 120)
     alone = [run_jobs([j])[0] for j in jobs]
     srv = Server(memory_budget=8 << 20, slots=3, max_batch_blocks=4096)
-    futs = [srv.submit(j) for j in jobs]
+    # all at once: the worker fills the free slots back to back, so batches overlap
+    futs = srv.submit_many(jobs[:100]) + [srv.submit(j) for j in jobs[100:]]
     outs = [f.result(timeout=120) for f in futs]
     srv.close()
     assert outs == alone
