@@ -80,14 +80,14 @@ CONFIG = {
 BC1_DRAM_BYTES_PER_BLOCK = (4662272 + 29184) / 65536
 
 
-def measure_hbm_paths(dev, stream):
-    """The bandwidth-bound kernels on 16384^2 textures (1 GiB of texels, far larger than L2):
-    BC4 and BC5 encode, BC1 and BC4 decode; achieved = algorithmic bytes / CUDA-event time."""
+def measure_hbm_paths(dev, stream, side: int = 16384, reps: int = 5):
+    """The bandwidth-bound kernels on side^2 textures (16384^2 = 1 GiB of texels, far larger
+    than L2): BC4 and BC5 encode, BC1, BC3, BC4 and BC5 decode; achieved = algorithmic bytes
+    (64 B of texels + 8 or 16 B of blocks per block) / CUDA-event time."""
     import torch
 
     from quicktex_b200 import capi
 
-    side = 16384
     nb = (side // 4) ** 2
     rng = np.random.default_rng(7)
     tex = torch.from_numpy(rng.integers(0, 256, side * side * 4, dtype=np.uint8)).to(dev)
@@ -100,13 +100,15 @@ def measure_hbm_paths(dev, stream):
         "bc5_encode": (lambda: capi.check(L.qt_bc5_encode_device(capi._vp(tex.data_ptr()), side, side, 0, 1, capi._vp(blocks16.data_ptr()), capi._vp(sptr))), nb * (64 + 16)),
         "bc1_decode": (lambda: capi.check(L.qt_bc1_decode_device(capi._vp(blocks16.data_ptr()), side, side, 0, 0, capi._vp(out.data_ptr()), capi._vp(sptr))), nb * (8 + 64)),
         "bc4_decode": (lambda: capi.check(L.qt_bc4_decode_device(capi._vp(blocks16.data_ptr()), side, side, 0, capi._vp(out.data_ptr()), capi._vp(sptr))), nb * (8 + 64)),
+        "bc3_decode": (lambda: capi.check(L.qt_bc3_decode_device(capi._vp(blocks16.data_ptr()), side, side, 0, capi._vp(out.data_ptr()), capi._vp(sptr))), nb * (16 + 64)),
+        "bc5_decode": (lambda: capi.check(L.qt_bc5_decode_device(capi._vp(blocks16.data_ptr()), side, side, 0, 1, capi._vp(out.data_ptr()), capi._vp(sptr))), nb * (16 + 64)),
     }
     res = {}
     for name, (fn, nbytes) in cases.items():
         fn()
         fn()
         ts = []
-        for _ in range(5):
+        for _ in range(reps):
             a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             a.record(stream)
             fn()
@@ -580,7 +582,17 @@ def main():
     ap.add_argument("--serve-seconds", type=float, nargs="+", default=[2.0, 2.0, 1.0])
     ap.add_argument("--size", type=int, default=4096, help="texture side (profiling variants only)")
     ap.add_argument("--levels", type=str, default="0,10,18", help="levels (profiling variants only)")
+    ap.add_argument("--hbm-only", action="store_true",
+                    help="profiling variant: only the bandwidth-bound kernels on --size^2 textures, one JSON line")
     args = ap.parse_args()
+    if args.hbm_only:
+        import torch
+
+        dev = torch.device("cuda", 0)
+        torch.cuda.set_device(dev)
+        res = measure_hbm_paths(dev, torch.cuda.current_stream(dev), side=args.size, reps=max(1, args.steps))
+        print(json.dumps({"hbm_paths": res, "side": args.size}))
+        return
     configure(args.size, tuple(int(x) for x in args.levels.split(",")))
     if args.impl == "reference":  # CPU only: rank 0 runs it, the other ranks exit without work
         run_reference_arm(args, int(os.environ.get("WORLD_SIZE", "1")), int(os.environ.get("RANK", "0")))

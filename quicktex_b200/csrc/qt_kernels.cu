@@ -1153,6 +1153,65 @@ __device__ __forceinline__ uint2 bc4_block_thread(const uint32_t px[16], int ch)
     return make_uint2(mx | (mn << 8) | (lo << 16), (lo >> 16) | (hi << 16));
 }
 
+__device__ __forceinline__ uint32_t min_u16x2(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("min.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+__device__ __forceinline__ uint32_t max_u16x2(uint32_t a, uint32_t b) {
+    uint32_t d;
+    asm("max.u16x2 %0, %1, %2;" : "=r"(d) : "r"(a), "r"(b));
+    return d;
+}
+
+// BC5Encoder::EncodeBlock (BC5Encoder.cpp:25-30): BC4 of channel c0, then of c1,
+// with the two channels carried side by side in 16-bit halves. One packed
+// min/max per texel covers both channels, and one IMAD forms both numerators
+// 14*value + K: a negative low-half K borrows one from the high half, which its
+// high constant pre-compensates, so each half holds its channel's exact value.
+// Per channel the rest is bc4_block_thread's arithmetic.
+__device__ __forceinline__ uint4 bc5_block_thread(const uint32_t px[16], int c0, int c1) {
+    const uint32_t sel = 0x4040u | (uint32_t)c0 | ((uint32_t)c1 << 8);  // byte c0 -> bits 0..7, byte c1 -> bits 16..23
+    uint32_t v[16];
+    uint32_t mn = 0x00FF00FFu, mx = 0u;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        v[i] = __byte_perm(px[i], 0u, sel);
+        mn = min_u16x2(mn, v[i]);
+        mx = max_u16x2(mx, v[i]);
+    }
+    const uint32_t mn0 = mn & 0xFFFFu, mn1 = mn >> 16, d0 = (mx & 0xFFFFu) - mn0, d1 = (mx >> 16) - mn1;
+    const uint32_t M0 = __ldg(&g_bc4_magic.m[d0]), M1 = __ldg(&g_bc4_magic.m[d1]);  // m[0] = 0: solid, fixed below
+    const int K0 = 4 + (int)d0 - 14 * (int)mn0, K1 = 4 + (int)d1 - 14 * (int)mn1;
+    const uint32_t Kp = ((uint32_t)K0 & 0xFFFFu) + ((uint32_t)(K1 - (K0 < 0 ? 1 : 0)) << 16);
+    uint32_t lo0 = 0u, hi0 = 0u, lo1 = 0u, hi1 = 0u;
+#pragma unroll
+    for (int i = 0; i < 16; i++) {
+        const uint32_t num = 14u * v[i] + Kp;
+        const uint32_t l0 = min(__umulhi(num & 0xFFFFu, M0), 7u), l1 = min(__umulhi(num >> 16, M1), 7u);
+        const uint32_t s0 = __byte_perm(kBC4MapLo, kBC4MapHi, l0) & 7u, s1 = __byte_perm(kBC4MapLo, kBC4MapHi, l1) & 7u;
+        if (i < 10) {
+            lo0 |= s0 << (3 * i);
+            lo1 |= s1 << (3 * i);
+        } else if (i == 10) {
+            lo0 |= s0 << 30;
+            hi0 |= s0 >> 2;
+            lo1 |= s1 << 30;
+            hi1 |= s1 >> 2;
+        } else {
+            hi0 |= s0 << (3 * i - 32);
+            hi1 |= s1 << (3 * i - 32);
+        }
+    }
+    const uint32_t mx0 = mn0 + d0, mx1 = mn1 + d1;
+    uint4 r;
+    r.x = d0 ? (mx0 | (mn0 << 8) | (lo0 << 16)) : (mn0 | (mn0 << 8));  // BC4Block(min) when solid
+    r.y = d0 ? ((lo0 >> 16) | (hi0 << 16)) : 0u;
+    r.z = d1 ? (mx1 | (mn1 << 8) | (lo1 << 16)) : (mn1 | (mn1 << 8));
+    r.w = d1 ? ((lo1 >> 16) | (hi1 << 16)) : 0u;
+    return r;
+}
+
 // One thread per block. Idx is uint32_t whenever the block count and the grid fit
 // 31 bits (the common case: no 64-bit division per block), else uint64_t.
 template <bool BC5, typename Idx>
@@ -1163,13 +1222,8 @@ __global__ void __launch_bounds__(256) k_bc4_encode(const uint8_t *__restrict__ 
         const bool fast = aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h);
         uint32_t px[16];
         load_block_thread(rgba, w, h, bx, by, fast, px);
-        const uint2 a = bc4_block_thread(px, c0);
-        if (BC5) {
-            const uint2 c = bc4_block_thread(px, c1);
-            reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, c.x, c.y);
-        } else {
-            reinterpret_cast<uint2 *>(out)[b] = a;
-        }
+        if (BC5) reinterpret_cast<uint4 *>(out)[b] = bc5_block_thread(px, c0, c1);
+        else reinterpret_cast<uint2 *>(out)[b] = bc4_block_thread(px, c0);
     }
 }
 
@@ -1382,13 +1436,8 @@ __device__ __forceinline__ void batch_block(const BatchItemDev &__restrict__ I, 
     uint32_t v[16];
     load_block_thread(I.src, I.w, I.h, bx, by, aligned && (bx * 4 + 4 <= I.w) && (by * 4 + 4 <= I.h), v);
     if (I.fmt == 4 || I.fmt == 5) {
-        const uint2 a = bc4_block_thread(v, I.c0);
-        if (I.fmt == 5) {
-            const uint2 c = bc4_block_thread(v, I.c1);
-            reinterpret_cast<uint4 *>(I.dst)[b] = make_uint4(a.x, a.y, c.x, c.y);
-        } else {
-            reinterpret_cast<uint2 *>(I.dst)[b] = a;
-        }
+        if (I.fmt == 5) reinterpret_cast<uint4 *>(I.dst)[b] = bc5_block_thread(v, I.c0, I.c1);
+        else reinterpret_cast<uint2 *>(I.dst)[b] = bc4_block_thread(v, I.c0);
         return;
     }
     int pp = 0;
