@@ -7,7 +7,7 @@ reference exposes under ``quicktex`` and ``quicktex.s3tc``, with the same names,
 defaults and exceptions. Every encode and decode runs on the GPU through
 ``libquicktex_cuda.so`` (C-ABI: ``include/quicktex_cuda.h``); there is no CPU
 fallback, and importing fails if the native extension was not built
-(``python -m quicktex_b200.build``).
+(``python quicktex_b200/build.py``).
 """
 
 import os

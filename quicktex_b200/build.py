@@ -9,7 +9,9 @@ Kernels are compiled for sm_100a only (``-gencode arch=compute_100a,code=sm_100a
 with -lineinfo for profiling. nvcc cross-compiles, so this runs on a machine
 without a GPU.
 
-Usage:  python -m quicktex_b200.build [--force]
+Usage:  python quicktex_b200/build.py [--force]
+
+(Run it as a script: importing the package needs the extension this builds.)
 """
 
 from __future__ import annotations

@@ -63,7 +63,7 @@ def lib() -> ctypes.CDLL:
     if _lib is None:
         path = library_path()
         if not os.path.exists(path):
-            raise ImportError(f"{path} is missing: build it with `python -m quicktex_b200.build`")
+            raise ImportError(f"{path} is missing: build it with `python quicktex_b200/build.py`")
         L = ctypes.CDLL(path)
         P = ctypes.POINTER(BC1Params)
         sig = {
