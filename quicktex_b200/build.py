@@ -36,7 +36,9 @@ BLOB = os.path.join(HERE, "data", "bc1_order_tables.bin")
 
 KERNEL_SRCS = ["qt_kernels.cu", "qt_noalloc.cu"]
 HOST_SRCS = ["qt_capi.cpp", "qt_batch.cpp", "qt_server.cpp"]
-HEADERS = [os.path.join(CSRC, "qt_internal.h"), os.path.join(INCLUDE, "quicktex_cuda.h")]
+# every header a source may include: the kernels include qt_bc1_thread.cuh
+HEADERS = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))) + \
+    [os.path.join(INCLUDE, "quicktex_cuda.h")]
 
 
 def _newer(out: str, deps: list[str]) -> bool:

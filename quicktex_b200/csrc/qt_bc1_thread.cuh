@@ -75,6 +75,12 @@ __device__ __noinline__ M metrics(bool ignore_black) {
 // FindSelectors<M>(error_mode), BC1Encoder.cpp:679-779; K is one of the group kernel's kinds
 template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, int hi) {
     const Pal P = make_pal<IT>(lo, hi, kind_three(K));
+    // palette colours (internal order) as packed RGB words and their |c|^2: the error of texel p
+    // against colour k is |p|^2 + v_k - 2 p.c_k, exact in integers (dp4a)
+    const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
+    const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
+    const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
+    const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
     uint32_t sel = 0, tot = 0;
     if (K == K_F4_NONE || K == K_F4_FASTER) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
@@ -87,46 +93,45 @@ template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, in
             const int pr = cr(v), pg = cg(v), pb = cb(v);
             const int dot = 2 * ar * pr + 2 * ag * pg + 2 * ab * pb;
             const int s = 3 - ((dot <= t0) + (dot < t1) + (dot < t2));
-            if (K == K_F4_FASTER)
-                tot += sq3(pr - sel4(P.r0, P.r1, P.r2, P.r3, s), pg - sel4(P.g0, P.g1, P.g2, P.g3, s),
-                           pb - sel4(P.b0, P.b1, P.b2, P.b3, s));
+            if (K == K_F4_FASTER) {
+                const uint32_t u = v & 0x00FFFFFFu;
+                const uint32_t c = s == 0 ? c0 : s == 1 ? c1 : s == 2 ? c2 : c3;
+                const int vc = s == 0 ? v0 : s == 1 ? v1 : s == 2 ? v2 : v3;
+                tot += (uint32_t)((int)__dp4a(u, u, 0u) + vc - 2 * (int)__dp4a(u, c, 0u));
+            }
             sel |= (uint32_t)s << (2 * i);
         }
     } else if (K == K_F4_CHECK2) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
         const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
+        const int dbase = P.r0 * ar + P.g0 * ag + P.b0 * ab;
 #pragma unroll 4
         for (int i = 0; i < 16; i++) {
-            const uint32_t v = px(i);
-            const int pr = cr(v), pg = cg(v), pb = cb(v);
-            const int dd = (pr - P.r0) * ar + (pg - P.g0) * ag + (pb - P.b0) * ab;
+            const uint32_t v = px(i), u = v & 0x00FFFFFFu;
+            const int dd = cr(v) * ar + cg(v) * ag + cb(v) * ab - dbase;  // (p - c0).axis, exact
             const float sf = __fadd_rn(__fmul_rn(__int2float_rn(dd), f), 0.5f);
             const int sl = clampi(f2i_x86(sf), 1, 3);
-            const unsigned e0 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - pr, sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - pg,
-                                    sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - pb);
-            const unsigned e1 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl) - pr, sel4(P.g0, P.g1, P.g2, P.g3, sl) - pg,
-                                    sel4(P.b0, P.b1, P.b2, P.b3, sl) - pb);
-            int s = sl;
-            unsigned e = e1;
+            // the two candidates sl-1 and sl
+            const bool one = sl == 1, two = sl == 2;
+            const uint32_t ca = one ? c0 : two ? c1 : c2, cb_ = one ? c1 : two ? c2 : c3;
+            const int va = one ? v0 : two ? v1 : v2, vb = one ? v1 : two ? v2 : v3;
+            const int e0 = va - 2 * (int)__dp4a(u, ca, 0u), e1 = vb - 2 * (int)__dp4a(u, cb_, 0u);
+            int s = sl, e = e1;
             if (e0 == e1) {
                 if (s == 1) s = 0;
             } else if (e0 < e) {
                 s = sl - 1;
                 e = e0;
             }
-            tot += e;
+            tot += (uint32_t)(e + (int)__dp4a(u, u, 0u));
             sel |= (uint32_t)s << (2 * i);
         }
     } else {
-        const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
-        const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
-        const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
-        const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
 #pragma unroll 4
         for (int i = 0; i < 16; i++) {
             const uint32_t u = px(i) & 0x00FFFFFFu;
             const int pp = (int)__dp4a(u, u, 0u);
-            // |p - c|^2 = |p|^2 + |c|^2 - 2 p.c, exact; ties keep the lower index except selector 3 (:762)
+            // ties keep the lower index except selector 3 (:762)
             int e = v0 - 2 * (int)__dp4a(u, c0, 0u), s = 0;
             const int e1 = v1 - 2 * (int)__dp4a(u, c1, 0u);
             if (e1 < e) { e = e1; s = 1; }
