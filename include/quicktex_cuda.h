@@ -200,6 +200,16 @@ typedef struct qt_copy {
 } qt_copy;
 int qt_copy_async(const qt_copy *copies, size_t n, void *stream);
 
+/* ---- mip chains ----
+ *
+ * BILINEAR resize of an RGBA8 texture (w x h -> dw x dh), each channel on its
+ * own: the mip-level resize of quicktex's dds.encode / image_utils
+ * (quicktex/image_utils.py:40-52 resize_no_premultiply, quicktex/dds.py:275-280),
+ * which is Pillow's Image.resize(size, Image.BILINEAR); byte-identical to it.
+ * Device buffers, 4-byte aligned; enqueued on `stream` (temporary tap tables
+ * and the intermediate rows come from the stream-ordered allocator). */
+int qt_resize_bilinear_device(const uint8_t *src, int w, int h, uint8_t *dst, int dw, int dh, void *stream);
+
 /* ---- serving: continuous batching on one GPU (no counterpart in the reference) ----
  *
  * A qt_server owns a device arena of `memory_budget` bytes, `slots` batch

@@ -34,7 +34,7 @@ LIB = os.path.join(HERE, "libquicktex_cuda.so")
 EXT = os.path.join(HERE, "_quicktex" + sysconfig.get_config_var("EXT_SUFFIX"))
 BLOB = os.path.join(HERE, "data", "bc1_order_tables.bin")
 
-KERNEL_SRCS = ["qt_kernels.cu", "qt_noalloc.cu"]
+KERNEL_SRCS = ["qt_kernels.cu", "qt_noalloc.cu", "qt_resize.cu"]
 HOST_SRCS = ["qt_capi.cpp", "qt_batch.cpp", "qt_server.cpp"]
 # every header a source may include: the kernels include qt_bc1_thread.cuh
 HEADERS = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))) + \
