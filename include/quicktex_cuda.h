@@ -210,6 +210,14 @@ int qt_copy_async(const qt_copy *copies, size_t n, void *stream);
  * and the intermediate rows come from the stream-ordered allocator). */
 int qt_resize_bilinear_device(const uint8_t *src, int w, int h, uint8_t *dst, int dw, int dh, void *stream);
 
+/* Vertical flip and/or BC3nm swizzle of an RGBA8 texture, as the command-line
+ * encoder prepares images (quicktex/cli/encode.py:52-58): flip != 0 reverses the
+ * row order (Image.FLIP_TOP_BOTTOM); c0 >= 0 writes (255, in[c1], in[c1], in[c0])
+ * (Image.merge('RGBA', (one, bands[1], bands[1], bands[0])) with the bands at
+ * channels c0, c1); c0 < 0 leaves the texels as they are. Device buffers, 4-byte
+ * aligned, not overlapping; enqueued on `stream`. */
+int qt_flip_swizzle_device(const uint8_t *src, int w, int h, uint8_t *dst, int flip, int c0, int c1, void *stream);
+
 /* ---- serving: continuous batching on one GPU (no counterpart in the reference) ----
  *
  * A qt_server owns a device arena of `memory_budget` bytes, `slots` batch

@@ -31,7 +31,7 @@ EXPORTS = (
     "qt_batch_last_tiles", "qt_batch_reserve", "qt_copy_async", "qt_batch_run_noalloc",
     "qt_server_create", "qt_server_destroy", "qt_server_set_rules", "qt_server_set_grid", "qt_server_submit",
     "qt_server_poll", "qt_server_get_stats", "qt_server_clock",
-    "qt_resize_bilinear_device",
+    "qt_resize_bilinear_device", "qt_flip_swizzle_device",
 )
 
 
@@ -88,6 +88,7 @@ def lib() -> ctypes.CDLL:
             "qt_bc4_decode_device": [_vp, _i, _i, _i, _vp, _vp],
             "qt_bc5_decode_device": [_vp, _i, _i, _i, _i, _vp, _vp],
             "qt_resize_bilinear_device": [_vp, _i, _i, _vp, _i, _i, _vp],
+            "qt_flip_swizzle_device": [_vp, _i, _i, _vp, _i, _i, _i, _vp],
         }
         for name, args in sig.items():
             f = getattr(L, name)

@@ -202,3 +202,46 @@ extern "C" int qt_resize_bilinear_device(const uint8_t *src, int w, int h, uint8
     cudaFreeAsync(d_taps, s);
     return e == cudaSuccess ? QT_OK : qtk::cuda_error((int)e, "resize");
 }
+
+// ---------------------------------------------------------------------------
+// Vertical flip and the BC3nm swizzle of the command-line encoder
+// (quicktex/cli/encode.py:52-58: image.transpose(FLIP_TOP_BOTTOM), then
+// Image.merge('RGBA', (255, band c1, band c1, band c0))), one texel per thread.
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void __launch_bounds__(256) k_flip_swizzle(const uint32_t *__restrict__ src, int w, int h,
+                                                      uint32_t *__restrict__ dst, int flip, int c0, int c1) {
+    const long n = (long)w * h;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        const int y = (int)(i / w), x = (int)(i - (long)y * w);
+        uint32_t v = __ldg(src + (size_t)(flip ? h - 1 - y : y) * w + x);
+        if (c0 >= 0) {
+            const uint32_t a = (v >> (8 * c0)) & 0xFF, g = (v >> (8 * c1)) & 0xFF;
+            v = 0xFFu | (g << 8) | (g << 16) | (a << 24);
+        }
+        dst[i] = v;
+    }
+}
+
+}  // namespace
+
+extern "C" int qt_flip_swizzle_device(const uint8_t *src, int w, int h, uint8_t *dst, int flip, int c0, int c1,
+                                      void *stream) {
+    if (!src || !dst) return qtk::set_error(QT_ERR_ARG, "NULL buffer");
+    if (w <= 0 || h <= 0) return qtk::set_error(QT_ERR_ARG, "Texture sizes must be greater than 0");
+    if ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 3)
+        return qtk::set_error(QT_ERR_ARG, "flip/swizzle: buffers must be 4-byte aligned");
+    if (c0 >= 0 && (c0 > 3 || c1 < 0 || c1 > 3)) return qtk::set_error(QT_ERR_ARG, "Channel out of range");
+    const size_t bytes = (size_t)w * h * 4;
+    if (src < dst + bytes && dst < src + bytes) return qtk::set_error(QT_ERR_ARG, "flip/swizzle: buffers overlap");
+    if (int rc = qtk::ensure_current_device(nullptr)) return rc;
+    const long n = (long)w * h;
+    long blocks = (n + 255) / 256;
+    if (blocks > 148L * 64) blocks = 148L * 64;
+    k_flip_swizzle<<<(unsigned)blocks, 256, 0, (cudaStream_t)stream>>>(reinterpret_cast<const uint32_t *>(src), w, h,
+                                                                     reinterpret_cast<uint32_t *>(dst), flip != 0,
+                                                                     c0 >= 0 ? c0 : -1, c1);
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? QT_OK : qtk::cuda_error((int)e, "flip/swizzle");
+}

@@ -226,64 +226,137 @@ def _decode_item(fmt: str, decoder) -> typing.Optional[dict]:
     return None
 
 
-def encode(image, encoder, four_cc: str, mip_count: typing.Optional[int] = None) -> DDSFile:
-    """Encode a PIL image and its mip chain (quicktex/dds.py:275-303): the chain's
-    sizes halve down to 1x1 (or ``mip_count`` levels), every level is the
-    original resized with BILINEAR filtering, RGB and alpha separately."""
-    import torch
+class EncodeRequest:
+    """One image to encode into a DDS file, as ``dds.encode`` and the command-line
+    encoder take it: ``flip`` turns it upside down first (Image.FLIP_TOP_BOTTOM)
+    and ``swizzle`` applies the BC3nm swizzle (RGBA = 1, G, G, R) after that."""
 
-    from .batch import Batch, Job
+    def __init__(self, image, encoder, four_cc: str, mip_count: typing.Optional[int] = None, flip: bool = False,
+                 swizzle: bool = False):
+        self.image, self.encoder, self.four_cc, self.mip_count = image, encoder, four_cc, mip_count
+        self.flip, self.swizzle = flip, swizzle
 
-    # as the reference: always convert (it tests `mode != 'RGBA' or mode != 'RGBX'`)
-    mode = "RGBA" if "A" in image.mode else "RGBX"
+
+def _prepare(r: EncodeRequest):
+    """CPU side of one request: the texels as dds.encode converts them, and what is
+    left for the device to do (flip, swizzle channels). Conversions act on each
+    texel alone, so doing them before the flip gives the same texels."""
+    from PIL import Image
+
+    image, flip, swz = r.image, r.flip, None
+    if r.swizzle:
+        if image.mode in ("RGB", "RGBA", "RGBX", "RGBa"):
+            swz, mode = (0, 1), "RGBA"
+        elif image.mode in ("LA", "La"):
+            swz, mode = (0, 3), "RGBA"  # LA -> RGBA is (L, L, L, A): bands 0 and 1 sit at channels 0 and 3
+        else:  # other modes: the reference's own steps on the CPU
+            if flip:
+                image = image.transpose(Image.FLIP_TOP_BOTTOM)
+                flip = False
+            bands = image.split()
+            one = Image.new("L", image.size, 0xFF)
+            image = Image.merge("RGBA", (one, bands[1], bands[1], bands[0]))
+            mode = "RGBA"
+    else:
+        mode = "RGBA" if "A" in image.mode else "RGBX"
     image.apply_transparency()
     image = image.convert(mode)
-    sizes = image_utils.mip_sizes(image.size, mip_count)
-    item = _encode_item(encoder)
-    fmt_name = {"DXT1": "BC1", "DXT5": "BC3", "ATI1": "BC4", "ATI2": "BC5"}.get(four_cc)
-    if item is not None:
-        fmt_name = item["fmt"].upper()
-    fmt = next((f for f in dds_formats if f.name == fmt_name), None)
-    raw = image.tobytes("raw", mode)
+    return image, mode, flip, swz
 
-    if item is None or fmt is None:  # an encoder the batch path does not know: one call per level
-        from . import RawTexture
 
-        levels = [image] + [image_utils.resize_no_premultiply(image, s) for s in sizes[1:]]
-        textures = [encoder.encode(RawTexture.frombytes(i.tobytes("raw", mode), *i.size)) for i in levels]
-    else:
-        dev = torch.device("cuda", torch.cuda.current_device())
-        stream = torch.cuda.current_stream(dev)
-        w0, h0 = sizes[0]
-        align = lambda n: (n + 255) // 256 * 256  # noqa: E731
+def encode_many(requests: typing.Sequence[EncodeRequest], max_batch_bytes: int = 2 << 30) -> typing.List[DDSFile]:
+    """Encode many images with their mip chains. On the device: each image is
+    uploaded once, flipped / swizzled if asked, resized to every level; then the
+    levels of all images (up to ``max_batch_bytes`` of texels at a time) are
+    encoded in one persistent batch launch."""
+    import torch
+
+    from . import RawTexture
+    from .batch import Batch, Job
+
+    prepared = [_prepare(r) for r in requests]
+    out: typing.List[typing.Optional[DDSFile]] = [None] * len(requests)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+    align = lambda n: (n + 255) // 256 * 256  # noqa: E731
+    pending = []  # (index, sizes, fmt, item)
+
+    def flush():
+        if not pending:
+            return
         in_off, out_off, ni, no = [], [], 0, 0
-        bb = _BLOCK_BYTES[fmt.name]
-        for w, h in sizes:
-            in_off.append(ni)
-            out_off.append(no)
-            ni += align(w * h * 4)
-            no += align(((w + 3) // 4) * ((h + 3) // 4) * bb)
-        h_in = torch.frombuffer(bytearray(raw), dtype=torch.uint8).pin_memory()
+        for _, sizes, fmt, _item, _img in pending:
+            bb = _BLOCK_BYTES[fmt.name]
+            lv_in, lv_out = [], []
+            w0, h0 = sizes[0]
+            ni += align(w0 * h0 * 4)  # the uploaded image
+            for w, h in sizes:
+                lv_in.append(ni)
+                lv_out.append(no)
+                ni += align(w * h * 4)
+                no += align(((w + 3) // 4) * ((h + 3) // 4) * bb)
+            in_off.append(lv_in)
+            out_off.append(lv_out)
         d_in = torch.empty(ni, dtype=torch.uint8, device=dev)
-        d_out = torch.empty(no, dtype=torch.uint8, device=dev)
-        base, obase = d_in.data_ptr(), d_out.data_ptr()
-        d_in[: w0 * h0 * 4].copy_(h_in, non_blocking=True)
-        for (w, h), off in zip(sizes[1:], in_off[1:]):  # every level from the original
-            image_utils.resize_device(base, w0, h0, base + off, w, h, stream.cuda_stream)
-        kw = {k: v for k, v in item.items() if k != "fmt"}
-        jobs = [Job.encode(item["fmt"], np.zeros(0, np.uint8), w, h, **kw) for w, h in sizes]
-        items = [j.item(base + a, obase + b) for j, a, b in zip(jobs, in_off, out_off)]
+        d_out = torch.empty(max(no, 1), dtype=torch.uint8, device=dev)
+        base, obase, sp = d_in.data_ptr(), d_out.data_ptr(), stream.cuda_stream
+        items = []
+        for (i, sizes, fmt, item, img), lv_in, lv_out in zip(pending, in_off, out_off):
+            _, mode, flip, swz = prepared[i]
+            w0, h0 = sizes[0]
+            up = lv_in[0] - align(w0 * h0 * 4)
+            h_in = torch.frombuffer(bytearray(img.tobytes("raw", mode)), dtype=torch.uint8).pin_memory()
+            d_in[up: up + w0 * h0 * 4].copy_(h_in, non_blocking=True)
+            c0, c1 = swz if swz else (-1, 0)
+            capi.check(capi.lib().qt_flip_swizzle_device(capi._vp(base + up), w0, h0, capi._vp(base + lv_in[0]),
+                                                        int(flip), c0, c1, capi._vp(sp)))
+            for (w, h), off in zip(sizes[1:], lv_in[1:]):  # every level from the (prepared) original
+                image_utils.resize_device(base + lv_in[0], w0, h0, base + off, w, h, sp)
+            kw = {k: v for k, v in item.items() if k != "fmt"}
+            for (w, h), a, b in zip(sizes, lv_in, lv_out):
+                items.append(Job.encode(item["fmt"], np.zeros(0, np.uint8), w, h, **kw).item(base + a, obase + b))
         batch = Batch(dev.index)
         try:
-            batch.run(items, stream.cuda_stream)  # the whole chain in one persistent launch
+            batch.run(items, sp)  # every level of every image in one persistent launch
             host = d_out.cpu().numpy()
         finally:
             batch.close()
-        textures = []
-        for (w, h), off in zip(sizes, out_off):
-            n = ((w + 3) // 4) * ((h + 3) // 4) * bb
-            textures.append(fmt.texture.from_bytes(host[off: off + n].tobytes(), w, h))
+        for (i, sizes, fmt, _item, _img), lv_out in zip(pending, out_off):
+            bb = _BLOCK_BYTES[fmt.name]
+            texs = [fmt.texture.from_bytes(host[o: o + ((w + 3) // 4) * ((h + 3) // 4) * bb].tobytes(), w, h)
+                    for (w, h), o in zip(sizes, lv_out)]
+            out[i] = _dds_file(texs, requests[i].four_cc, fmt)
+        pending.clear()
 
+    held = 0
+    for i, (r, (img, mode, flip, swz)) in enumerate(zip(requests, prepared)):
+        sizes = image_utils.mip_sizes(img.size, r.mip_count)
+        item = _encode_item(r.encoder)
+        fmt = next((f for f in dds_formats if item is not None and f.name == item["fmt"].upper()), None)
+        if fmt is None:  # an encoder the batch path does not know: the reference's per-level calls
+            from PIL import Image
+
+            if flip:
+                img = img.transpose(Image.FLIP_TOP_BOTTOM)
+            if swz:
+                bands = img.split()
+                img = Image.merge("RGBA", (Image.new("L", img.size, 0xFF), bands[swz[1]], bands[swz[1]], bands[swz[0]]))
+            levels = [img] + [image_utils.resize_no_premultiply(img, s) for s in sizes[1:]]
+            texs = [r.encoder.encode(RawTexture.frombytes(lv.tobytes("raw", mode), *lv.size)) for lv in levels]
+            out[i] = _dds_file(texs, r.four_cc, None)
+            continue
+        need = 2 * sum(w * h * 4 for w, h in sizes)
+        if pending and held + need > max_batch_bytes:
+            flush()
+            held = 0
+        pending.append((i, sizes, fmt, item, img))
+        held += need
+    flush()
+    return out
+
+
+def _dds_file(textures, four_cc: str, fmt) -> DDSFile:
+    """Header fields as quicktex/dds.py:285-303 sets them."""
     dds = DDSFile()
     dds.textures = textures
     dds.flags = DDSFlags.TEXTURE | DDSFlags.LINEAR_SIZE
@@ -300,3 +373,58 @@ def encode(image, encoder, four_cc: str, mip_count: typing.Optional[int] = None)
     if fmt is not None:
         dds.format = fmt
     return dds
+
+
+def encode(image, encoder, four_cc: str, mip_count: typing.Optional[int] = None) -> DDSFile:
+    """Encode a PIL image and its mip chain (quicktex/dds.py:275-303): the chain's
+    sizes halve down to 1x1 (or ``mip_count`` levels), every level is the
+    original resized with BILINEAR filtering, RGB and alpha separately. The
+    whole chain is resized on the device and encoded in one batch launch."""
+    return encode_many([EncodeRequest(image, encoder, four_cc, mip_count)])[0]
+
+
+def decode_many(files: typing.Sequence[DDSFile], mip: int = 0, flip: bool = False) -> list:
+    """Level ``mip`` of every file as PIL images, with each format's default
+    decoder (as ``DDSFile.decode()``): all files in one batch launch, then, with
+    ``flip``, turned upside down on the device (the command-line decoder's
+    Image.FLIP_TOP_BOTTOM)."""
+    import torch
+    from PIL import Image
+
+    from .batch import Batch, Job
+
+    if not files:
+        return []
+    dev = torch.device("cuda", torch.cuda.current_device())
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+    align = lambda n: (n + 255) // 256 * 256  # noqa: E731
+    texs = [f.textures[mip] for f in files]
+    jobs = [Job.decode(f.format.name.lower(), np.frombuffer(bytes(t), np.uint8), t.width, t.height,
+                       **_decode_item(f.format.name, f.format.decoder())) for f, t in zip(files, texs)]
+    in_off, out_off, ni, no = [], [], 0, 0
+    for j in jobs:
+        in_off.append(ni)
+        out_off.append(no)
+        ni += align(j.data.nbytes)
+        no += align(j.out_bytes)
+    h_in = torch.empty(ni, dtype=torch.uint8).pin_memory()
+    hn = h_in.numpy()
+    for j, o in zip(jobs, in_off):
+        hn[o: o + j.data.nbytes] = j.data
+    d_in = h_in.to(dev, non_blocking=True)
+    d_out = torch.empty(no, dtype=torch.uint8, device=dev)
+    d_flip = torch.empty(no, dtype=torch.uint8, device=dev) if flip else d_out
+    ib, ob, fb = d_in.data_ptr(), d_out.data_ptr(), d_flip.data_ptr()
+    batch = Batch(dev.index)
+    try:
+        batch.run([j.item(ib + a, ob + b) for j, a, b in zip(jobs, in_off, out_off)], sp)
+        if flip:
+            for j, b in zip(jobs, out_off):
+                capi.check(capi.lib().qt_flip_swizzle_device(capi._vp(ob + b), j.width, j.height, capi._vp(fb + b),
+                                                            1, -1, 0, capi._vp(sp)))
+        host = d_flip.cpu().numpy()
+    finally:
+        batch.close()
+    return [Image.frombuffer("RGBA", (j.width, j.height), host[b: b + j.out_bytes].tobytes(), "raw", "RGBA", 0, 1)
+            for j, b in zip(jobs, out_off)]

@@ -59,3 +59,29 @@ def make_encoder(pkg, enc):
     if fmt == "BC4":
         return pkg.s3tc.bc4.BC4Encoder(*args)
     return pkg.s3tc.bc5.BC5Encoder(*args)
+
+
+# command-line cases: (input case name, input mode, argv after the program name, output name)
+CLI_INPUTS = {
+    "cli_rgba": {"size": (40, 24), "content": "alpha_mix", "seed": 21},
+    "cli_rgb": {"size": (36, 20), "content": "block_mix", "seed": 22, "mode": "RGB"},
+}
+CLI_ENCODE = [
+    ("cli_rgb", ["encode", "bc1", "-l", "5"], "bc1_l5"),
+    ("cli_rgb", ["encode", "bc1", "-l", "12", "-b", "-F"], "bc1_l12_black_noflip"),
+    ("cli_rgba", ["encode", "bc3", "-l", "6"], "bc3_l6"),
+    ("cli_rgb", ["encode", "bc3", "-l", "4", "-n"], "bc3_l4_normal"),
+    ("cli_rgba", ["encode", "bc4"], "bc4"),
+    ("cli_rgb", ["encode", "bc5", "-F"], "bc5_noflip"),
+    ("cli_rgba", ["encode", "auto", "-l", "3"], "auto_alpha"),
+    ("cli_rgb", ["encode", "auto", "-l", "3", "-4"], "auto_opaque_4color"),
+]
+
+
+def cli_image(name: str):
+    """The seeded PIL image of a command-line input."""
+    CASES[name] = dict(CLI_INPUTS[name], encoder=None, four_cc=None)
+    try:
+        return image(name)
+    finally:
+        del CASES[name]

@@ -45,9 +45,37 @@ def main():
         manifest[name] = {"file_sha256": hashlib.sha256(data).hexdigest(), "bytes": len(data),
                           "mips": back.mipmap_count, "decoded_level_sha256": levels}
         print(name, len(data), back.mipmap_count)
+    # the reference's command line (click commands run in-process) on seeded PNG inputs
+    import tempfile
+
+    from click.testing import CliRunner
+    from quicktex.__main__ import main as ref_main
+
+    cli = {}
+    with tempfile.TemporaryDirectory() as tmp:
+        for name in dds_cases.CLI_INPUTS:
+            dds_cases.cli_image(name).save(os.path.join(tmp, name + ".png"))
+        for src, argv, tag in dds_cases.CLI_ENCODE:
+            work = os.path.join(tmp, tag)  # -o names a directory unless the file already exists
+            os.makedirs(work)
+            r = CliRunner().invoke(ref_main, argv + ["-o", work, os.path.join(tmp, src + ".png")], catch_exceptions=False)
+            assert r.exit_code == 0, r.output
+            dst = os.path.join(out, "cli_" + tag + ".dds")
+            with open(os.path.join(work, src + ".dds"), "rb") as fi, open(dst, "wb") as fo:
+                fo.write(fi.read())
+            r = CliRunner().invoke(ref_main, ["decode", "-o", work, os.path.join(work, src + ".dds")], catch_exceptions=False)
+            assert r.exit_code == 0, r.output
+            png = os.path.join(work, src + ".png")
+            from PIL import Image
+
+            with Image.open(png) as im:
+                px = im.convert("RGBA").tobytes()
+            data = open(dst, "rb").read()
+            cli[tag] = {"file_sha256": hashlib.sha256(data).hexdigest(), "decoded_png_pixels_sha256": hashlib.sha256(px).hexdigest()}
+            print("cli", tag, len(data))
     with open(os.path.join(out, "manifest.json"), "w") as fh:
-        json.dump({"generator": "quicktex (reference) dds.encode / dds.read(...).decode_all(), "
-                                "pybind11 module built from its sources", "cases": manifest}, fh, indent=1)
+        json.dump({"generator": "quicktex (reference) dds.encode / dds.read(...).decode_all() and its click command "
+                                "line, pybind11 module built from its sources", "cases": manifest, "cli": cli}, fh, indent=1)
 
 
 if __name__ == "__main__":
