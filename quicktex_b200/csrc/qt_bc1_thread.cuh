@@ -613,8 +613,8 @@ template <int IT> __device__ __forceinline__ uint2 encode_block(const qt_bc1_par
 // one block per thread; BC3 adds the BC4 alpha block on channel 3
 template <int IT>
 __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_thread(const uint8_t *__restrict__ rgba, int w, int h, int bw,
-                                                                   long nblocks, qt_bc1_params p, uint8_t *__restrict__ out,
-                                                                   int bc3, int aligned) {
+                                                                   long b_begin, long nblocks, qt_bc1_params p,
+                                                                   uint8_t *__restrict__ out, int bc3, int aligned) {
     for (int i = threadIdx.x; i < 64; i += blockDim.x) {
         if (i < 32) s_mid5[i] = c_mid5[i];
         s_mid6[i] = c_mid6[i];
@@ -622,7 +622,7 @@ __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_thread(const uint8_t *
     }
     __syncthreads();
     const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
-    for (long b = (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x) {
+    for (long b = b_begin + (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x) {
         const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
         uint32_t v[16];
         load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);

@@ -274,6 +274,91 @@ int run_host(const void *src, size_t src_bytes, void *dst, size_t dst_bytes, boo
     return QT_OK;
 }
 
+// A second stream and an event per host thread and device, for the banded host path.
+cudaStream_t thread_stream2(int dev) {
+    thread_local cudaStream_t streams[kMaxDevices] = {};
+    if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+    return streams[dev];
+}
+cudaEvent_t thread_event(int dev) {
+    thread_local cudaEvent_t events[kMaxDevices] = {};
+    if (!events[dev]) cudaEventCreateWithFlags(&events[dev], cudaEventDisableTiming);
+    return events[dev];
+}
+
+// Host path, pipelined: the texture is cut into bands of block rows (about 8 MB of
+// texels each). Band k's upload and kernel go on one of two streams, all bands
+// first, then the downloads: so uploads, kernels and downloads of different bands
+// overlap, and a download into pageable memory (which the runtime completes
+// before returning) never holds back a later upload. Encode: a bottom band whose
+// last block row wraps (h % 4 != 0) reads texel rows 0-3, so it waits for band 0's
+// upload. Decode with h % 4 != 0 writes wrapped texels into the top rows from the
+// bottom band, so it is not banded. launch(in, out, b_begin, b_end, stream) runs
+// the kernel over the blocks [b_begin, b_end).
+template <typename Launch>
+int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h, size_t block_bytes, Launch &&launch,
+                    const char *what) {
+    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    const size_t texel_row = (size_t)w * 4, block_row = (size_t)bw * block_bytes;
+    const size_t texel_bytes = texel_row * (size_t)h, blocks_bytes = block_row * (size_t)bh;
+    const size_t per_brow = 4 * texel_row + block_row;
+    const int rows_per_band = (int)std::max<size_t>(1, (size_t(8) << 20) / per_brow);
+    const int nbands = (bh + rows_per_band - 1) / rows_per_band;
+    const bool ragged = (h & 3) != 0;
+    const size_t in_bytes = encode ? texel_bytes : blocks_bytes, out_bytes = encode ? blocks_bytes : texel_bytes;
+    if (nbands < 2 || (!encode && ragged))
+        return run_host(src, in_bytes, dst, out_bytes, false,
+                        [&](void *in, void *out, void *st) { return launch(in, out, 0L, (long)bw * bh, st); }, what);
+    int dev = 0;
+    int rc = ensure_device(&dev);
+    if (rc) return rc;
+    DevBuf din, dout;
+    if ((rc = acquire(din, dev, in_bytes)) || (rc = acquire(dout, dev, out_bytes))) return rc;
+    cudaStream_t st[2] = {thread_stream(dev), thread_stream2(dev)};
+    cudaEvent_t first_up = thread_event(dev);
+    uint8_t *di = static_cast<uint8_t *>(din.ptr), *dout_p = static_cast<uint8_t *>(dout.ptr);
+    cudaError_t e = cudaSuccess;
+    // uploads and kernels
+    for (int k = 0; k < nbands && e == cudaSuccess && rc == QT_OK; k++) {
+        const int r0 = k * rows_per_band, r1 = std::min(bh, r0 + rows_per_band);
+        cudaStream_t s = st[k & 1];
+        size_t off, len;
+        if (encode) {
+            off = (size_t)(4 * r0) * texel_row;
+            len = (size_t)(std::min(h, 4 * r1) - 4 * r0) * texel_row;
+        } else {
+            off = (size_t)r0 * block_row;
+            len = (size_t)(r1 - r0) * block_row;
+        }
+        e = cudaMemcpyAsync(di + off, src + off, len, cudaMemcpyHostToDevice, s);
+        if (e == cudaSuccess && k == 0) e = cudaEventRecord(first_up, s);
+        if (e == cudaSuccess && encode && ragged && k == nbands - 1 && (k & 1)) e = cudaStreamWaitEvent(s, first_up, 0);
+        if (e == cudaSuccess) {
+            const int lrc = launch(din.ptr, dout.ptr, (long)r0 * bw, (long)r1 * bw, (void *)s);
+            if (lrc) rc = cuda_err((cudaError_t)lrc, what);
+        }
+    }
+    // downloads
+    for (int k = 0; k < nbands && e == cudaSuccess && rc == QT_OK; k++) {
+        const int r0 = k * rows_per_band, r1 = std::min(bh, r0 + rows_per_band);
+        size_t off, len;
+        if (encode) {
+            off = (size_t)r0 * block_row;
+            len = (size_t)(r1 - r0) * block_row;
+        } else {
+            off = (size_t)(4 * r0) * texel_row;
+            len = (size_t)(std::min(h, 4 * r1) - 4 * r0) * texel_row;
+        }
+        e = cudaMemcpyAsync(dst + off, dout_p + off, len, cudaMemcpyDeviceToHost, st[k & 1]);
+    }
+    const cudaError_t e0 = cudaStreamSynchronize(st[0]), e1 = cudaStreamSynchronize(st[1]);
+    if (rc) return rc;
+    if (e != cudaSuccess) return cuda_err(e, what);
+    if (e0 != cudaSuccess) return cuda_err(e0, what);
+    if (e1 != cudaSuccess) return cuda_err(e1, what);
+    return QT_OK;
+}
+
 int set_level(qt_bc1_params *p, unsigned level) {
     // BC1Encoder::SetLevel (BC1Encoder.cpp:74-249)
     if (level > 19) return set_err(QT_ERR_ARG, "Level out of range, bust be between 0 and 18 inclusive");
@@ -432,9 +517,11 @@ int qt_bc1_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p
         (rc = check_ptr(blocks, 1, "blocks")))
         return rc;
     const qt_bc1_params pp = *p;
-    return run_host(rgba, (size_t)w * h * 4, blocks, nblocks(w, h) * 8, false,
-                    [&](void *in, void *out, void *s) { return qtk::launch_bc1_encode((const uint8_t *)in, w, h, pp, (uint8_t *)out, false, s); },
-                    "bc1 encode");
+    return run_host_banded(rgba, blocks, true, w, h, 8,
+                           [&](void *in, void *out, long b0, long b1, void *s) {
+                               return qtk::launch_bc1_encode_range((const uint8_t *)in, w, h, pp, (uint8_t *)out, false, b0, b1, s);
+                           },
+                           "bc1 encode");
 }
 
 int qt_bc3_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p, uint8_t *blocks) {
@@ -443,9 +530,11 @@ int qt_bc3_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p
         (rc = check_ptr(blocks, 1, "blocks")))
         return rc;
     const qt_bc1_params pp = *p;
-    return run_host(rgba, (size_t)w * h * 4, blocks, nblocks(w, h) * 16, false,
-                    [&](void *in, void *out, void *s) { return qtk::launch_bc1_encode((const uint8_t *)in, w, h, pp, (uint8_t *)out, true, s); },
-                    "bc3 encode");
+    return run_host_banded(rgba, blocks, true, w, h, 16,
+                           [&](void *in, void *out, long b0, long b1, void *s) {
+                               return qtk::launch_bc1_encode_range((const uint8_t *)in, w, h, pp, (uint8_t *)out, true, b0, b1, s);
+                           },
+                           "bc3 encode");
 }
 
 int qt_bc4_encode_host(const uint8_t *rgba, int w, int h, int channel, uint8_t *blocks) {
@@ -453,9 +542,11 @@ int qt_bc4_encode_host(const uint8_t *rgba, int w, int h, int channel, uint8_t *
     if ((rc = check_dims(w, h)) || (rc = check_channel(channel)) || (rc = check_ptr(rgba, 1, "rgba")) ||
         (rc = check_ptr(blocks, 1, "blocks")))
         return rc;
-    return run_host(rgba, (size_t)w * h * 4, blocks, nblocks(w, h) * 8, false,
-                    [&](void *in, void *out, void *s) { return qtk::launch_bc4_encode((const uint8_t *)in, w, h, channel, channel, false, (uint8_t *)out, s); },
-                    "bc4 encode");
+    return run_host_banded(rgba, blocks, true, w, h, 8,
+                           [&](void *in, void *out, long b0, long b1, void *s) {
+                               return qtk::launch_bc4_encode_range((const uint8_t *)in, w, h, channel, channel, false, (uint8_t *)out, b0, b1, s);
+                           },
+                           "bc4 encode");
 }
 
 int qt_bc5_encode_host(const uint8_t *rgba, int w, int h, int c0, int c1, uint8_t *blocks) {
@@ -463,9 +554,11 @@ int qt_bc5_encode_host(const uint8_t *rgba, int w, int h, int c0, int c1, uint8_
     if ((rc = check_dims(w, h)) || (rc = check_channel(c0)) || (rc = check_channel(c1)) ||
         (rc = check_ptr(rgba, 1, "rgba")) || (rc = check_ptr(blocks, 1, "blocks")))
         return rc;
-    return run_host(rgba, (size_t)w * h * 4, blocks, nblocks(w, h) * 16, false,
-                    [&](void *in, void *out, void *s) { return qtk::launch_bc4_encode((const uint8_t *)in, w, h, c0, c1, true, (uint8_t *)out, s); },
-                    "bc5 encode");
+    return run_host_banded(rgba, blocks, true, w, h, 16,
+                           [&](void *in, void *out, long b0, long b1, void *s) {
+                               return qtk::launch_bc4_encode_range((const uint8_t *)in, w, h, c0, c1, true, (uint8_t *)out, b0, b1, s);
+                           },
+                           "bc5 encode");
 }
 
 // ---- decoders ----
@@ -485,9 +578,11 @@ static int decode_host(int fmt, const uint8_t *blocks, int w, int h, int interp,
         (rc = check_ptr(blocks, 1, "blocks")) || (rc = check_ptr(rgba, 1, "rgba")))
         return rc;
     const size_t bsize = (fmt == 3 || fmt == 5) ? 16 : 8;
-    return run_host(blocks, nblocks(w, h) * bsize, rgba, (size_t)w * h * 4, false,
-                    [&](void *in, void *out, void *s) { return qtk::launch_decode(fmt, (const uint8_t *)in, w, h, interp, wa, c0, c1, (uint8_t *)out, s); },
-                    "decode");
+    return run_host_banded(blocks, rgba, false, w, h, bsize,
+                           [&](void *in, void *out, long b0, long b1, void *s) {
+                               return qtk::launch_decode_range(fmt, (const uint8_t *)in, w, h, interp, wa, c0, c1, (uint8_t *)out, b0, b1, s);
+                           },
+                           "decode");
 }
 
 int qt_bc1_decode_device(const uint8_t *b, int w, int h, int interp, int wa, uint8_t *rgba, void *s) {

@@ -62,6 +62,13 @@ int upload_tables(int device);
 int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
                       void *stream);
 int launch_bc4_encode(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc5, uint8_t *out, void *stream);
+// the same over the blocks [b_begin, b_end) of the texture only (row-major block indices)
+int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
+                            long b_begin, long b_end, void *stream);
+int launch_bc4_encode_range(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc5, uint8_t *out, long b_begin,
+                            long b_end, void *stream);
+int launch_decode_range(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
+                        uint8_t *rgba, long b_begin, long b_end, void *stream);
 // fmt: 1 = BC1, 3 = BC3, 4 = BC4, 5 = BC5
 int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
                   uint8_t *rgba, void *stream);

@@ -1032,8 +1032,8 @@ __device__ __forceinline__ uint2 encode_bc4_group(const Grp &G, int ch) {
 // BC1 / BC3 encode kernel: one block per 16-lane group, grid-stride
 // ---------------------------------------------------------------------------
 template <int IT>
-__global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long nblocks,
-                                                       qt_bc1_params p, uint8_t *__restrict__ out, int bc3) {
+__global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long b_begin,
+                                                       long nblocks, qt_bc1_params p, uint8_t *__restrict__ out, int bc3) {
     for (int i = threadIdx.x; i < 64; i += blockDim.x) {
         if (i < 32) s_mid5[i] = c_mid5[i];
         s_mid6[i] = c_mid6[i];
@@ -1043,7 +1043,7 @@ __global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict
     const Grp G = grp();
     const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
 
-    for (long b = (long)blockIdx.x * kGroupsPerCta + G.g; b < nblocks; b += (long)gridDim.x * kGroupsPerCta) {
+    for (long b = b_begin + (long)blockIdx.x * kGroupsPerCta + G.g; b < nblocks; b += (long)gridDim.x * kGroupsPerCta) {
         const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
         int sx = bx * 4 + (G.lane & 3), sy = by * 4 + (G.lane >> 2);
         if (sx >= w) sx %= w;  // RawTexture::GetBlock wraps at the edges (Texture.h:105-108)
@@ -1215,9 +1215,9 @@ __device__ __forceinline__ uint4 bc5_block_thread(const uint32_t px[16], int c0,
 // One thread per block. Idx is uint32_t whenever the block count and the grid fit
 // 31 bits (the common case: no 64-bit division per block), else uint64_t.
 template <bool BC5, typename Idx>
-__global__ void __launch_bounds__(256) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, Idx bw, Idx nblocks,
-                                                    int c0, int c1, int aligned, uint8_t *__restrict__ out) {
-    for (Idx b = (Idx)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (Idx)gridDim.x * blockDim.x) {
+__global__ void __launch_bounds__(256) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, Idx bw, Idx b_begin,
+                                                    Idx nblocks, int c0, int c1, int aligned, uint8_t *__restrict__ out) {
+    for (Idx b = b_begin + (Idx)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (Idx)gridDim.x * blockDim.x) {
         const int by = (int)(b / bw), bx = (int)(b - (Idx)by * bw);
         const bool fast = aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h);
         uint32_t px[16];
@@ -1402,9 +1402,9 @@ __device__ __forceinline__ void decode_block(const uint8_t *__restrict__ blocks,
 // One thread per block; Idx as in k_bc4_encode.
 template <int FMT, int IT, typename Idx>
 __global__ void __launch_bounds__(256) k_decode(const uint8_t *__restrict__ blocks, int w, int h, Idx bw, int bh,
-                                                Idx nblocks, int write_alpha, int c0, int c1, int aligned,
+                                                Idx b_begin, Idx nblocks, int write_alpha, int c0, int c1, int aligned,
                                                 uint8_t *__restrict__ rgba) {
-    for (Idx b = (Idx)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (Idx)gridDim.x * blockDim.x) {
+    for (Idx b = b_begin + (Idx)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (Idx)gridDim.x * blockDim.x) {
         const int by = (int)(b / bw), bx = (int)(b - (Idx)by * bw);
         decode_block_fmt<FMT, IT>(blocks, w, h, (int)bw, bh, (size_t)b, bx, by, write_alpha, c0, c1, aligned != 0, rgba);
     }
@@ -1526,29 +1526,35 @@ static int bc1_mapping() {
     return m;
 }
 
-int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3, void *stream) {
-    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
-    const long n = (long)bw * bh;
+int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
+                            long b_begin, long b_end, void *stream) {
+    const int bw = (w + 3) / 4;
+    const long n = b_end - b_begin;
+    if (n <= 0) return 0;
     cudaStream_t s = (cudaStream_t)stream;
     if (bc1_mapping() == 0) {
         const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
         const int g = grid_for(n, tpb::kThreads);
         switch (p.interpolator) {
-            case IT_IDEAL: k_bc1_thread<IT_IDEAL><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, n, p, out, bc3, aligned); break;
-            case IT_ROUND: k_bc1_thread<IT_ROUND><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, n, p, out, bc3, aligned); break;
-            case IT_NVIDIA: k_bc1_thread<IT_NVIDIA><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, n, p, out, bc3, aligned); break;
-            default: k_bc1_thread<IT_AMD><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, n, p, out, bc3, aligned); break;
+            case IT_IDEAL: k_bc1_thread<IT_IDEAL><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned); break;
+            case IT_ROUND: k_bc1_thread<IT_ROUND><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned); break;
+            case IT_NVIDIA: k_bc1_thread<IT_NVIDIA><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned); break;
+            default: k_bc1_thread<IT_AMD><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned); break;
         }
         return (int)cudaGetLastError();
     }
     const int grid = grid_for(n, kGroupsPerCta);
     switch (p.interpolator) {
-        case IT_IDEAL: k_bc1_encode<IT_IDEAL><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
-        case IT_ROUND: k_bc1_encode<IT_ROUND><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
-        case IT_NVIDIA: k_bc1_encode<IT_NVIDIA><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
-        default: k_bc1_encode<IT_AMD><<<grid, 128, 0, s>>>(rgba, w, h, bw, n, p, out, bc3); break;
+        case IT_IDEAL: k_bc1_encode<IT_IDEAL><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
+        case IT_ROUND: k_bc1_encode<IT_ROUND><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
+        case IT_NVIDIA: k_bc1_encode<IT_NVIDIA><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
+        default: k_bc1_encode<IT_AMD><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
     }
     return (int)cudaGetLastError();
+}
+
+int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3, void *stream) {
+    return launch_bc1_encode_range(rgba, w, h, p, out, bc3, 0, (long)((w + 3) / 4) * ((h + 3) / 4), stream);
 }
 
 int batch_sms() { return num_sms(); }
@@ -1577,34 +1583,40 @@ static bool small_index(long n, int *grid) {
     return false;
 }
 
-int launch_bc4_encode(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc5, uint8_t *out, void *stream) {
-    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
-    const long n = (long)bw * bh;
+int launch_bc4_encode_range(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc5, uint8_t *out, long b_begin,
+                            long b_end, void *stream) {
+    const int bw = (w + 3) / 4;
+    if (b_end <= b_begin) return 0;
     const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
     cudaStream_t s = (cudaStream_t)stream;
     int grid = 0;
-    if (small_index(n, &grid)) {
-        const uint32_t ubw = (uint32_t)bw, un = (uint32_t)n;
-        if (bc5) k_bc4_encode<true, uint32_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, un, c0, c1, aligned, out);
-        else k_bc4_encode<false, uint32_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, un, c0, c1, aligned, out);
+    if (small_index(b_end, &grid)) {
+        grid = (int)((b_end - b_begin + 255) / 256);
+        const uint32_t ubw = (uint32_t)bw, u0 = (uint32_t)b_begin, un = (uint32_t)b_end;
+        if (bc5) k_bc4_encode<true, uint32_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, u0, un, c0, c1, aligned, out);
+        else k_bc4_encode<false, uint32_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, u0, un, c0, c1, aligned, out);
     } else {
-        const uint64_t ubw = (uint64_t)bw, un = (uint64_t)n;
-        if (bc5) k_bc4_encode<true, uint64_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, un, c0, c1, aligned, out);
-        else k_bc4_encode<false, uint64_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, un, c0, c1, aligned, out);
+        const uint64_t ubw = (uint64_t)bw, u0 = (uint64_t)b_begin, un = (uint64_t)b_end;
+        if (bc5) k_bc4_encode<true, uint64_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, u0, un, c0, c1, aligned, out);
+        else k_bc4_encode<false, uint64_t><<<grid, 256, 0, s>>>(rgba, w, h, ubw, u0, un, c0, c1, aligned, out);
     }
     return (int)cudaGetLastError();
 }
 
+int launch_bc4_encode(const uint8_t *rgba, int w, int h, int c0, int c1, bool bc5, uint8_t *out, void *stream) {
+    return launch_bc4_encode_range(rgba, w, h, c0, c1, bc5, out, 0, (long)((w + 3) / 4) * ((h + 3) / 4), stream);
+}
+
 template <int FMT, int IT, typename Idx>
-static void launch_decode_t(int grid, cudaStream_t s, const uint8_t *blocks, int w, int h, int bw, int bh, long n,
-                            int write_alpha, int c0, int c1, int aligned, uint8_t *rgba) {
-    k_decode<FMT, IT, Idx><<<grid, 256, 0, s>>>(blocks, w, h, (Idx)bw, bh, (Idx)n, write_alpha, c0, c1, aligned, rgba);
+static void launch_decode_t(int grid, cudaStream_t s, const uint8_t *blocks, int w, int h, int bw, int bh, long b0,
+                            long n, int write_alpha, int c0, int c1, int aligned, uint8_t *rgba) {
+    k_decode<FMT, IT, Idx><<<grid, 256, 0, s>>>(blocks, w, h, (Idx)bw, bh, (Idx)b0, (Idx)n, write_alpha, c0, c1, aligned, rgba);
 }
 
 template <typename Idx>
 static void launch_decode_idx(int fmt, int interp, int grid, cudaStream_t s, const uint8_t *blocks, int w, int h,
-                              int bw, int bh, long n, int write_alpha, int c0, int c1, int aligned, uint8_t *rgba) {
-#define QT_DEC(F, I) launch_decode_t<F, I, Idx>(grid, s, blocks, w, h, bw, bh, n, write_alpha, c0, c1, aligned, rgba)
+                              int bw, int bh, long b0, long n, int write_alpha, int c0, int c1, int aligned, uint8_t *rgba) {
+#define QT_DEC(F, I) launch_decode_t<F, I, Idx>(grid, s, blocks, w, h, bw, bh, b0, n, write_alpha, c0, c1, aligned, rgba)
     if (fmt == 4) { QT_DEC(4, IT_IDEAL); return; }
     if (fmt == 5) { QT_DEC(5, IT_IDEAL); return; }
     if (fmt == 1) {
@@ -1625,17 +1637,25 @@ static void launch_decode_idx(int fmt, int interp, int grid, cudaStream_t s, con
 #undef QT_DEC
 }
 
-int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
-                  uint8_t *rgba, void *stream) {
+int launch_decode_range(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
+                        uint8_t *rgba, long b_begin, long b_end, void *stream) {
     const int bw = (w + 3) / 4, bh = (h + 3) / 4;
-    const long n = (long)bw * bh;
+    if (b_end <= b_begin) return 0;
     const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
     int grid = 0;
-    if (small_index(n, &grid))
-        launch_decode_idx<uint32_t>(fmt, interp, grid, (cudaStream_t)stream, blocks, w, h, bw, bh, n, write_alpha, c0, c1, aligned, rgba);
-    else
-        launch_decode_idx<uint64_t>(fmt, interp, grid, (cudaStream_t)stream, blocks, w, h, bw, bh, n, write_alpha, c0, c1, aligned, rgba);
+    if (small_index(b_end, &grid)) {
+        grid = (int)((b_end - b_begin + 255) / 256);
+        launch_decode_idx<uint32_t>(fmt, interp, grid, (cudaStream_t)stream, blocks, w, h, bw, bh, b_begin, b_end, write_alpha, c0, c1, aligned, rgba);
+    } else {
+        launch_decode_idx<uint64_t>(fmt, interp, grid, (cudaStream_t)stream, blocks, w, h, bw, bh, b_begin, b_end, write_alpha, c0, c1, aligned, rgba);
+    }
     return (int)cudaGetLastError();
+}
+
+int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
+                  uint8_t *rgba, void *stream) {
+    return launch_decode_range(fmt, blocks, w, h, interp, write_alpha, c0, c1, rgba, 0,
+                               (long)((w + 3) / 4) * ((h + 3) / 4), stream);
 }
 
 }  // namespace qtk
