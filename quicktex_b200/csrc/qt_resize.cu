@@ -28,6 +28,7 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -140,7 +141,108 @@ __global__ void __launch_bounds__(256) k_resample_v(const uint32_t *__restrict__
     }
 }
 
+// Wide filters (the deep levels of a chain resize the original by up to its full
+// size, so one output sums thousands of taps): the taps of one output are split
+// over several threads and their partial sums added. The sums are exact 32-bit
+// integers, so the order of the additions does not change the result.
+
+// horizontal: one warp per output pixel, lanes stride over the taps (coalesced row reads)
+__global__ void __launch_bounds__(256) k_resample_h_wide(const uint32_t *__restrict__ src, int w, int y0, int rows,
+                                                         uint32_t *__restrict__ dst, int dw,
+                                                         const int2 *__restrict__ bounds,
+                                                         const int32_t *__restrict__ kk, int ksize) {
+    const int lane = threadIdx.x & 31;
+    const long nout = (long)dw * rows;
+    for (long o = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5; o < nout; o += ((long)gridDim.x * blockDim.x) >> 5) {
+        const int y = (int)(o / dw), x = (int)(o - (long)y * dw);
+        const int2 b = bounds[x];
+        const int32_t *k = kk + (size_t)x * ksize;
+        const uint32_t *row = src + (size_t)(y0 + y) * w + b.x;
+        int s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        for (int t = lane; t < b.y; t += 32) {
+            const uint32_t p = __ldg(row + t);
+            const int c = __ldg(k + t);
+            s0 += (int)(p & 0xFF) * c;
+            s1 += (int)((p >> 8) & 0xFF) * c;
+            s2 += (int)((p >> 16) & 0xFF) * c;
+            s3 += (int)(p >> 24) * c;
+        }
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            s0 += __shfl_xor_sync(0xffffffffu, s0, d);
+            s1 += __shfl_xor_sync(0xffffffffu, s1, d);
+            s2 += __shfl_xor_sync(0xffffffffu, s2, d);
+            s3 += __shfl_xor_sync(0xffffffffu, s3, d);
+        }
+        if (lane == 0) {
+            const int half = 1 << (kPrecisionBits - 1);
+            dst[(size_t)y * dw + x] = weighted(s0 + half, s1 + half, s2 + half, s3 + half);
+        }
+    }
+}
+
+// vertical: a CTA of 32 columns x 8 tap groups; the 8 partial sums of a column meet in shared memory
+__global__ void __launch_bounds__(256) k_resample_v_wide(const uint32_t *__restrict__ src, int w,
+                                                         uint32_t *__restrict__ dst, int dh,
+                                                         const int2 *__restrict__ bounds,
+                                                         const int32_t *__restrict__ kk, int ksize) {
+    __shared__ int4 part[8][32];
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+    const int x = blockIdx.x * 32 + tx;
+    for (int yy = blockIdx.y; yy < dh; yy += gridDim.y) {
+        const int2 b = bounds[yy];
+        const int32_t *k = kk + (size_t)yy * ksize;
+        int s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+        if (x < w)
+            for (int t = ty; t < b.y; t += 8) {
+                const uint32_t p = __ldg(src + (size_t)(b.x + t) * w + x);
+                const int c = __ldg(k + t);
+                s0 += (int)(p & 0xFF) * c;
+                s1 += (int)((p >> 8) & 0xFF) * c;
+                s2 += (int)((p >> 16) & 0xFF) * c;
+                s3 += (int)(p >> 24) * c;
+            }
+        part[ty][tx] = make_int4(s0, s1, s2, s3);
+        __syncthreads();
+        if (ty == 0 && x < w) {
+            const int half = 1 << (kPrecisionBits - 1);
+            int4 a = make_int4(half, half, half, half);
+#pragma unroll
+            for (int g = 0; g < 8; g++) {
+                a.x += part[g][tx].x;
+                a.y += part[g][tx].y;
+                a.z += part[g][tx].z;
+                a.w += part[g][tx].w;
+            }
+            dst[(size_t)yy * w + x] = weighted(a.x, a.y, a.z, a.w);
+        }
+        __syncthreads();
+    }
+}
+
+constexpr int kWideTaps = 16;  // above this many taps per output, the split kernels run
+
 dim3 grid_2d(int x, int y) { return dim3((unsigned)((x + 255) / 256), (unsigned)(y < 65535 ? y : 65535)); }
+
+void resample_h(const uint32_t *in, int w, int y0, int rows, uint32_t *out, int dw, const int2 *b, const int32_t *k,
+                int ksize, cudaStream_t s) {
+    if (ksize > kWideTaps) {
+        const long warps = (long)dw * rows;
+        const long ctas = std::min<long>((warps + 7) / 8, 148L * 64);
+        k_resample_h_wide<<<(unsigned)ctas, 256, 0, s>>>(in, w, y0, rows, out, dw, b, k, ksize);
+    } else {
+        k_resample_h<<<grid_2d(dw, rows), 256, 0, s>>>(in, w, y0, rows, out, dw, b, k, ksize);
+    }
+}
+
+void resample_v(const uint32_t *in, int w, uint32_t *out, int dh, const int2 *b, const int32_t *k, int ksize,
+                cudaStream_t s) {
+    if (ksize > kWideTaps)
+        k_resample_v_wide<<<dim3((unsigned)((w + 31) / 32), (unsigned)(dh < 65535 ? dh : 65535)), 256, 0, s>>>(
+            in, w, out, dh, b, k, ksize);
+    else
+        k_resample_v<<<grid_2d(w, dh), 256, 0, s>>>(in, w, out, dh, b, k, ksize);
+}
 
 }  // namespace
 
@@ -189,12 +291,12 @@ extern "C" int qt_resize_bilinear_device(const uint8_t *src, int w, int h, uint8
         const uint32_t *in = reinterpret_cast<const uint32_t *>(src);
         uint32_t *out = reinterpret_cast<uint32_t *>(dst);
         if (need_h && need_v) {
-            k_resample_h<<<grid_2d(dw, tmp_rows), 256, 0, s>>>(in, w, y_first, tmp_rows, d_tmp, dw, b_h, k_h, th.ksize);
-            k_resample_v<<<grid_2d(dw, dh), 256, 0, s>>>(d_tmp, dw, out, dh, b_v, k_v, tv.ksize);
+            resample_h(in, w, y_first, tmp_rows, d_tmp, dw, b_h, k_h, th.ksize, s);
+            resample_v(d_tmp, dw, out, dh, b_v, k_v, tv.ksize, s);
         } else if (need_h) {
-            k_resample_h<<<grid_2d(dw, h), 256, 0, s>>>(in, w, 0, h, out, dw, b_h, k_h, th.ksize);
+            resample_h(in, w, 0, h, out, dw, b_h, k_h, th.ksize, s);
         } else {
-            k_resample_v<<<grid_2d(w, dh), 256, 0, s>>>(in, w, out, dh, b_v, k_v, tv.ksize);
+            resample_v(in, w, out, dh, b_v, k_v, tv.ksize, s);
         }
         e = cudaGetLastError();
     }

@@ -260,8 +260,23 @@ def _prepare(r: EncodeRequest):
     else:
         mode = "RGBA" if "A" in image.mode else "RGBX"
     image.apply_transparency()
-    image = image.convert(mode)
+    if image.mode != mode:  # convert() would return an identical copy
+        image = image.convert(mode)
     return image, mode, flip, swz
+
+
+_staging = None
+
+
+def _pinned(nbytes: int):
+    """A pinned host buffer of at least ``nbytes``, reused across calls (callers finish
+    their copies before returning)."""
+    import torch
+
+    global _staging
+    if _staging is None or _staging.numel() < nbytes:
+        _staging = torch.empty(max(nbytes, 1 << 24), dtype=torch.uint8).pin_memory()
+    return _staging
 
 
 def encode_many(requests: typing.Sequence[EncodeRequest], max_batch_bytes: int = 2 << 30) -> typing.List[DDSFile]:
@@ -284,37 +299,43 @@ def encode_many(requests: typing.Sequence[EncodeRequest], max_batch_bytes: int =
     def flush():
         if not pending:
             return
-        in_off, out_off, ni, no = [], [], 0, 0
+        # device layout: packed uploads, then every level's texels, then every level's blocks
+        up_off, lv_off, out_off, nu, nl, no = [], [], [], 0, 0, 0
         for _, sizes, fmt, _item, _img in pending:
             bb = _BLOCK_BYTES[fmt.name]
+            w0, h0 = sizes[0]
+            up_off.append(nu)
+            nu += align(w0 * h0 * 4)
             lv_in, lv_out = [], []
-            w0, h0 = sizes[0]
-            ni += align(w0 * h0 * 4)  # the uploaded image
             for w, h in sizes:
-                lv_in.append(ni)
+                lv_in.append(nl)
                 lv_out.append(no)
-                ni += align(w * h * 4)
+                nl += align(w * h * 4)
                 no += align(((w + 3) // 4) * ((h + 3) // 4) * bb)
-            in_off.append(lv_in)
+            lv_off.append(lv_in)
             out_off.append(lv_out)
-        d_in = torch.empty(ni, dtype=torch.uint8, device=dev)
+        stage = _pinned(nu).numpy()
+        for (i, sizes, *_rest), o in zip(pending, up_off):
+            img, mode = pending_img[i], prepared[i][1]
+            raw = np.frombuffer(img.tobytes("raw", mode), np.uint8)
+            stage[o: o + raw.size] = raw
+        d_up = torch.empty(nu, dtype=torch.uint8, device=dev)
+        d_lv = torch.empty(nl, dtype=torch.uint8, device=dev)
         d_out = torch.empty(max(no, 1), dtype=torch.uint8, device=dev)
-        base, obase, sp = d_in.data_ptr(), d_out.data_ptr(), stream.cuda_stream
+        d_up.copy_(_staging[:nu], non_blocking=True)  # one upload for all images
+        ub, lb, ob, sp = d_up.data_ptr(), d_lv.data_ptr(), d_out.data_ptr(), stream.cuda_stream
         items = []
-        for (i, sizes, fmt, item, img), lv_in, lv_out in zip(pending, in_off, out_off):
-            _, mode, flip, swz = prepared[i]
+        for (i, sizes, fmt, item, _img), uo, lv_in, lv_out in zip(pending, up_off, lv_off, out_off):
+            _, _mode, flip, swz = prepared[i]
             w0, h0 = sizes[0]
-            up = lv_in[0] - align(w0 * h0 * 4)
-            h_in = torch.frombuffer(bytearray(img.tobytes("raw", mode)), dtype=torch.uint8).pin_memory()
-            d_in[up: up + w0 * h0 * 4].copy_(h_in, non_blocking=True)
             c0, c1 = swz if swz else (-1, 0)
-            capi.check(capi.lib().qt_flip_swizzle_device(capi._vp(base + up), w0, h0, capi._vp(base + lv_in[0]),
+            capi.check(capi.lib().qt_flip_swizzle_device(capi._vp(ub + uo), w0, h0, capi._vp(lb + lv_in[0]),
                                                         int(flip), c0, c1, capi._vp(sp)))
             for (w, h), off in zip(sizes[1:], lv_in[1:]):  # every level from the (prepared) original
-                image_utils.resize_device(base + lv_in[0], w0, h0, base + off, w, h, sp)
+                image_utils.resize_device(lb + lv_in[0], w0, h0, lb + off, w, h, sp)
             kw = {k: v for k, v in item.items() if k != "fmt"}
             for (w, h), a, b in zip(sizes, lv_in, lv_out):
-                items.append(Job.encode(item["fmt"], np.zeros(0, np.uint8), w, h, **kw).item(base + a, obase + b))
+                items.append(Job.encode(item["fmt"], np.zeros(0, np.uint8), w, h, **kw).item(lb + a, ob + b))
         batch = Batch(dev.index)
         try:
             batch.run(items, sp)  # every level of every image in one persistent launch
@@ -328,6 +349,7 @@ def encode_many(requests: typing.Sequence[EncodeRequest], max_batch_bytes: int =
             out[i] = _dds_file(texs, requests[i].four_cc, fmt)
         pending.clear()
 
+    pending_img = {}
     held = 0
     for i, (r, (img, mode, flip, swz)) in enumerate(zip(requests, prepared)):
         sizes = image_utils.mip_sizes(img.size, r.mip_count)
@@ -350,6 +372,7 @@ def encode_many(requests: typing.Sequence[EncodeRequest], max_batch_bytes: int =
             flush()
             held = 0
         pending.append((i, sizes, fmt, item, img))
+        pending_img[i] = img
         held += need
     flush()
     return out
