@@ -99,7 +99,10 @@ const char *qt_version(void);
 
 /* ---- encoders: BlockEncoder<T>::Encode (Encoder.h:36-56) ---- */
 
-/* BC1Encoder::Encode -> EncodeBlock (BC1Encoder.cpp:261-342) per block. */
+/* BC1Encoder::Encode -> EncodeBlock (BC1Encoder.cpp:261-342) per block.
+ * On textures of 16384 blocks or more the device entry points first write the
+ * solid blocks and list the others (stream-ordered scratch of 4 bytes per block
+ * from the library's own memory pool, which keeps freed memory cached). */
 int qt_bc1_encode_host(const uint8_t *rgba, int width, int height, const qt_bc1_params *params, uint8_t *blocks);
 int qt_bc1_encode_device(const uint8_t *rgba, int width, int height, const qt_bc1_params *params, uint8_t *blocks,
                          void *stream);
@@ -207,7 +210,7 @@ int qt_copy_async(const qt_copy *copies, size_t n, void *stream);
  * (quicktex/image_utils.py:40-52 resize_no_premultiply, quicktex/dds.py:275-280),
  * which is Pillow's Image.resize(size, Image.BILINEAR); byte-identical to it.
  * Device buffers, 4-byte aligned; enqueued on `stream` (temporary tap tables
- * and the intermediate rows come from the stream-ordered allocator). */
+ * and the intermediate rows come from the library's stream-ordered memory pool). */
 int qt_resize_bilinear_device(const uint8_t *src, int w, int h, uint8_t *dst, int dw, int dh, void *stream);
 
 /* Vertical flip and/or BC3nm swizzle of an RGBA8 texture, as the command-line

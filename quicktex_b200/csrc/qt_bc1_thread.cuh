@@ -610,11 +610,15 @@ template <int IT> __device__ __forceinline__ uint2 encode_block(const qt_bc1_par
 
 }  // namespace tpb
 
-// one block per thread; BC3 adds the BC4 alpha block on channel 3
-template <int IT>
+// one block per thread; BC3 adds the BC4 alpha block on channel 3. With LIST the
+// thread's blocks are list[i] for i < *count (the non-solid blocks that
+// k_bc1_split left), so no lane of a warp idles on a solid block.
+template <int IT, bool LIST>
 __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_thread(const uint8_t *__restrict__ rgba, int w, int h, int bw,
                                                                    long b_begin, long nblocks, qt_bc1_params p,
-                                                                   uint8_t *__restrict__ out, int bc3, int aligned) {
+                                                                   uint8_t *__restrict__ out, int bc3, int aligned,
+                                                                   const uint32_t *__restrict__ list,
+                                                                   const uint32_t *__restrict__ count) {
     for (int i = threadIdx.x; i < 64; i += blockDim.x) {
         if (i < 32) s_mid5[i] = c_mid5[i];
         s_mid6[i] = c_mid6[i];
@@ -622,7 +626,10 @@ __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_thread(const uint8_t *
     }
     __syncthreads();
     const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
-    for (long b = b_begin + (long)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (long)gridDim.x * blockDim.x) {
+    const long end = LIST ? (long)*count : nblocks;
+    for (long i = (LIST ? 0 : b_begin) + (long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
+         i += (long)gridDim.x * blockDim.x) {
+        const long b = LIST ? (long)list[i] : i;
         const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
         uint32_t v[16];
         load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
@@ -642,5 +649,47 @@ __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_thread(const uint8_t *
         } else {
             reinterpret_cast<uint2 *>(out)[b] = blk;
         }
+    }
+}
+
+// Split pass: one thread per block of [b_begin, b_end). A solid block (all 16
+// texels equal in RGBA, ColorBlock::IsSingleColor) is written here, as
+// EncodeBlock's first step does (BC1Encoder.cpp:264-266, WriteBlockSolid, plus
+// BC3's alpha); every other block's index is appended to list (warp-aggregated).
+template <int IT>
+__global__ void __launch_bounds__(256) k_bc1_split(const uint8_t *__restrict__ rgba, int w, int h, int bw, long b_begin,
+                                                   long b_end, uint8_t *__restrict__ out, int bc3, int aligned,
+                                                   uint32_t *__restrict__ list, uint32_t *__restrict__ count) {
+    const int lane = threadIdx.x & 31;
+    // every lane of a warp runs the same number of iterations, so the ballot sees whole warps
+    const long stride = (long)gridDim.x * blockDim.x;
+    const long first = b_begin + (long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long base_warp = first - lane;
+    for (long wb = base_warp; wb < b_end; wb += stride) {
+        const long b = wb + lane;
+        bool keep = false;
+        if (b < b_end) {
+            const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+            uint32_t v[16];
+            load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
+            bool solid = true;
+#pragma unroll
+            for (int i = 1; i < 16; i++) solid &= v[i] == v[0];
+            if (solid) {
+                const uint2 blk = write_block_solid<IT>(v[0]);
+                if (bc3) {
+                    const uint2 a = bc4_block_thread(v, 3);
+                    reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
+                } else {
+                    reinterpret_cast<uint2 *>(out)[b] = blk;
+                }
+            }
+            keep = !solid;
+        }
+        const uint32_t m = __ballot_sync(0xffffffffu, keep);
+        uint32_t pos = 0;
+        if (lane == 0 && m) pos = atomicAdd(count, (uint32_t)__popc(m));
+        pos = __shfl_sync(0xffffffffu, pos, 0);
+        if (keep) list[pos + __popc(m & ((1u << lane) - 1))] = (uint32_t)b;
     }
 }

@@ -218,6 +218,10 @@ int acquire(DevBuf &b, int dev, size_t n) {
     return QT_OK;
 }
 
+// the library's stream-ordered scratch pool, one per device, created on first use
+std::mutex g_mempool_mu;
+cudaMemPool_t g_mempool[kMaxDevices];
+
 // one non-blocking stream per host thread and device for the host-buffer calls
 cudaStream_t thread_stream(int dev) {
     thread_local cudaStream_t streams[kMaxDevices] = {};
@@ -432,6 +436,34 @@ int set_error(int code, const char *msg) { return set_err(code, "%s", msg); }
 int cuda_error(int e, const char *what) { return cuda_err((cudaError_t)e, what); }
 int ensure_current_device(int *dev) { return ensure_device(dev); }
 int check_bc1_params(const qt_bc1_params *p, bool bc3) { return check_params(p, bc3); }
+
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    cudaMemPool_t pool;
+    {
+        std::lock_guard<std::mutex> lk(g_mempool_mu);
+        if (!g_mempool[dev]) {
+            cudaMemPoolProps props = {};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.handleTypes = cudaMemHandleTypeNone;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = dev;
+            if ((e = cudaMemPoolCreate(&g_mempool[dev], &props)) != cudaSuccess) {
+                g_mempool[dev] = nullptr;
+                return e;
+            }
+            uint64_t keep = UINT64_MAX;
+            cudaMemPoolSetAttribute(g_mempool[dev], cudaMemPoolAttrReleaseThreshold, &keep);
+        }
+        pool = g_mempool[dev];
+    }
+    return cudaMallocFromPoolAsync(ptr, bytes, pool, stream);
+}
+
+cudaError_t scratch_free(void *ptr, cudaStream_t stream) { return ptr ? cudaFreeAsync(ptr, stream) : cudaSuccess; }
 }  // namespace qtk
 
 // ===========================================================================

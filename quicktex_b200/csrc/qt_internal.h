@@ -5,6 +5,8 @@
 #include <cstddef>
 #include <cstdint>
 
+#include <cuda_runtime.h>
+
 #include "quicktex_cuda.h"
 
 namespace qtk {
@@ -54,6 +56,11 @@ int check_bc1_params(const qt_bc1_params *p, bool bc3);
 // Checks of a qt_batch_item other than its buffers: op, format, size, channels,
 // interpolator and BC1 settings (qt_batch.cpp).
 int check_item_fields(const qt_batch_item &it);
+// Stream-ordered scratch from the library's own memory pool on the current
+// device (its release threshold is unlimited, so freed memory stays cached
+// for the next call instead of going back to the driver at every sync).
+cudaError_t scratch_alloc(void **ptr, size_t bytes, cudaStream_t stream);
+cudaError_t scratch_free(void *ptr, cudaStream_t stream);
 
 // Kernel-side entry points (qt_kernels.cu). Each returns a cudaError_t value
 // cast to int (0 on success). All pointers are device pointers.

@@ -1526,6 +1526,9 @@ static int bc1_mapping() {
     return m;
 }
 
+// below this many blocks the split pass costs more than idle solid lanes do
+constexpr long kSplitMinBlocks = 16384;
+
 int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
                             long b_begin, long b_end, void *stream) {
     const int bw = (w + 3) / 4;
@@ -1535,13 +1538,45 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
     if (bc1_mapping() == 0) {
         const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
         const int g = grid_for(n, tpb::kThreads);
-        switch (p.interpolator) {
-            case IT_IDEAL: k_bc1_thread<IT_IDEAL><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned); break;
-            case IT_ROUND: k_bc1_thread<IT_ROUND><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned); break;
-            case IT_NVIDIA: k_bc1_thread<IT_NVIDIA><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned); break;
-            default: k_bc1_thread<IT_AMD><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned); break;
+        if (n < kSplitMinBlocks || n > 0xFFFFFFFFL) {
+            switch (p.interpolator) {
+                case IT_IDEAL: k_bc1_thread<IT_IDEAL, false><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned, nullptr, nullptr); break;
+                case IT_ROUND: k_bc1_thread<IT_ROUND, false><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned, nullptr, nullptr); break;
+                case IT_NVIDIA: k_bc1_thread<IT_NVIDIA, false><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned, nullptr, nullptr); break;
+                default: k_bc1_thread<IT_AMD, false><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned, nullptr, nullptr); break;
+            }
+            return (int)cudaGetLastError();
         }
-        return (int)cudaGetLastError();
+        // solid blocks first, then the encoder over the rest (list + count, stream-ordered scratch)
+        uint32_t *scratch = nullptr;
+        cudaError_t e = scratch_alloc((void **)&scratch, (size_t)(n + 64) * sizeof(uint32_t), s);
+        if (e != cudaSuccess) return (int)e;
+        uint32_t *count = scratch, *list = scratch + 64;
+        e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);
+        if (e == cudaSuccess) {
+            const int gs = grid_for(n, 256);
+            switch (p.interpolator) {
+                case IT_IDEAL:
+                    k_bc1_split<IT_IDEAL><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count);
+                    k_bc1_thread<IT_IDEAL, true><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, 0, 0, p, out, bc3, aligned, list, count);
+                    break;
+                case IT_ROUND:
+                    k_bc1_split<IT_ROUND><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count);
+                    k_bc1_thread<IT_ROUND, true><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, 0, 0, p, out, bc3, aligned, list, count);
+                    break;
+                case IT_NVIDIA:
+                    k_bc1_split<IT_NVIDIA><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count);
+                    k_bc1_thread<IT_NVIDIA, true><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, 0, 0, p, out, bc3, aligned, list, count);
+                    break;
+                default:
+                    k_bc1_split<IT_AMD><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count);
+                    k_bc1_thread<IT_AMD, true><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, 0, 0, p, out, bc3, aligned, list, count);
+                    break;
+            }
+            e = cudaGetLastError();
+        }
+        scratch_free(scratch, s);
+        return (int)e;
     }
     const int grid = grid_for(n, kGroupsPerCta);
     switch (p.interpolator) {

@@ -279,10 +279,10 @@ extern "C" int qt_resize_bilinear_device(const uint8_t *src, int w, int h, uint8
     uint8_t *d_taps = nullptr;
     uint32_t *d_tmp = nullptr;
     const int tmp_rows = y_last - y_first;
-    if ((e = cudaMallocAsync((void **)&d_taps, host.size(), s)) != cudaSuccess) return qtk::cuda_error((int)e, "resize taps");
+    if ((e = qtk::scratch_alloc((void **)&d_taps, host.size(), s)) != cudaSuccess) return qtk::cuda_error((int)e, "resize taps");
     // from pageable memory: the call returns once `host` has been staged
     e = cudaMemcpyAsync(d_taps, host.data(), host.size(), cudaMemcpyHostToDevice, s);
-    if (e == cudaSuccess && need_h && need_v) e = cudaMallocAsync((void **)&d_tmp, (size_t)dw * tmp_rows * 4, s);
+    if (e == cudaSuccess && need_h && need_v) e = qtk::scratch_alloc((void **)&d_tmp, (size_t)dw * tmp_rows * 4, s);
     if (e == cudaSuccess) {
         const int2 *b_h = reinterpret_cast<const int2 *>(d_taps);
         const int32_t *k_h = reinterpret_cast<const int32_t *>(d_taps + o_kh);
@@ -300,8 +300,8 @@ extern "C" int qt_resize_bilinear_device(const uint8_t *src, int w, int h, uint8
         }
         e = cudaGetLastError();
     }
-    if (d_tmp) cudaFreeAsync(d_tmp, s);
-    cudaFreeAsync(d_taps, s);
+    qtk::scratch_free(d_tmp, s);
+    qtk::scratch_free(d_taps, s);
     return e == cudaSuccess ? QT_OK : qtk::cuda_error((int)e, "resize");
 }
 
