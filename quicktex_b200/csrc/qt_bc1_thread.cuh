@@ -535,8 +535,18 @@ __device__ __forceinline__ uint2 write(const R &r) {
     return write_block(g);
 }
 
-// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342), one thread
-template <int IT> __device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_mode, int pp_sum) {
+// A block whose EndpointSearch runs later, in k_bc1_search: its result so far and
+// the queue of its colour mode (0 four-colour, 1 three-colour, 2 three-colour + black).
+struct Deferred {
+    bool need;
+    int queue;
+    R r;
+};
+
+// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342), one thread. With `d`, a block
+// that needs EndpointSearch stops before it and is returned in *d instead.
+template <int IT>
+__device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_mode, int pp_sum, Deferred *d = nullptr) {
     const uint32_t c0 = px(0);
     bool solid = true;
     for (int i = 1; i < 16; i++) solid &= px(i) == c0;
@@ -603,6 +613,12 @@ template <int IT> __device__ __forceinline__ uint2 encode_block(const qt_bc1_par
 
     if (res.err > 0 && p.search_rounds > 0) {
         const int Md = res.mode == CM_THREE ? CM_THREE : (res.mode == CM_TB ? CM_TB : CM_FOUR);
+        if (d) {
+            d->need = true;
+            d->queue = Md == CM_FOUR ? 0 : (Md == CM_THREE ? 1 : 2);
+            d->r = res;
+            return make_uint2(0u, 0u);
+        }
         res = search_any<IT>(kind_for(Md, Md == CM_FOUR ? p.error_mode : EM_FULL), res, p.search_rounds, pp_sum);
     }
     return write(res);
@@ -692,4 +708,186 @@ __global__ void __launch_bounds__(256) k_bc1_split(const uint8_t *__restrict__ r
         pos = __shfl_sync(0xffffffffu, pos, 0);
         if (keep) list[pos + __popc(m & ((1u << lane) - 1))] = (uint32_t)b;
     }
+}
+
+// ---------------------------------------------------------------------------
+// EndpointSearch as a separate pass with lane refill. In the single-pass
+// kernel a warp runs until the longest of its 32 searches stops (most stop
+// after 33 rounds, a few run to 256), so most lanes idle through the search.
+// Here the encoder (k_bc1_defer) queues the blocks that need the search, one
+// queue per colour mode so that a warp runs one selector kind, and
+// k_bc1_search runs one search round per step in every lane: a lane whose
+// search has stopped writes its block and takes the next queued one.
+// ---------------------------------------------------------------------------
+struct SearchQueues {
+    uint32_t *count;  // [3] entries per queue
+    uint32_t *head;   // [3] next entry to take
+    uint32_t *b, *lohi, *err, *sel, *mode;  // [3][cap] each
+    long cap;
+};
+
+template <int IT>
+__global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_defer(const uint8_t *__restrict__ rgba, int w, int h, int bw,
+                                                                  qt_bc1_params p, uint8_t *__restrict__ out, int bc3,
+                                                                  int aligned, const uint32_t *__restrict__ list,
+                                                                  const uint32_t *__restrict__ count, SearchQueues q) {
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+        if (i < 32) s_mid5[i] = c_mid5[i];
+        s_mid6[i] = c_mid6[i];
+        if (i < 16) s_vox[i] = c_voxels[i];
+    }
+    __syncthreads();
+    const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
+    const int lane = threadIdx.x & 31;
+    const long end = (long)*count, stride = (long)gridDim.x * blockDim.x;
+    // warp-uniform iterations, so the ballots below see whole warps
+    for (long wb = (long)blockIdx.x * blockDim.x + threadIdx.x - lane; wb < end; wb += stride) {
+        const long i = wb + lane;
+        tpb::Deferred d;
+        d.need = false;
+        d.queue = 0;
+        long b = 0;
+        if (i < end) {
+            b = (long)list[i];
+            const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+            uint32_t v[16];
+            load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
+            int pp = 0;
+#pragma unroll
+            for (int k = 0; k < 16; k++) {
+                tpb::t_px[k][threadIdx.x] = v[k];
+                const uint32_t u = v[k] & 0x00FFFFFFu;
+                pp += (int)__dp4a(u, u, 0u);
+            }
+            const uint2 blk = tpb::encode_block<IT>(p, color_mode, pp, &d);
+            if (bc3) {  // the alpha half now; a queued block's colour half is written by k_bc1_search
+#pragma unroll
+                for (int k = 0; k < 16; k++) v[k] = tpb::t_px[k][threadIdx.x];
+                const uint2 a = bc4_block_thread(v, 3);
+                reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
+            } else if (!d.need) {
+                reinterpret_cast<uint2 *>(out)[b] = blk;
+            }
+        }
+#pragma unroll
+        for (int qq = 0; qq < 3; qq++) {
+            const bool mine = d.need && d.queue == qq;
+            const uint32_t m = __ballot_sync(0xffffffffu, mine);
+            if (!m) continue;
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(q.count + qq, (uint32_t)__popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (mine) {
+                const long slot = (long)qq * q.cap + base + __popc(m & ((1u << lane) - 1));
+                q.b[slot] = (uint32_t)b;
+                q.lohi[slot] = (uint32_t)d.r.lo | ((uint32_t)d.r.hi << 16);
+                q.err[slot] = d.r.err;
+                q.sel[slot] = d.r.sel;
+                q.mode[slot] = (uint32_t)d.r.mode;
+            }
+        }
+    }
+}
+
+// One queue of searches (the reference's loop, BC1Encoder.cpp:930-996, one round per step).
+template <int IT, int K>
+__device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__ rgba, int w, int h, int bw,
+                                             unsigned rounds, uint8_t *__restrict__ out, int bc3, int aligned,
+                                             const SearchQueues &q) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t total = q.count[qq];
+    bool active = false, drained = false, moved = false;
+    long b = 0;
+    tpb::R r = tpb::rinit();
+    int forbidden = -1, pp = 0;
+    unsigned prev = 0, i = 0;
+    for (;;) {
+        const uint32_t need = __ballot_sync(0xffffffffu, !active && !drained);
+        if (need) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(q.head + qq, (uint32_t)__popc(need));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (!active && !drained) {
+                const uint32_t idx = base + __popc(need & ((1u << lane) - 1));
+                if (idx < total) {
+                    const long slot = (long)qq * q.cap + idx;
+                    b = (long)q.b[slot];
+                    const uint32_t lh = q.lohi[slot];
+                    r.lo = (int)(lh & 0xFFFF);
+                    r.hi = (int)(lh >> 16);
+                    r.err = q.err[slot];
+                    r.sel = q.sel[slot];
+                    r.mode = (int)q.mode[slot];
+                    const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+                    uint32_t v[16];
+                    load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
+                    pp = 0;
+#pragma unroll
+                    for (int k = 0; k < 16; k++) {
+                        tpb::t_px[k][threadIdx.x] = v[k];
+                        const uint32_t u = v[k] & 0x00FFFFFFu;
+                        pp += (int)__dp4a(u, u, 0u);
+                    }
+                    forbidden = -1;
+                    prev = 0;
+                    i = 0;
+                    moved = false;
+                    active = true;
+                } else {
+                    drained = true;
+                }
+            }
+        }
+        if (!__any_sync(0xffffffffu, active)) break;
+        if (!active) continue;
+        bool done = false;
+        if ((int)(i & 31) != forbidden) {
+            const uint16_t vx = s_vox[i & 15];
+            const int ddr = ((int)((unsigned)vx << 30)) >> 30, ddg = ((int)((unsigned)vx << 28)) >> 30;
+            const int ddb = ((int)((unsigned)vx << 26)) >> 30;
+            int lo = r.lo, hi = r.hi;
+            if (i & 16) lo = eppack(clampi(epr(lo) + ddr, 0, 31), clampi(epg(lo) + ddg, 0, 63), clampi(epb(lo) + ddb, 0, 31));
+            else hi = eppack(clampi(epr(hi) + ddr, 0, 31), clampi(epg(hi) + ddg, 0, 63), clampi(epb(hi) + ddb, 0, 31));
+            const uint32_t e = tpb::block_error<IT, K>(lo, hi, pp);
+            if (e < r.err) {
+                r.lo = lo;
+                r.hi = hi;
+                r.err = e;
+                forbidden = (int)((vx >> 8) & 15) | (int)(i & 16);
+                prev = i;
+                moved = true;
+            }
+            if (i - prev > 32) done = true;
+        }
+        i++;
+        if (i >= rounds) done = true;
+        if (done) {
+            if (moved) r.sel = tpb::find_selectors<IT, K>(r.lo, r.hi).x;
+            const uint2 blk = tpb::write(r);
+            if (bc3) reinterpret_cast<uint2 *>(out)[2 * b + 1] = blk;  // the colour half of the 16-byte block
+            else reinterpret_cast<uint2 *>(out)[b] = blk;
+            active = false;
+        }
+    }
+}
+
+template <int IT>
+__global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_search(const uint8_t *__restrict__ rgba, int w, int h, int bw,
+                                                                   qt_bc1_params p, uint8_t *__restrict__ out, int bc3,
+                                                                   int aligned, SearchQueues q) {
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+        if (i < 32) s_mid5[i] = c_mid5[i];
+        s_mid6[i] = c_mid6[i];
+        if (i < 16) s_vox[i] = c_voxels[i];
+    }
+    __syncthreads();
+    const unsigned rounds = p.search_rounds;
+    switch (p.error_mode) {  // four-colour searches use the encoder's error mode (kind_for)
+        case EM_NONE: search_queue<IT, K_F4_NONE>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;
+        case EM_FASTER: search_queue<IT, K_F4_FASTER>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;
+        case EM_CHECK2: search_queue<IT, K_F4_CHECK2>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;
+        default: search_queue<IT, K_F4_FULL>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;
+    }
+    search_queue<IT, K_T3>(1, rgba, w, h, bw, rounds, out, bc3, aligned, q);
+    search_queue<IT, K_TB>(2, rgba, w, h, bw, rounds, out, bc3, aligned, q);
 }

@@ -1547,13 +1547,41 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
             }
             return (int)cudaGetLastError();
         }
-        // solid blocks first, then the encoder over the rest (list + count, stream-ordered scratch)
+        // solid blocks first, then the encoder over the rest (list + count, stream-ordered scratch);
+        // with EndpointSearch, the encoder queues the searches and k_bc1_search runs them
+        const bool defer = p.search_rounds > 0;
+        const size_t words = 64 + (size_t)n + (defer ? 15 * (size_t)n : 0);
         uint32_t *scratch = nullptr;
-        cudaError_t e = scratch_alloc((void **)&scratch, (size_t)(n + 64) * sizeof(uint32_t), s);
+        cudaError_t e = scratch_alloc((void **)&scratch, words * sizeof(uint32_t), s);
         if (e != cudaSuccess) return (int)e;
         uint32_t *count = scratch, *list = scratch + 64;
-        e = cudaMemsetAsync(count, 0, sizeof(uint32_t), s);
-        if (e == cudaSuccess) {
+        e = cudaMemsetAsync(scratch, 0, 64 * sizeof(uint32_t), s);  // list count, queue counts and heads
+        if (e == cudaSuccess && defer) {
+            SearchQueues q;
+            q.count = scratch + 1;
+            q.head = scratch + 4;
+            q.cap = n;
+            uint32_t *qb = list + n;
+            q.b = qb;
+            q.lohi = qb + 3 * (size_t)n;
+            q.err = qb + 6 * (size_t)n;
+            q.sel = qb + 9 * (size_t)n;
+            q.mode = qb + 12 * (size_t)n;
+            const int gs = grid_for(n, 256);
+            const int gsearch = num_sms() * 4;
+            switch (p.interpolator) {
+#define QT_DEFER(I)                                                                                                        \
+    k_bc1_split<I><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count);                      \
+    k_bc1_defer<I><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, list, count, q);                       \
+    k_bc1_search<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, q);
+                case IT_IDEAL: QT_DEFER(IT_IDEAL) break;
+                case IT_ROUND: QT_DEFER(IT_ROUND) break;
+                case IT_NVIDIA: QT_DEFER(IT_NVIDIA) break;
+                default: QT_DEFER(IT_AMD) break;
+#undef QT_DEFER
+            }
+            e = cudaGetLastError();
+        } else if (e == cudaSuccess) {
             const int gs = grid_for(n, 256);
             switch (p.interpolator) {
                 case IT_IDEAL:
