@@ -301,12 +301,15 @@ cudaEvent_t thread_event(int dev) {
 // the kernel over the blocks [b_begin, b_end).
 template <typename Launch>
 int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h, size_t block_bytes, Launch &&launch,
-                    const char *what) {
+                    const char *what, long min_band_blocks = 0) {
     const int bw = (w + 3) / 4, bh = (h + 3) / 4;
     const size_t texel_row = (size_t)w * 4, block_row = (size_t)bw * block_bytes;
     const size_t texel_bytes = texel_row * (size_t)h, blocks_bytes = block_row * (size_t)bh;
     const size_t per_brow = 4 * texel_row + block_row;
-    const int rows_per_band = (int)std::max<size_t>(1, (size_t(8) << 20) / per_brow);
+    // ~8 MB of texels per band, and at least min_band_blocks blocks (a launch that large
+    // runs the BC1 EndpointSearch as its own refill pass)
+    const size_t by_bytes = std::max<size_t>(1, (size_t(8) << 20) / per_brow);
+    const int rows_per_band = (int)std::max<size_t>(by_bytes, (size_t)((min_band_blocks + bw - 1) / bw));
     const int nbands = (bh + rows_per_band - 1) / rows_per_band;
     const bool ragged = (h & 3) != 0;
     const size_t in_bytes = encode ? texel_bytes : blocks_bytes, out_bytes = encode ? blocks_bytes : texel_bytes;
@@ -553,7 +556,7 @@ int qt_bc1_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p
                            [&](void *in, void *out, long b0, long b1, void *s) {
                                return qtk::launch_bc1_encode_range((const uint8_t *)in, w, h, pp, (uint8_t *)out, false, b0, b1, s);
                            },
-                           "bc1 encode");
+                           "bc1 encode", pp.search_rounds > 0 ? qtk::defer_min_blocks() : 0);
 }
 
 int qt_bc3_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p, uint8_t *blocks) {
@@ -566,7 +569,7 @@ int qt_bc3_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p
                            [&](void *in, void *out, long b0, long b1, void *s) {
                                return qtk::launch_bc1_encode_range((const uint8_t *)in, w, h, pp, (uint8_t *)out, true, b0, b1, s);
                            },
-                           "bc3 encode");
+                           "bc3 encode", pp.search_rounds > 0 ? qtk::defer_min_blocks() : 0);
 }
 
 int qt_bc4_encode_host(const uint8_t *rgba, int w, int h, int channel, uint8_t *blocks) {
