@@ -90,8 +90,9 @@ template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, in
 #pragma unroll 4
         for (int i = 0; i < 16; i++) {
             const uint32_t v = px(i);
-            const int pr = cr(v), pg = cg(v), pb = cb(v);
-            const int dot = 2 * ar * pr + 2 * ag * pg + 2 * ab * pb;
+            // 2 p.axis, with axis = palette entry 3 - entry 0 (the palette words' byte 3 is 0)
+            const int p0 = (int)__dp4a(v, c0, 0u), p3 = (int)__dp4a(v, c3, 0u);
+            const int dot = 2 * (p3 - p0);
             const int s = 3 - ((dot <= t0) + (dot < t1) + (dot < t2));
             if (K == K_F4_FASTER) {
                 const uint32_t u = v & 0x00FFFFFFu;
@@ -108,14 +109,15 @@ template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, in
 #pragma unroll 4
         for (int i = 0; i < 16; i++) {
             const uint32_t v = px(i), u = v & 0x00FFFFFFu;
-            const int dd = cr(v) * ar + cg(v) * ag + cb(v) * ab - dbase;  // (p - c0).axis, exact
-            const float sf = __fadd_rn(__fmul_rn(__int2float_rn(dd), f), 0.5f);
-            const int sl = clampi(f2i_x86(sf), 1, 3);
+            const int p0 = (int)__dp4a(v, c0, 0u), p1 = (int)__dp4a(v, c1, 0u);
+            const int p2 = (int)__dp4a(v, c2, 0u), p3 = (int)__dp4a(v, c3, 0u);
+            const int dd = p3 - p0 - dbase;  // (p - c0).axis, exact
+            // |dd * f + 0.5| stays far inside int range (f <= 4 whenever the axis is non-zero)
+            const int sl = clampi(__float2int_rz(__fadd_rn(__fmul_rn(__int2float_rn(dd), f), 0.5f)), 1, 3);
             // the two candidates sl-1 and sl
             const bool one = sl == 1, two = sl == 2;
-            const uint32_t ca = one ? c0 : two ? c1 : c2, cb_ = one ? c1 : two ? c2 : c3;
-            const int va = one ? v0 : two ? v1 : v2, vb = one ? v1 : two ? v2 : v3;
-            const int e0 = va - 2 * (int)__dp4a(u, ca, 0u), e1 = vb - 2 * (int)__dp4a(u, cb_, 0u);
+            const int e0 = one ? v0 - 2 * p0 : two ? v1 - 2 * p1 : v2 - 2 * p2;
+            const int e1 = one ? v1 - 2 * p1 : two ? v2 - 2 * p2 : v3 - 2 * p3;
             int s = sl, e = e1;
             if (e0 == e1) {
                 if (s == 1) s = 0;
@@ -184,6 +186,48 @@ template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo,
             t1 += n;
         }
         return (uint32_t)(pp_sum + t0 + t1);
+    }
+    if (K == K_F4_CHECK2 || K == K_F4_FASTER) {
+        // The total of FindSelectors' Check2 / Faster modes (BC1Encoder.cpp:697-749) without the
+        // selectors: ties choose between selectors of equal error, so they do not change it. The
+        // axis is palette entry 3 - entry 0, so p.axis = p.c3 - p.c0 from the same dp4a products.
+        const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
+        const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
+        const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
+        const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
+        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
+        int t = 0;
+        if (K == K_F4_CHECK2) {
+            const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
+            const int dbase = P.r0 * ar + P.g0 * ag + P.b0 * ab;
+#pragma unroll 4
+            for (int i = 0; i < 16; i++) {
+                const uint32_t u = px(i);  // the palette words' byte 3 is 0: alpha drops out of dp4a
+                const int d0 = (int)__dp4a(u, c0, 0u), d1 = (int)__dp4a(u, c1, 0u);
+                const int d2 = (int)__dp4a(u, c2, 0u), d3 = (int)__dp4a(u, c3, 0u);
+                // |dd * f + 0.5| stays far inside int range (f <= 4 whenever the axis is non-zero)
+                const int sl = clampi(__float2int_rz(__fadd_rn(__fmul_rn(__int2float_rn(d3 - d0 - dbase), f), 0.5f)), 1, 3);
+                const bool one = sl == 1, two = sl == 2;
+                const int ea = one ? v0 - 2 * d0 : two ? v1 - 2 * d1 : v2 - 2 * d2;
+                const int eb = one ? v1 - 2 * d1 : two ? v2 - 2 * d2 : v3 - 2 * d3;
+                t += min(ea, eb);
+            }
+        } else {
+            const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
+            const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
+            const int t0 = d0 + d1, t1 = d1 + d2, t2 = d2 + d3;
+#pragma unroll 4
+            for (int i = 0; i < 16; i++) {
+                const uint32_t u = px(i);
+                const int e0 = (int)__dp4a(u, c0, 0u), e3 = (int)__dp4a(u, c3, 0u);
+                const int dot = 2 * (e3 - e0);  // 2 p.axis
+                const int s = 3 - ((dot <= t0) + (dot < t1) + (dot < t2));
+                const uint32_t c = s == 0 ? c0 : s == 1 ? c1 : s == 2 ? c2 : c3;
+                const int vc = s == 0 ? v0 : s == 1 ? v1 : s == 2 ? v2 : v3;
+                t += vc - 2 * (int)__dp4a(u, c, 0u);
+            }
+        }
+        return (uint32_t)(pp_sum + t);
     }
     return find_selectors<IT, K>(lo, hi).y;
 }
