@@ -349,15 +349,17 @@ def run_ours(args, world, rank, local):
             "bound": "fp32_issue", "achieved": achieved, "peak": peak_tops, "unit": "Tlane-op/s",
             "frac": achieved / peak_tops, "traffic": BC1_DRAM_BYTES_PER_BLOCK * NB,
             "traffic_source": "ncu dram bytes of a 1024^2 L18 launch, scaled to this launch's blocks",
-            "kernel": "qtk::k_bc1_thread (+ its qtk::k_bc1_split pass; all 36 settings)",
+            "kernel": "BC1 encode call: qtk::k_bc1_split, then qtk::k_bc1_thread, or qtk::k_bc1_defer + "
+                      "qtk::k_bc1_search for settings with EndpointSearch (all settings)",
             "work": "10 lane-ops x oracle-counted candidate evaluations per block",
             "peak_source": f"{sms} SMs x 128 lanes x sm_max_mhz ({peaks_kind})",
         },
         "by_level_mblocks_s": {k: v[1] / (v[0] / 1e3) / 1e6 for k, v in by_level.items()},
         "e2e": {"value": e2e_value, "unit": "Mblocks/s", "h2d_bytes_per_step": W * H * 4 * len(SETTINGS),
                 "d2h_bytes_per_step": NB * 8 * len(SETTINGS)},
-        # per encode call: the split pass and the encoder (textures of >= 16384 blocks), else the encoder
-        "gpu_launches": len(SETTINGS) * args.steps * (2 if NB >= 16384 else 1),
+        # per encode call, as the library reports it: the encoder, the split pass (>= 16384 blocks)
+        # and, for settings with EndpointSearch on large textures, the search pass
+        "gpu_launches": args.steps * sum(capi.bc1_encode_kernels(W, H, p) for p in params),
         "clocks": clk.summary(),
     }
     peaks_hbm = peaks.get("hbm_gbs", 6650.0)

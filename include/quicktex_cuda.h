@@ -113,6 +113,13 @@ int qt_bc3_encode_host(const uint8_t *rgba, int width, int height, const qt_bc1_
 int qt_bc3_encode_device(const uint8_t *rgba, int width, int height, const qt_bc1_params *params, uint8_t *blocks,
                          void *stream);
 
+/* No reference counterpart: the number of kernels one qt_bc1_encode_device or
+ * qt_bc3_encode_device call on a width x height texture launches on the current
+ * device with these params (1 = the encoder; 2 = a split pass that writes the solid
+ * blocks, then the encoder; 3 = split, encoder, then EndpointSearch as its own pass).
+ * The host entry points launch this per band. params->color_mode is not checked. */
+int qt_bc1_encode_kernels(int width, int height, const qt_bc1_params *params, int *kernels);
+
 /* BC4Encoder(channel)::Encode -> EncodeBlock (BC4Encoder.cpp:30-71). */
 int qt_bc4_encode_host(const uint8_t *rgba, int width, int height, int channel, uint8_t *blocks);
 int qt_bc4_encode_device(const uint8_t *rgba, int width, int height, int channel, uint8_t *blocks, void *stream);

@@ -31,7 +31,7 @@ EXPORTS = (
     "qt_batch_last_tiles", "qt_batch_reserve", "qt_copy_async", "qt_batch_run_noalloc",
     "qt_server_create", "qt_server_destroy", "qt_server_set_rules", "qt_server_set_grid", "qt_server_submit",
     "qt_server_poll", "qt_server_get_stats", "qt_server_clock",
-    "qt_resize_bilinear_device", "qt_flip_swizzle_device",
+    "qt_resize_bilinear_device", "qt_flip_swizzle_device", "qt_bc1_encode_kernels",
 )
 
 
@@ -77,6 +77,7 @@ def lib() -> ctypes.CDLL:
             "qt_bc5_encode_host": [_vp, _i, _i, _i, _i, _vp],
             "qt_bc1_encode_device": [_vp, _i, _i, P, _vp, _vp],
             "qt_bc3_encode_device": [_vp, _i, _i, P, _vp, _vp],
+            "qt_bc1_encode_kernels": [_i, _i, P, ctypes.POINTER(_i)],
             "qt_bc4_encode_device": [_vp, _i, _i, _i, _vp, _vp],
             "qt_bc5_encode_device": [_vp, _i, _i, _i, _i, _vp, _vp],
             "qt_bc1_decode_host": [_vp, _i, _i, _i, _i, _vp],
@@ -186,6 +187,13 @@ def bc1_encode_device(d_rgba: int, w: int, h: int, params: BC1Params, d_out: int
 
 def bc3_encode_device(d_rgba: int, w: int, h: int, params: BC1Params, d_out: int, stream: int = 0) -> None:
     check(lib().qt_bc3_encode_device(_vp(d_rgba), w, h, ctypes.byref(params), _vp(d_out), _vp(stream)))
+
+
+def bc1_encode_kernels(w: int, h: int, params: BC1Params) -> int:
+    """Kernels one bc1/bc3 device encode call of a w x h texture launches on the current device."""
+    n = ctypes.c_int(0)
+    check(lib().qt_bc1_encode_kernels(w, h, ctypes.byref(params), ctypes.byref(n)))
+    return n.value
 
 
 def bc4_encode_device(d_rgba: int, w: int, h: int, channel: int, d_out: int, stream: int = 0) -> None:

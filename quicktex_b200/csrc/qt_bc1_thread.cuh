@@ -437,24 +437,59 @@ template <int IT> __device__ __forceinline__ R refine_ls_any(int K, R r, const M
 }
 
 // RefineBlockCF<M> (BC1Encoder.cpp:877-928): the reference's loop as written
-template <int IT, int K> __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool exhaustive, int pp_sum) {
+// OrderTable::GetHash of the selectors' histogram (OrderTable.h:91-104), the first
+// ordering of RefineBlockCF (BC1Encoder.cpp:886-889)
+__device__ __forceinline__ int cf_start_hash(bool four, uint32_t w) {
+    const int n1 = __popc(w & ~(w >> 1) & 0x55555555u), n2 = __popc(~w & (w >> 1) & 0x55555555u);
+    const int n3 = __popc(w & (w >> 1) & 0x55555555u), n0 = 16 - n1 - n2 - n3;
+    if (four) return n0 == 16 ? 15 : n1 == 16 ? 700 : n2 == 16 ? 753 : n3 == 16 ? 515 : (int)g_tab.hash4[n0 | (n1 << 4) | (n2 << 8)];
+    return n0 == 16 ? 12 : n1 == 16 ? 15 : n2 == 16 ? 89 : (int)g_tab.hash3[n0 | (n1 << 4)];
+}
+
+// RefineBlockCF's sort key of texel i (BC1Encoder.cpp:895-900): its dot with the axis, then i
+__device__ __forceinline__ uint32_t cf_key(uint32_t v, int axr, int axg, int axb, int i) {
+    return ((uint32_t)(0x1000000 + cr(v) * axr + cg(v) * axg + cb(v) * axb) << 4) | (uint32_t)i;
+}
+
+// RefineBlockCF's trials (BC1Encoder.cpp:905-927) depend on its input only through the
+// start hash (the histogram of the input selectors) and the texel order along the input's
+// axis; its single-colour trial depends on neither. A second pass whose input gives the
+// same hash and order as the first pass's input runs the same trials against a best error
+// that is already the minimum of them, so it changes nothing. True when r (the first
+// pass's result) gives start hash `start` and texel order `order` (rank k -> texel in
+// nibble k).
+__device__ __forceinline__ bool cf_same_trials(bool four, const R &r, int start, uint64_t order) {
+    if (cf_start_hash(four, r.sel) != start) return false;
+    const int axr = s5to8(epr(r.hi)) - s5to8(epr(r.lo));
+    const int axg = s6to8(epg(r.hi)) - s6to8(epg(r.lo));
+    const int axb = s5to8(epb(r.hi)) - s5to8(epb(r.lo));
+    // the keys under r's axis, read in the first pass's order, must still increase
+    int i = (int)(order & 0xF);
+    uint32_t prev = cf_key(px(i), axr, axg, axb, i);
+    bool same = true;
+#pragma unroll 4
+    for (int k = 1; k < 16; k++) {
+        i = (int)((order >> (4 * k)) & 0xF);
+        const uint32_t key = cf_key(px(i), axr, axg, axb, i);
+        same &= prev < key;
+        prev = key;
+    }
+    return same;
+}
+
+// With ORDER, *order_out receives the texel order of the input (rank k -> texel in nibble k).
+template <int IT, int K, bool ORDER = false>
+__device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool exhaustive, int pp_sum, uint64_t *order_out = nullptr) {
     constexpr bool four = !kind_three(K);
     const int tid = threadIdx.x;
     const R orig = r;
-    const uint32_t w = orig.sel;
-    const int n1 = __popc(w & ~(w >> 1) & 0x55555555u), n2 = __popc(~w & (w >> 1) & 0x55555555u);
-    const int n3 = __popc(w & (w >> 1) & 0x55555555u), n0 = 16 - n1 - n2 - n3;
-    int start;
-    if (four) start = n0 == 16 ? 15 : n1 == 16 ? 700 : n2 == 16 ? 753 : n3 == 16 ? 515 : (int)g_tab.hash4[n0 | (n1 << 4) | (n2 << 8)];
-    else start = n0 == 16 ? 12 : n1 == 16 ? 15 : n2 == 16 ? 89 : (int)g_tab.hash3[n0 | (n1 << 4)];
+    const int start = cf_start_hash(four, orig.sel);
     // projection keys, rank by counting (keys are distinct), prefix sums in rank order
     const int axr = s5to8(epr(orig.hi)) - s5to8(epr(orig.lo));
     const int axg = s6to8(epg(orig.hi)) - s6to8(epg(orig.lo));
     const int axb = s5to8(epb(orig.hi)) - s5to8(epb(orig.lo));
-    for (int i = 0; i < 16; i++) {
-        const uint32_t v = px(i);
-        t_key[i][tid] = ((uint32_t)(0x1000000 + cr(v) * axr + cg(v) * axg + cb(v) * axb) << 4) | (uint32_t)i;
-    }
+    for (int i = 0; i < 16; i++) t_key[i][tid] = cf_key(px(i), axr, axg, axb, i);
+    uint64_t order = 0;
     for (int i = 0; i < 16; i++) {  // t_srg/t_sb[k] first hold the colour of rank k-1
         const uint32_t ki = t_key[i][tid];
         int rank = 0;
@@ -463,7 +498,9 @@ template <int IT, int K> __device__ __noinline__ R refine_cf(R r, const M &m, un
         const uint32_t v = px(i);
         t_srg[rank + 1][tid] = (uint32_t)cr(v) | ((uint32_t)cg(v) << 16);
         t_sb[rank + 1][tid] = (uint16_t)cb(v);
+        if (ORDER) order |= (uint64_t)i << (4 * rank);
     }
+    if (ORDER) *order_out = order;
     uint32_t arg = 0, ab = 0;
     t_srg[0][tid] = 0;
     t_sb[0][tid] = 0;
@@ -548,13 +585,14 @@ template <int IT, int K> __device__ __noinline__ R endpoint_search(R r, unsigned
     return r;
 }
 
-template <int IT> __device__ __forceinline__ R refine_cf_any(int K, R r, const M &m, unsigned o, bool ex, int pp) {
+template <int IT, bool ORDER = false>
+__device__ __forceinline__ R refine_cf_any(int K, R r, const M &m, unsigned o, bool ex, int pp, uint64_t *order = nullptr) {
     switch (K) {
-        case K_F4_NONE: return refine_cf<IT, K_F4_NONE>(r, m, o, ex, pp);
-        case K_F4_FASTER: return refine_cf<IT, K_F4_FASTER>(r, m, o, ex, pp);
-        case K_F4_CHECK2: return refine_cf<IT, K_F4_CHECK2>(r, m, o, ex, pp);
-        case K_F4_FULL: return refine_cf<IT, K_F4_FULL>(r, m, o, ex, pp);
-        default: return refine_cf<IT, K_T3>(r, m, o, ex, pp);
+        case K_F4_NONE: return refine_cf<IT, K_F4_NONE, ORDER>(r, m, o, ex, pp, order);
+        case K_F4_FASTER: return refine_cf<IT, K_F4_FASTER, ORDER>(r, m, o, ex, pp, order);
+        case K_F4_CHECK2: return refine_cf<IT, K_F4_CHECK2, ORDER>(r, m, o, ex, pp, order);
+        case K_F4_FULL: return refine_cf<IT, K_F4_FULL, ORDER>(r, m, o, ex, pp, order);
+        default: return refine_cf<IT, K_T3, ORDER>(r, m, o, ex, pp, order);
     }
 }
 
@@ -579,56 +617,27 @@ __device__ __forceinline__ uint2 write(const R &r) {
     return write_block(g);
 }
 
-// A block whose EndpointSearch runs later, in k_bc1_search: its result so far and
-// the queue of its colour mode (0 four-colour, 1 three-colour, 2 three-colour + black).
+// A block whose remaining work runs later in a pass of its own: its result so far.
+// need: EndpointSearch, in k_bc1_search; queue is the search queue of its colour mode
+// (0 four-colour, 1 three-colour, 2 three-colour + black).
+// cf2: the rest of EncodeBlock after the first four-colour cluster-fit pass, in k_bc1_cf2:
+// the second pass when pass2, then the 3-colour trials; orig holds the endpoints the
+// 3-colour trial starts from.
 struct Deferred {
-    bool need;
+    bool need, cf2, pass2;
     int queue;
-    R r;
+    R r, orig;
 };
 
-// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342), one thread. With `d`, a block
-// that needs EndpointSearch stops before it and is returned in *d instead.
+// EncodeBlock from the 3-colour trials on (BC1Encoder.cpp:305-341): res is the
+// four-colour result after its cluster-fit passes, orig the endpoints before the
+// four-colour refinement. With `d`, a block that needs EndpointSearch stops before it
+// and is returned in *d instead.
 template <int IT>
-__device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_mode, int pp_sum, Deferred *d = nullptr) {
-    const uint32_t c0 = px(0);
-    bool solid = true;
-    for (int i = 1; i < 16; i++) solid &= px(i) == c0;
-    if (solid) return write_block_solid<IT>(c0);
-
-    const M m = metrics(false);
+__device__ __forceinline__ uint2 encode_tail(const qt_bc1_params &p, int color_mode, int pp_sum, const M &m, R res,
+                                             const R &orig, Deferred *d) {
     const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
-    bool needs_err = use_likely;
-    needs_err |= color_mode == CM_THREE;
-    needs_err |= (color_mode == CM_TB) && m.has_black;
-    needs_err |= p.error_mode != EM_NONE;
-    needs_err |= p.search_rounds > 0;
-    const int em = needs_err ? p.error_mode : EM_NONE;
     const int ls_passes = p.two_ls_passes ? 2 : 1, cf_passes = p.two_cf_passes ? 2 : 1;
-    const int ep_passes = (needs_err && p.two_ep_passes) ? 2 : 1;
-    const int k4 = kind_for(CM_FOUR, em);
-
-    R orig = rinit(), res = rinit();
-    for (int round = 0; round < ep_passes; round++) {
-        const int2 ep = find_endpoints(m, round == 1 ? EP_BB : p.endpoint_mode, false, (int)p.power_iterations);
-        R to = rinit();
-        to.lo = ep.x;
-        to.hi = ep.y;
-        R tr = to;
-        const uint2 se = fs_any<IT>(k4, tr.lo, tr.hi);
-        tr.sel = se.x;
-        tr.err = se.y;
-        tr.mode = CM_FOUR;
-        tr = refine_ls_any<IT>(k4, tr, m, ls_passes);
-        if (!needs_err || tr.err < res.err) {
-            res = tr;
-            orig = to;
-        }
-    }
-    if (res.err > 0 && use_likely)
-        for (int it = 0; it < cf_passes; it++)
-            res = refine_cf_any<IT>(kind_for(CM_FOUR, p.error_mode), res, m, p.orderings4, p.exhaustive, pp_sum);
-
     if (res.err > 0 && (color_mode & CM_THREE)) {
         R t = orig;
         const uint2 se = find_selectors<IT, K_T3>(t.lo, t.hi);
@@ -666,6 +675,69 @@ __device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_
         res = search_any<IT>(kind_for(Md, Md == CM_FOUR ? p.error_mode : EM_FULL), res, p.search_rounds, pp_sum);
     }
     return write(res);
+}
+
+// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342), one thread. With `d`, a block that
+// needs EndpointSearch stops before it, and at settings with two four-colour cluster-fit
+// passes a block stops after the first when the second can change its result or when the
+// 3-colour trials follow; either is returned in *d instead.
+template <int IT>
+__device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_mode, int pp_sum, Deferred *d = nullptr) {
+    const uint32_t c0 = px(0);
+    bool solid = true;
+    for (int i = 1; i < 16; i++) solid &= px(i) == c0;
+    if (solid) return write_block_solid<IT>(c0);
+
+    const M m = metrics(false);
+    const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
+    bool needs_err = use_likely;
+    needs_err |= color_mode == CM_THREE;
+    needs_err |= (color_mode == CM_TB) && m.has_black;
+    needs_err |= p.error_mode != EM_NONE;
+    needs_err |= p.search_rounds > 0;
+    const int em = needs_err ? p.error_mode : EM_NONE;
+    const int ls_passes = p.two_ls_passes ? 2 : 1, cf_passes = p.two_cf_passes ? 2 : 1;
+    const int ep_passes = (needs_err && p.two_ep_passes) ? 2 : 1;
+    const int k4 = kind_for(CM_FOUR, em);
+
+    R orig = rinit(), res = rinit();
+    for (int round = 0; round < ep_passes; round++) {
+        const int2 ep = find_endpoints(m, round == 1 ? EP_BB : p.endpoint_mode, false, (int)p.power_iterations);
+        R to = rinit();
+        to.lo = ep.x;
+        to.hi = ep.y;
+        R tr = to;
+        const uint2 se = fs_any<IT>(k4, tr.lo, tr.hi);
+        tr.sel = se.x;
+        tr.err = se.y;
+        tr.mode = CM_FOUR;
+        tr = refine_ls_any<IT>(k4, tr, m, ls_passes);
+        if (!needs_err || tr.err < res.err) {
+            res = tr;
+            orig = to;
+        }
+    }
+    if (res.err > 0 && use_likely) {
+        const int kcf = kind_for(CM_FOUR, p.error_mode);
+        if (d && cf_passes == 2) {
+            const int start = cf_start_hash(true, res.sel);
+            uint64_t order = 0;
+            res = refine_cf_any<IT, true>(kcf, res, m, p.orderings4, p.exhaustive, pp_sum, &order);
+            // a zero error cannot drop further; the same trials cannot beat their own minimum
+            const bool pass2 = res.err > 0 && !cf_same_trials(true, res, start, order);
+            if (pass2 || (res.err > 0 && (color_mode & CM_THREE))) {
+                d->cf2 = true;
+                d->pass2 = pass2;
+                d->r = res;
+                d->orig = orig;
+                return make_uint2(0u, 0u);
+            }
+        } else {
+            for (int it = 0; it < cf_passes; it++)
+                res = refine_cf_any<IT>(kcf, res, m, p.orderings4, p.exhaustive, pp_sum);
+        }
+    }
+    return encode_tail<IT>(p, color_mode, pp_sum, m, res, orig, d);
 }
 
 }  // namespace tpb
@@ -770,17 +842,72 @@ struct SearchQueues {
     long cap;
 };
 
-template <int IT>
-__global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_defer(const uint8_t *__restrict__ rgba, int w, int h, int bw,
-                                                                  qt_bc1_params p, uint8_t *__restrict__ out, int bc3,
-                                                                  int aligned, const uint32_t *__restrict__ list,
-                                                                  const uint32_t *__restrict__ count, SearchQueues q) {
+// Blocks whose EncodeBlock continues in k_bc1_cf2 after the first four-colour cluster-fit
+// pass (one entry per block: its index, the result after the first pass, the endpoints
+// before refinement). Entries that run the second pass fill the arrays from the front,
+// entries that only run the 3-colour trials from the back, so warps of k_bc1_cf2 see one
+// kind.
+struct Cf2Queue {
+    uint32_t *count;  // [2]: second-pass entries, 3-colour-only entries
+    uint32_t *b, *lohi, *err, *sel, *mode, *orig;  // [cap] each
+    long cap;
+};
+
+__device__ __forceinline__ uint32_t pack_lohi(const tpb::R &r) { return (uint32_t)r.lo | ((uint32_t)r.hi << 16); }
+
+// Appends the lanes' deferred searches to their queues (warp-aggregated). Every lane of
+// the warp calls it.
+__device__ __forceinline__ void push_searches(const SearchQueues &q, const tpb::Deferred &d, long b, int lane) {
+#pragma unroll
+    for (int qq = 0; qq < 3; qq++) {
+        const bool mine = d.need && d.queue == qq;
+        const uint32_t m = __ballot_sync(0xffffffffu, mine);
+        if (!m) continue;
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(q.count + qq, (uint32_t)__popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (mine) {
+            const long slot = (long)qq * q.cap + base + __popc(m & ((1u << lane) - 1));
+            q.b[slot] = (uint32_t)b;
+            q.lohi[slot] = pack_lohi(d.r);
+            q.err[slot] = d.r.err;
+            q.sel[slot] = d.r.sel;
+            q.mode[slot] = (uint32_t)d.r.mode;
+        }
+    }
+}
+
+__device__ __forceinline__ void load_tables_smem() {
     for (int i = threadIdx.x; i < 64; i += blockDim.x) {
         if (i < 32) s_mid5[i] = c_mid5[i];
         s_mid6[i] = c_mid6[i];
         if (i < 16) s_vox[i] = c_voxels[i];
     }
     __syncthreads();
+}
+
+// the block's texels into the thread's shared-memory column; returns sum |p|^2
+__device__ __forceinline__ int stage_block(const uint8_t *__restrict__ rgba, int w, int h, int bw, long b, int aligned,
+                                           uint32_t v[16]) {
+    const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+    load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
+    int pp = 0;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        tpb::t_px[k][threadIdx.x] = v[k];
+        const uint32_t u = v[k] & 0x00FFFFFFu;
+        pp += (int)__dp4a(u, u, 0u);
+    }
+    return pp;
+}
+
+template <int IT>
+__global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_defer(const uint8_t *__restrict__ rgba, int w, int h, int bw,
+                                                                  qt_bc1_params p, uint8_t *__restrict__ out, int bc3,
+                                                                  int aligned, const uint32_t *__restrict__ list,
+                                                                  const uint32_t *__restrict__ count, SearchQueues q,
+                                                                  Cf2Queue c) {
+    load_tables_smem();
     const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
     const int lane = threadIdx.x & 31;
     const long end = (long)*count, stride = (long)gridDim.x * blockDim.x;
@@ -788,48 +915,88 @@ __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_defer(const uint8_t *_
     for (long wb = (long)blockIdx.x * blockDim.x + threadIdx.x - lane; wb < end; wb += stride) {
         const long i = wb + lane;
         tpb::Deferred d;
-        d.need = false;
+        d.need = d.cf2 = d.pass2 = false;
         d.queue = 0;
         long b = 0;
         if (i < end) {
             b = (long)list[i];
-            const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
             uint32_t v[16];
-            load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
-            int pp = 0;
-#pragma unroll
-            for (int k = 0; k < 16; k++) {
-                tpb::t_px[k][threadIdx.x] = v[k];
-                const uint32_t u = v[k] & 0x00FFFFFFu;
-                pp += (int)__dp4a(u, u, 0u);
-            }
+            const int pp = stage_block(rgba, w, h, bw, b, aligned, v);
             const uint2 blk = tpb::encode_block<IT>(p, color_mode, pp, &d);
-            if (bc3) {  // the alpha half now; a queued block's colour half is written by k_bc1_search
+            if (bc3) {  // the alpha half now; a queued block's colour half is written by a later pass
 #pragma unroll
                 for (int k = 0; k < 16; k++) v[k] = tpb::t_px[k][threadIdx.x];
                 const uint2 a = bc4_block_thread(v, 3);
                 reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
-            } else if (!d.need) {
+            } else if (!d.need && !d.cf2) {
                 reinterpret_cast<uint2 *>(out)[b] = blk;
             }
         }
+        push_searches(q, d, b, lane);
 #pragma unroll
-        for (int qq = 0; qq < 3; qq++) {
-            const bool mine = d.need && d.queue == qq;
+        for (int kind = 0; kind < 2; kind++) {
+            const bool mine = d.cf2 && d.pass2 == (kind == 0);
             const uint32_t m = __ballot_sync(0xffffffffu, mine);
             if (!m) continue;
             uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(q.count + qq, (uint32_t)__popc(m));
+            if (lane == 0) base = atomicAdd(c.count + kind, (uint32_t)__popc(m));
             base = __shfl_sync(0xffffffffu, base, 0);
             if (mine) {
-                const long slot = (long)qq * q.cap + base + __popc(m & ((1u << lane) - 1));
-                q.b[slot] = (uint32_t)b;
-                q.lohi[slot] = (uint32_t)d.r.lo | ((uint32_t)d.r.hi << 16);
-                q.err[slot] = d.r.err;
-                q.sel[slot] = d.r.sel;
-                q.mode[slot] = (uint32_t)d.r.mode;
+                const long idx = (long)base + __popc(m & ((1u << lane) - 1));
+                const long slot = kind == 0 ? idx : c.cap - 1 - idx;
+                c.b[slot] = (uint32_t)b;
+                c.lohi[slot] = pack_lohi(d.r);
+                c.err[slot] = d.r.err;
+                c.sel[slot] = d.r.sel;
+                c.mode[slot] = (uint32_t)d.r.mode;
+                c.orig[slot] = pack_lohi(d.orig);
             }
         }
+    }
+}
+
+// The queued blocks' second four-colour cluster-fit pass (BC1Encoder.cpp:300-302), for the
+// entries that need it, and the rest of EncodeBlock after it; their searches go to the
+// search queues. Entries of one kind are uniform work, so a plain grid-stride loop over the
+// second-pass entries, then the others, keeps warps full.
+template <int IT>
+__global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_cf2(const uint8_t *__restrict__ rgba, int w, int h, int bw,
+                                                                qt_bc1_params p, uint8_t *__restrict__ out, int bc3,
+                                                                int aligned, Cf2Queue c, SearchQueues q) {
+    load_tables_smem();
+    const int color_mode = bc3 ? CM_FOUR : p.color_mode;
+    const int lane = threadIdx.x & 31;
+    const long n2 = (long)c.count[0], end = n2 + (long)c.count[1], stride = (long)gridDim.x * blockDim.x;
+    for (long wb = (long)blockIdx.x * blockDim.x + threadIdx.x - lane; wb < end; wb += stride) {
+        const long idx = wb + lane;
+        tpb::Deferred d;
+        d.need = d.cf2 = d.pass2 = false;
+        d.queue = 0;
+        long b = 0;
+        if (idx < end) {
+            const bool pass2 = idx < n2;
+            const long i = pass2 ? idx : c.cap - 1 - (idx - n2);
+            b = (long)c.b[i];
+            uint32_t v[16];
+            const int pp = stage_block(rgba, w, h, bw, b, aligned, v);
+            const tpb::M m = tpb::metrics(false);
+            tpb::R res, orig = tpb::rinit();
+            const uint32_t lh = c.lohi[i], ol = c.orig[i];
+            res.lo = (int)(lh & 0xFFFF);
+            res.hi = (int)(lh >> 16);
+            res.err = c.err[i];
+            res.sel = c.sel[i];
+            res.mode = (int)c.mode[i];
+            orig.lo = (int)(ol & 0xFFFF);
+            orig.hi = (int)(ol >> 16);
+            if (pass2) res = tpb::refine_cf_any<IT>(kind_for(CM_FOUR, p.error_mode), res, m, p.orderings4, p.exhaustive, pp);
+            const uint2 blk = tpb::encode_tail<IT>(p, color_mode, pp, m, res, orig, &d);
+            if (!d.need) {
+                if (bc3) reinterpret_cast<uint2 *>(out)[2 * b + 1] = blk;  // the colour half of the 16-byte block
+                else reinterpret_cast<uint2 *>(out)[b] = blk;
+            }
+        }
+        push_searches(q, d, b, lane);
     }
 }
 
@@ -862,16 +1029,8 @@ __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__
                     r.err = q.err[slot];
                     r.sel = q.sel[slot];
                     r.mode = (int)q.mode[slot];
-                    const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
                     uint32_t v[16];
-                    load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
-                    pp = 0;
-#pragma unroll
-                    for (int k = 0; k < 16; k++) {
-                        tpb::t_px[k][threadIdx.x] = v[k];
-                        const uint32_t u = v[k] & 0x00FFFFFFu;
-                        pp += (int)__dp4a(u, u, 0u);
-                    }
+                    pp = stage_block(rgba, w, h, bw, b, aligned, v);
                     forbidden = -1;
                     prev = 0;
                     i = 0;
@@ -919,12 +1078,7 @@ template <int IT>
 __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_search(const uint8_t *__restrict__ rgba, int w, int h, int bw,
                                                                    qt_bc1_params p, uint8_t *__restrict__ out, int bc3,
                                                                    int aligned, SearchQueues q) {
-    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
-        if (i < 32) s_mid5[i] = c_mid5[i];
-        s_mid6[i] = c_mid6[i];
-        if (i < 16) s_vox[i] = c_voxels[i];
-    }
-    __syncthreads();
+    load_tables_smem();
     const unsigned rounds = p.search_rounds;
     switch (p.error_mode) {  // four-colour searches use the encoder's error mode (kind_for)
         case EM_NONE: search_queue<IT, K_F4_NONE>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;

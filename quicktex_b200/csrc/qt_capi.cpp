@@ -530,6 +530,15 @@ int qt_bc3_encode_device(const uint8_t *rgba, int w, int h, const qt_bc1_params 
     return finish_launch(qtk::launch_bc1_encode(rgba, w, h, *p, blocks, true, stream), "bc3 encode");
 }
 
+int qt_bc1_encode_kernels(int w, int h, const qt_bc1_params *p, int *kernels) {
+    int rc;
+    if ((rc = check_dims(w, h)) || (rc = check_params(p, true)) || (rc = check_ptr(kernels, 4, "kernels")) ||
+        (rc = ensure_device(nullptr)))
+        return rc;
+    *kernels = qtk::bc1_encode_kernels((long)((w + 3) / 4) * ((h + 3) / 4), *p);
+    return QT_OK;
+}
+
 int qt_bc4_encode_device(const uint8_t *rgba, int w, int h, int channel, uint8_t *blocks, void *stream) {
     int rc;
     if ((rc = check_dims(w, h)) || (rc = check_channel(channel)) || (rc = check_ptr(rgba, 4, "rgba")) ||

@@ -77,6 +77,9 @@ int launch_bc4_encode_range(const uint8_t *rgba, int w, int h, int c0, int c1, b
 // The fewest blocks for which a BC1/BC3 launch with EndpointSearch runs the search as its own
 // refill pass (two searches per resident lane of that pass).
 long defer_min_blocks();
+// kernels one launch_bc1_encode_range over n blocks issues (0 for none): the encoder, plus the
+// split pass from kSplitMinBlocks blocks, plus the search pass from defer_min_blocks() blocks
+int bc1_encode_kernels(long n, const qt_bc1_params &p);
 int launch_decode_range(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
                         uint8_t *rgba, long b_begin, long b_end, void *stream);
 // fmt: 1 = BC1, 3 = BC3, 4 = BC4, 5 = BC5

@@ -1531,6 +1531,12 @@ constexpr long kSplitMinBlocks = 16384;
 
 long defer_min_blocks() { return 2L * num_sms() * 4 * tpb::kThreads; }
 
+// the four-colour cluster fit runs twice (EncodeBlock, BC1Encoder.cpp:299-302); exactly then
+// encode_block, given a Deferred, stops blocks before the second pass
+static bool cf2_pass(const qt_bc1_params &p) {
+    return p.two_cf_passes && (p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0);
+}
+
 int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
                             long b_begin, long b_end, void *stream) {
     const int bw = (w + 3) / 4;
@@ -1555,7 +1561,10 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
         // search kernel: below that no lane gets a second entry to refill from, and the extra
         // pass costs more than it saves (measured at L18: -5% at 1024^2, +10% at 2048^2)
         const bool defer = p.search_rounds > 0 && n >= defer_min_blocks();
-        const size_t words = 64 + (size_t)n + (defer ? 15 * (size_t)n : 0);
+        // and the second four-colour cluster-fit pass, when there is one, runs in its own pass
+        // for the blocks where it can change the result
+        const bool cf2 = defer && cf2_pass(p);
+        const size_t words = 64 + (size_t)n + (defer ? 15 * (size_t)n : 0) + (cf2 ? 6 * (size_t)n : 0);
         uint32_t *scratch = nullptr;
         cudaError_t e = scratch_alloc((void **)&scratch, words * sizeof(uint32_t), s);
         if (e != cudaSuccess) return (int)e;
@@ -1572,12 +1581,25 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
             q.err = qb + 6 * (size_t)n;
             q.sel = qb + 9 * (size_t)n;
             q.mode = qb + 12 * (size_t)n;
+            Cf2Queue c{};
+            if (cf2) {
+                uint32_t *cb = qb + 15 * (size_t)n;
+                c.count = scratch + 8;
+                c.b = cb;
+                c.lohi = cb + (size_t)n;
+                c.err = cb + 2 * (size_t)n;
+                c.sel = cb + 3 * (size_t)n;
+                c.mode = cb + 4 * (size_t)n;
+                c.orig = cb + 5 * (size_t)n;
+                c.cap = n;
+            }
             const int gs = grid_for(n, 256);
             const int gsearch = num_sms() * 4;
             switch (p.interpolator) {
 #define QT_DEFER(I)                                                                                                        \
     k_bc1_split<I><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count);                      \
-    k_bc1_defer<I><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, list, count, q);                       \
+    k_bc1_defer<I><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, list, count, q, c);                    \
+    if (cf2) k_bc1_cf2<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, c, q);                    \
     k_bc1_search<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, q);
                 case IT_IDEAL: QT_DEFER(IT_IDEAL) break;
                 case IT_ROUND: QT_DEFER(IT_ROUND) break;
@@ -1619,6 +1641,13 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
         default: k_bc1_encode<IT_AMD><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
     }
     return (int)cudaGetLastError();
+}
+
+int bc1_encode_kernels(long n, const qt_bc1_params &p) {
+    if (n <= 0) return 0;
+    if (bc1_mapping() != 0 || n < kSplitMinBlocks || n > 0xFFFFFFFFL) return 1;
+    if (p.search_rounds == 0 || n < defer_min_blocks()) return 2;
+    return cf2_pass(p) ? 4 : 3;
 }
 
 int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3, void *stream) {

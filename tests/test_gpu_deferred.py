@@ -1,5 +1,6 @@
-"""GPU: the three-pass encoder of large BC1/BC3 textures at levels with
-EndpointSearch (solid blocks written by the split pass, searches queued per
+"""GPU: the multi-pass encoder of large BC1/BC3 textures at levels with
+EndpointSearch (solid blocks written by the split pass, the second cluster-fit
+pass of level 18 queued for the blocks it can change, searches queued per
 colour mode and run by the refill kernel) gives, block for block, the oracle's
 output. A block depends only on its own 16 texels, so block-aligned crops of
 the large texture, encoded by the oracle, pin the corresponding blocks; the
@@ -57,3 +58,49 @@ def test_bc3_deferred_search_matches_oracle(oracle_lib):
         crop = np.ascontiguousarray(img[y:y + 64, x:x + 64])
         exp = oracle_lib.bc3_encode(crop, 64, 64, BC1Params(level=18, color_mode=capi.FOUR_COLOR, interpolator=2))
         assert _crop_blocks(out, 16, x, y) == exp, (x, y)
+
+
+@pytest.mark.parametrize("mode,interp", [(0x04, 0), (0x03, 2), (0x13, 3)])
+def test_bc1_level18_whole_texture_matches_oracle(oracle_lib, mode, interp):
+    """Every block of a 2048^2 texture at level 18, through all four passes (split, encoder,
+    the second cluster-fit pass for the blocks it can change, search), against the oracle."""
+    img = np.ascontiguousarray(syn.block_mix(SIDE, SIDE, workload=14, stream=18 + mode + interp))
+    p = capi.params_for_level(18, mode, interp)
+    assert capi.bc1_encode_kernels(SIDE, SIDE, p) == 4
+    out = _device_encode(capi.bc1_encode_device, img, p, 8)
+    exp = oracle_lib.bc1_encode(img, SIDE, SIDE, BC1Params(level=18, color_mode=mode, interpolator=interp))
+    if out != exp:
+        a, b = np.frombuffer(out, np.uint64), np.frombuffer(exp, np.uint64)
+        bad = np.flatnonzero(a != b)
+        raise AssertionError(f"{bad.size} of {a.size} blocks differ, first at block {bad[0]}")
+
+
+def test_bc3_level18_whole_texture_matches_oracle(oracle_lib):
+    img = np.ascontiguousarray(syn.alpha_mix(SIDE, SIDE, workload=14, stream=181))
+    p = capi.params_for_level(18, capi.FOUR_COLOR, 0)
+    out = _device_encode(capi.bc3_encode_device, img, p, 16)
+    exp = oracle_lib.bc3_encode(img, SIDE, SIDE, BC1Params(level=18, color_mode=capi.FOUR_COLOR, interpolator=0))
+    assert out == exp
+
+
+def test_encode_kernel_count():
+    """qt_bc1_encode_kernels reports the passes one device call launches: the encoder alone on
+    small textures, the split pass first from 16384 blocks, the search pass on top of that for
+    levels with EndpointSearch once the texture holds two searches per resident lane, and the
+    second cluster-fit pass as its own kernel at levels with two of them (level 18)."""
+    import torch
+
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    side_defer = 4 * int(np.ceil(np.sqrt(2 * sms * 4 * 128)))
+    p18, p10 = capi.params_for_level(18), capi.params_for_level(10)
+    assert capi.bc1_encode_kernels(64, 64, p18) == 1
+    assert capi.bc1_encode_kernels(508, 508, p18) == 1  # 127^2 = 16129 blocks
+    assert capi.bc1_encode_kernels(512, 512, p18) == 2  # 16384 blocks
+    assert capi.bc1_encode_kernels(side_defer, side_defer, p10) == 2
+    assert capi.bc1_encode_kernels(side_defer, side_defer, p18) == 4
+    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(13)) == 3
+    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(17)) == 3
+    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(18)) == 4
+    with pytest.raises(capi.QtError) as e:
+        capi.bc1_encode_kernels(0, 64, p18)
+    assert e.value.code == 1
