@@ -215,6 +215,7 @@ class Oracle(_Lib):
     def __init__(self, path: str = ORACLE_SO, tables: str = ORDER_TABLES):
         super().__init__(path)
         self.lib.qo_ce_count.restype = ctypes.c_ulonglong
+        self.lib.qo_ce_repeated_count.restype = ctypes.c_ulonglong
         self.lib.qo_init.argtypes = [ctypes.c_char_p]
         self.lib.qo_init.restype = _i
         if self.lib.qo_init(tables.encode()) != 0:
@@ -225,6 +226,12 @@ class Oracle(_Lib):
         """Candidate evaluations (SSD + select of one texel vs one palette colour)
         performed by the encodes since the last ``ce_reset``."""
         return int(self.lib.qo_ce_count())
+
+    def ce_repeated_count(self) -> int:
+        """Of ``ce_count``, the evaluations in second four-colour cluster-fit passes that repeat
+        the first pass's trials (same start hash and texel order, or zero error), which cannot
+        change the result."""
+        return int(self.lib.qo_ce_repeated_count())
 
     def ce_reset(self) -> None:
         self.lib.qo_ce_reset()

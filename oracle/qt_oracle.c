@@ -41,6 +41,16 @@ static __thread char g_err[256];
  * the endpoint search stop rule) are honoured because they stop the calls. */
 static __thread unsigned long long t_ce;
 static unsigned long long g_ce;
+/* The part of t_ce spent in second four-colour cluster-fit passes that repeat the first
+ * pass's trials: the pass's input gives the same start hash and texel order as the first
+ * pass's input (or its error is already 0), so it cannot change the result. An encoder may
+ * skip them with identical output; counted so that executed work can be told apart from
+ * the reference's. */
+static __thread unsigned long long t_ce_rep;
+static unsigned long long g_ce_rep;
+/* the start hash and texel order of the last refine_block_cf's input */
+static __thread int t_cf_start;
+static __thread uint32_t t_cf_order[16];
 static int fail(const char *m) { snprintf(g_err, sizeof g_err, "%s", m); return 1; }
 const char *qo_last_error(void) { return g_err; }
 
@@ -668,6 +678,8 @@ static void refine_block_cf(const bc1p_t *p, int M, result_t *r, const color_t p
         dots[i] = ((uint32_t)dot << 4) | (uint32_t)i;
     }
     qsort(dots, 16, sizeof dots[0], cmp_u32);
+    t_cf_start = start;
+    for (int i = 0; i < 16; i++) t_cf_order[i] = dots[i] & 0xF;
     float sums[17][4];
     memset(sums, 0, sizeof sums);
     for (int i = 0; i < 16; i++) {
@@ -816,8 +828,21 @@ static void encode_bc1_block(const bc1p_t *p, const color_t px[16], uint8_t out[
         refine_block_ls(p, CM_FOUR, &tr, px, &m, em, ls_passes);
         if (!needs_err || tr.error < res.error) { res = tr; orig = to; }
     }
-    if (res.error > 0 && use_likely)
-        for (unsigned it = 0; it < cf_passes; it++) refine_block_cf(p, CM_FOUR, &res, px, &m, p->error_mode, p->orderings4);
+    if (res.error > 0 && use_likely) {
+        int start1 = 0;
+        uint32_t order1[16];
+        for (unsigned it = 0; it < cf_passes; it++) {
+            const unsigned long long ce0 = t_ce;
+            const unsigned err0 = res.error;
+            refine_block_cf(p, CM_FOUR, &res, px, &m, p->error_mode, p->orderings4);
+            if (it == 0) {
+                start1 = t_cf_start;
+                memcpy(order1, t_cf_order, sizeof order1);
+            } else if (err0 == 0 || (t_cf_start == start1 && !memcmp(t_cf_order, order1, sizeof order1))) {
+                t_ce_rep += t_ce - ce0;
+            }
+        }
+    }
 
     if (res.error > 0 && (p->color_mode & CM_THREE)) {
         result_t t = orig;
@@ -918,18 +943,21 @@ static int encode_texture(const uint8_t *rgba, int w, int h, const void *ctx, bl
         for (long i = 0; i < n; i++) {
             color_t px[16];
             get_block(rgba, w, h, (int)(i % bw), (int)(i / bw), px);
-            t_ce = 0;
+            t_ce = t_ce_rep = 0;
             fn(ctx, px, out + i * bsize);
 #pragma omp atomic
             g_ce += t_ce;
+#pragma omp atomic
+            g_ce_rep += t_ce_rep;
         }
     } else {
         for (long i = 0; i < n; i++) {
             color_t px[16];
             get_block(rgba, w, h, (int)(i % bw), (int)(i / bw), px);
-            t_ce = 0;
+            t_ce = t_ce_rep = 0;
             fn(ctx, px, out + i * bsize);
             g_ce += t_ce;
+            g_ce_rep += t_ce_rep;
         }
     }
     return 0;
@@ -974,7 +1002,9 @@ static int make_params(bc1p_t *p, int level, int color_mode, int interp, const i
 /* ------------------------------------------------------------------------- */
 /* total candidate evaluations of the encodes since the last reset */
 unsigned long long qo_ce_count(void) { return g_ce; }
-void qo_ce_reset(void) { g_ce = 0; }
+/* of those, the evaluations in repeated second cluster-fit passes */
+unsigned long long qo_ce_repeated_count(void) { return g_ce_rep; }
+void qo_ce_reset(void) { g_ce = g_ce_rep = 0; }
 
 int qo_num_threads(void) {
 #ifdef _OPENMP

@@ -3,7 +3,7 @@
 Run where the reference source tree exists (it builds and runs the unmodified
 reference, oracle/_ref/libqtref.so):
 
-    python tests/golden/make_golden.py [--skip-full]
+    python tests/golden/make_golden.py [--skip-full | --ce-only]
 
 Writes
   kat.json         the reference's own known-answer vectors: the 4x4 PNG
@@ -19,7 +19,11 @@ Writes
                    against the oracle restatement (qt_oracle.c) before writing.
   ce_counts.json   candidate evaluations per block (the algorithmic work unit
                    of the BC1 issue roofline) counted by the oracle on the
-                   4096^2 workload for each of its 36 settings.
+                   4096^2 workload for each of its 36 settings, and the part of
+                   them in second cluster-fit passes that repeat the first
+                   pass's trials (work an encoder may skip with identical
+                   output). --ce-only writes only this file, from the oracle
+                   alone.
 """
 
 from __future__ import annotations
@@ -82,10 +86,42 @@ def checked(name, ref_out, orc_out):
     return sha(ref_out)
 
 
+def write_ce_counts(ce: dict, rep: dict) -> None:
+    with open(os.path.join(HERE, "ce_counts.json"), "w") as f:
+        json.dump({"unit": "candidate evaluations per 4x4 block, 4096^2 block_mix workload", "per_block": ce,
+                   "per_block_repeated": rep,
+                   "repeated": "of per_block, the evaluations in second four-colour cluster-fit passes whose "
+                               "input gives the first pass's start hash and texel order (or zero error): "
+                               "they repeat the first pass's trials and cannot change the result"},
+                  f, indent=1)
+
+
+def ce_only() -> None:
+    """ce_counts.json from the oracle alone (the counts need no reference run)."""
+    oracle.build(with_ref=False)
+    orc = oracle.Oracle()
+    orc.set_threads(os.cpu_count())
+    img = syn.block_mix(4096, 4096)
+    ce, rep = {}, {}
+    for L in (0, 10, 18):
+        for mn, m in MODES.items():
+            for iname, it in INTERPS.items():
+                orc.ce_reset()
+                orc.bc1_encode(img, 4096, 4096, BC1Params(level=L, color_mode=m, interpolator=it))
+                ce[f"L{L}_{mn}_{iname}"] = orc.ce_count() / (1024 * 1024)
+                rep[f"L{L}_{mn}_{iname}"] = orc.ce_repeated_count() / (1024 * 1024)
+                print(f"  4096 L{L} {mn} {iname}", flush=True)
+    write_ce_counts(ce, rep)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-full", action="store_true", help="only the 512^2 cases")
+    ap.add_argument("--ce-only", action="store_true", help="only ce_counts.json, from the oracle")
     args = ap.parse_args()
+    if args.ce_only:
+        ce_only()
+        return
 
     oracle.build(with_ref=True)
     ref, orc = oracle.Reference(), oracle.Oracle()
@@ -121,7 +157,7 @@ def main():
                                          "sha256": sha(img)}, "bc1": sweep}
     print(f"512 cases done in {time.time() - t0:.0f}s", flush=True)
 
-    ce = {}
+    ce, rep = {}, {}
     if not args.skip_full:
         img = syn.block_mix(4096, 4096)
         runs = {}
@@ -133,6 +169,7 @@ def main():
                     orc.ce_reset()
                     o = orc.bc1_encode(img, 4096, 4096, p)
                     ce[f"L{L}_{mn}_{iname}"] = orc.ce_count() / (1024 * 1024)
+                    rep[f"L{L}_{mn}_{iname}"] = orc.ce_repeated_count() / (1024 * 1024)
                     runs[f"L{L}_{mn}_{iname}"] = checked(f"4096 L{L} {mn} {iname}", r, o)
                     print(f"  4096 L{L} {mn} {iname} ({time.time() - t0:.0f}s)", flush=True)
         hashes["mix_4096"] = {"input": {"gen": "block_mix", "w": 4096, "h": 4096, "sha256": sha(img)}, "bc1": runs}
@@ -155,8 +192,7 @@ def main():
                                  "bc5_01": checked("bc5", e5, orc.bc5_encode(img, 8192, 8192, 0, 1)),
                                  "bc5_decode_01": checked("bc5 dec", ref.bc5_decode(e5, 8192, 8192, 0, 1),
                                                           orc.bc5_decode(e5, 8192, 8192, 0, 1))}
-        with open(os.path.join(HERE, "ce_counts.json"), "w") as f:
-            json.dump({"unit": "candidate evaluations per 4x4 block, 4096^2 block_mix workload", "per_block": ce}, f, indent=1)
+        write_ce_counts(ce, rep)
 
     with open(os.path.join(HERE, "ref_hashes.json"), "w") as f:
         json.dump(hashes, f, indent=1)
