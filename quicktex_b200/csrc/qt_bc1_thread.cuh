@@ -79,8 +79,8 @@ template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, in
     // against colour k is |p|^2 + v_k - 2 p.c_k, exact in integers (dp4a)
     const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
     const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
-    const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
-    const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
+    const int v0 = (int)__dp4a(c0, c0, 0u), v1 = (int)__dp4a(c1, c1, 0u);
+    const int v2 = (int)__dp4a(c2, c2, 0u), v3 = (int)__dp4a(c3, c3, 0u);
     uint32_t sel = 0, tot = 0;
     if (K == K_F4_NONE || K == K_F4_FASTER) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
@@ -167,8 +167,8 @@ template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo,
     if (K == K_F4_FULL || K == K_T3 || K == K_TB) {
         const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
         const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
-        const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
-        const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
+        const int v0 = (int)__dp4a(c0, c0, 0u), v1 = (int)__dp4a(c1, c1, 0u);
+        const int v2 = (int)__dp4a(c2, c2, 0u), v3 = (int)__dp4a(c3, c3, 0u);
         int t0 = 0, t1 = 0;
 #pragma unroll 2
         for (int i = 0; i < 16; i += 2) {
@@ -193,8 +193,8 @@ template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo,
         // axis is palette entry 3 - entry 0, so p.axis = p.c3 - p.c0 from the same dp4a products.
         const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
         const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
-        const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
-        const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
+        const int v0 = (int)__dp4a(c0, c0, 0u), v1 = (int)__dp4a(c1, c1, 0u);
+        const int v2 = (int)__dp4a(c2, c2, 0u), v3 = (int)__dp4a(c3, c3, 0u);
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
         int t = 0;
         if (K == K_F4_CHECK2) {
@@ -537,10 +537,10 @@ __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool ex
             }
             const float fr = (float)(qrg & 0xFFFF), fg = (float)(qrg >> 16), fb = (float)qb;
             const float q0r = t16r * denom - fr, q0g = t16g * denom - fg, q0b = t16b * denom - fb;
-            t.lo = precise_round565(__fadd_rn(__fmul_rn(f.x, q0r), __fmul_rn(f.y, fr)),
+            t.lo = precise_round565_cf(__fadd_rn(__fmul_rn(f.x, q0r), __fmul_rn(f.y, fr)),
                                     __fadd_rn(__fmul_rn(f.x, q0g), __fmul_rn(f.y, fg)),
                                     __fadd_rn(__fmul_rn(f.x, q0b), __fmul_rn(f.y, fb)), s_mid5, s_mid6);
-            t.hi = precise_round565(__fadd_rn(__fmul_rn(f.z, q0r), __fmul_rn(f.w, fr)),
+            t.hi = precise_round565_cf(__fadd_rn(__fmul_rn(f.z, q0r), __fmul_rn(f.w, fr)),
                                     __fadd_rn(__fmul_rn(f.z, q0g), __fmul_rn(f.w, fg)),
                                     __fadd_rn(__fmul_rn(f.z, q0b), __fmul_rn(f.w, fb)), s_mid5, s_mid6);
             t.err = block_error<IT, K>(t.lo, t.hi, pp_sum);

@@ -126,6 +126,20 @@ __device__ __forceinline__ int precise_round565(float v0, float v1, float v2, co
     return eppack(r, g, b);
 }
 
+// PreciseRound565 of a cluster-fit trial's endpoint. The trial endpoints are table factors
+// times sums of at most 3 * 16 * 255: over the factor tables |v| * 63 < 9500, finite and far
+// inside int range, so truncation needs no x86 out-of-range case; the unsigned conversion
+// saturates negatives to 0, which is the lower clamp.
+__device__ __forceinline__ int precise_round565_cf(float v0, float v1, float v2, const float *mid5, const float *mid6) {
+    int r = (int)min(__float2uint_rz(__fmul_rn(v0, 31.0f)), 31u);
+    int g = (int)min(__float2uint_rz(__fmul_rn(v1, 63.0f)), 63u);
+    int b = (int)min(__float2uint_rz(__fmul_rn(v2, 31.0f)), 31u);
+    r += v0 > mid5[r];
+    g += v1 > mid6[g];
+    b += v2 > mid5[b];
+    return eppack(r, g, b);
+}
+
 // ---------------------------------------------------------------------------
 // interpolators (Interpolator.cpp:47-138)
 // ---------------------------------------------------------------------------
