@@ -517,9 +517,11 @@ __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool ex
     bool sc_done = false, from_ls = false;
     R sc;
     for (unsigned q = 0; q < total; q++) {
-        const int th = exhaustive ? (int)q : (int)row[q];
+        // BestOrders entries carry bit 15 for the single-colour orderings
+        const int raw = exhaustive ? (int)q : (int)row[q], th = raw & 0x7FFF;
+        const bool single = exhaustive ? is_single_hash(four, th) : raw >= 0x8000;
         R t;
-        if (is_single_hash(four, th)) {
+        if (single) {
             if (!sc_done) {  // the same trial for every single-colour ordering of this call
                 sc = single_color<IT>(orig.lo, orig.hi, m.av[0], m.av[1], m.av[2], !four);
                 sc.mode = kind_mode(K);
@@ -549,7 +551,7 @@ __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool ex
         }
         if (t.err < r.err) {
             r = t;
-            from_ls = !is_single_hash(four, th);
+            from_ls = !single;
         }
         if (t.err == 0) break;
     }

@@ -135,8 +135,16 @@ qtk::HostTables *make_tables() {
         std::abort();
     }
     const uint8_t *o4 = kOrderBlob + kBlobOrders4, *o3 = kOrderBlob + kBlobOrders3;
-    for (int i = 0; i < 969 * 128; i++) t->best4[i] = (uint16_t)(kOrderBlob[kBlobBest4 + 2 * i] | (kOrderBlob[kBlobBest4 + 2 * i + 1] << 8));
-    for (int i = 0; i < 153 * 32; i++) t->best3[i] = (uint16_t)(kOrderBlob[kBlobBest3 + 2 * i] | (kOrderBlob[kBlobBest3 + 2 * i + 1] << 8));
+    // bit 15 flags the single-colour orderings (OrderTable<4>::SingleColorHashes {15, 700, 753, 515},
+    // OrderTable<3>: {12, 15, 89}), so the encoder tests one bit per trial
+    for (int i = 0; i < 969 * 128; i++) {
+        const uint16_t h = (uint16_t)(kOrderBlob[kBlobBest4 + 2 * i] | (kOrderBlob[kBlobBest4 + 2 * i + 1] << 8));
+        t->best4[i] = (uint16_t)(h | ((h == 15 || h == 700 || h == 753 || h == 515) ? 0x8000 : 0));
+    }
+    for (int i = 0; i < 153 * 32; i++) {
+        const uint16_t h = (uint16_t)(kOrderBlob[kBlobBest3 + 2 * i] | (kOrderBlob[kBlobBest3 + 2 * i + 1] << 8));
+        t->best3[i] = (uint16_t)(h | ((h == 12 || h == 15 || h == 89) ? 0x8000 : 0));
+    }
     build_factors(4, 969, o4, t->factors4, t->hash4, t->orders4);
     build_factors(3, 153, o3, t->factors3, t->hash3, t->orders3);
     for (int it = 0; it < 4; it++) {

@@ -143,15 +143,19 @@ __device__ __forceinline__ int precise_round565_cf(float v0, float v1, float v2,
 // ---------------------------------------------------------------------------
 // interpolators (Interpolator.cpp:47-138)
 // ---------------------------------------------------------------------------
+// a, b are channel values (non-negative), so unsigned division gives the same quotients
 template <int IT> __device__ __forceinline__ int i8(int a, int b) {
-    if (IT == IT_ROUND) return (a * 2 + b + 1) / 3;
-    if (IT == IT_AMD) return (a * 43 + b * 21 + 32) >> 6;
-    return (a * 2 + b) / 3;
+    const unsigned ua = (unsigned)a, ub = (unsigned)b;
+    if (IT == IT_ROUND) return (int)((ua * 2 + ub + 1) / 3);
+    if (IT == IT_AMD) return (int)((ua * 43 + ub * 21 + 32) >> 6);
+    return (int)((ua * 2 + ub) / 3);
 }
-template <int IT> __device__ __forceinline__ int h8(int a, int b) { return IT == IT_AMD ? ((a + b + 1) >> 1) : ((a + b) / 2); }
-__device__ __forceinline__ int nv5(int a, int b) { return ((2 * a + b) * 22) / 8; }
+template <int IT> __device__ __forceinline__ int h8(int a, int b) {
+    return (int)(IT == IT_AMD ? (((unsigned)a + (unsigned)b + 1) >> 1) : (((unsigned)a + (unsigned)b) / 2));
+}
+__device__ __forceinline__ int nv5(int a, int b) { return (int)((((unsigned)a * 2 + (unsigned)b) * 22) / 8); }
 __device__ __forceinline__ int nv6(int a, int b) { int gd = b - a; return (256 * a + (gd / 4) + 128 + gd * 80) >> 8; }
-__device__ __forceinline__ int nvh5(int a, int b) { return ((a + b) * 33) / 8; }
+__device__ __forceinline__ int nvh5(int a, int b) { return (int)((((unsigned)a + (unsigned)b) * 33) / 8); }
 __device__ __forceinline__ int nvh6(int a, int b) { int gd = b - a; return (256 * a + gd / 4 + 128 + gd * 128) >> 8; }
 
 // Palette in FindSelectors' internal selector order (BC1Encoder.cpp:684-693):
@@ -714,7 +718,7 @@ template <int IT, int K> __device__ __noinline__ Res refine_cf(Res r, unsigned o
     uint16_t *row = s_row[G.g];
     if (!exhaustive) {  // stage the BestOrders row (8 or 2 entries per lane)
         const uint16_t *src = four ? g_tab.best4 + start * 128 : g_tab.best3 + start * 32;
-        for (unsigned q = G.lane; q < total; q += 16) row[q] = src[q];
+        for (unsigned q = G.lane; q < total; q += 16) row[q] = src[q] & 0x7FFF;  // without the single-colour flag
     }
     // projection onto high - low, sort, prefix sums (:891-909); all values exact integers
     const uint32_t v = s_px[G.g][G.lane];
