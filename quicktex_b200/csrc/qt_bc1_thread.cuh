@@ -17,7 +17,6 @@ constexpr int kThreads = 128;
 __shared__ uint32_t t_px[16][kThreads];     // texel i of the thread's block
 __shared__ uint32_t t_srg[17][kThreads];    // cluster-fit prefix sums: r | g << 16
 __shared__ uint16_t t_sb[17][kThreads];     //                          b
-__shared__ uint32_t t_key[16][kThreads];    // cluster-fit projection keys
 
 struct R {  // EncodeResults (BC1Encoder.h:147-153); endpoints packed 5:6:5
     int lo, hi;
@@ -437,6 +436,18 @@ template <int IT> __device__ __forceinline__ R refine_ls_any(int K, R r, const M
 }
 
 // RefineBlockCF<M> (BC1Encoder.cpp:877-928): the reference's loop as written
+// Ascending sort of 16 keys in registers: Batcher's odd-even merge network (63
+// compare-exchanges, each an unsigned min and max).
+__device__ __forceinline__ void sort16(uint32_t k[16]) {
+    constexpr int kNet[63][2] = {{0, 1}, {2, 3}, {0, 2}, {1, 3}, {1, 2}, {4, 5}, {6, 7}, {4, 6}, {5, 7}, {5, 6}, {0, 4}, {2, 6}, {2, 4}, {1, 5}, {3, 7}, {3, 5}, {1, 2}, {3, 4}, {5, 6}, {8, 9}, {10, 11}, {8, 10}, {9, 11}, {9, 10}, {12, 13}, {14, 15}, {12, 14}, {13, 15}, {13, 14}, {8, 12}, {10, 14}, {10, 12}, {9, 13}, {11, 15}, {11, 13}, {9, 10}, {11, 12}, {13, 14}, {0, 8}, {4, 12}, {4, 8}, {2, 10}, {6, 14}, {6, 10}, {2, 4}, {6, 8}, {10, 12}, {1, 9}, {5, 13}, {5, 9}, {3, 11}, {7, 15}, {7, 11}, {3, 5}, {7, 9}, {11, 13}, {1, 2}, {3, 4}, {5, 6}, {7, 8}, {9, 10}, {11, 12}, {13, 14}};
+#pragma unroll
+    for (int c = 0; c < 63; c++) {
+        const uint32_t a = k[kNet[c][0]], b = k[kNet[c][1]];
+        k[kNet[c][0]] = min(a, b);
+        k[kNet[c][1]] = max(a, b);
+    }
+}
+
 // OrderTable::GetHash of the selectors' histogram (OrderTable.h:91-104), the first
 // ordering of RefineBlockCF (BC1Encoder.cpp:886-889)
 __device__ __forceinline__ int cf_start_hash(bool four, uint32_t w) {
@@ -488,28 +499,25 @@ __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool ex
     const int axr = s5to8(epr(orig.hi)) - s5to8(epr(orig.lo));
     const int axg = s6to8(epg(orig.hi)) - s6to8(epg(orig.lo));
     const int axb = s5to8(epb(orig.hi)) - s5to8(epb(orig.lo));
-    for (int i = 0; i < 16; i++) t_key[i][tid] = cf_key(px(i), axr, axg, axb, i);
+    uint32_t key[16];
+#pragma unroll
+    for (int i = 0; i < 16; i++) key[i] = cf_key(px(i), axr, axg, axb, i);
+    sort16(key);  // the keys are distinct, so this is the reference's std::sort order
     uint64_t order = 0;
-    for (int i = 0; i < 16; i++) {  // t_srg/t_sb[k] first hold the colour of rank k-1
-        const uint32_t ki = t_key[i][tid];
-        int rank = 0;
-#pragma unroll 4
-        for (int j = 0; j < 16; j++) rank += t_key[j][tid] < ki;
-        const uint32_t v = px(i);
-        t_srg[rank + 1][tid] = (uint32_t)cr(v) | ((uint32_t)cg(v) << 16);
-        t_sb[rank + 1][tid] = (uint16_t)cb(v);
-        if (ORDER) order |= (uint64_t)i << (4 * rank);
-    }
-    if (ORDER) *order_out = order;
     uint32_t arg = 0, ab = 0;
     t_srg[0][tid] = 0;
     t_sb[0][tid] = 0;
-    for (int k = 1; k <= 16; k++) {
-        arg += t_srg[k][tid];
-        ab += t_sb[k][tid];
-        t_srg[k][tid] = arg;
-        t_sb[k][tid] = (uint16_t)ab;
+#pragma unroll
+    for (int k = 0; k < 16; k++) {  // prefix sums of the colours in rank order
+        const int i = (int)(key[k] & 15);
+        const uint32_t v = px(i);
+        arg += (uint32_t)cr(v) | ((uint32_t)cg(v) << 16);
+        ab += (uint32_t)cb(v);
+        t_srg[k + 1][tid] = arg;
+        t_sb[k + 1][tid] = (uint16_t)ab;
+        if (ORDER) order |= (uint64_t)i << (4 * k);
     }
+    if (ORDER) *order_out = order;
     const float t16r = (float)(arg & 0xFFFF), t16g = (float)(arg >> 16), t16b = (float)ab;
     const float denom = four ? 3.0f : 2.0f;
     const unsigned total = exhaustive ? (four ? 969u : 153u) : orderings;
