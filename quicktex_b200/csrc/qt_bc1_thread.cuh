@@ -14,6 +14,11 @@ namespace tpb {
 
 constexpr int kThreads = 128;
 
+// -2 that the compiler cannot fold: d * kNeg2 + v stays one IMAD on the FMA pipe. The trial
+// error loops use it for half of their |c|^2 - 2 p.c terms, so that the integer ALU pipe
+// (min, add) and the FMA pipe (dp4a, IMAD) share the work.
+__constant__ int kNeg2 = -2;
+
 __shared__ uint32_t t_px[16][kThreads];     // texel i of the thread's block
 __shared__ uint32_t t_srg[17][kThreads];    // cluster-fit prefix sums: r | g << 16
 __shared__ uint16_t t_sb[17][kThreads];     //                          b
@@ -169,17 +174,17 @@ template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo,
         const int v0 = (int)__dp4a(c0, c0, 0u), v1 = (int)__dp4a(c1, c1, 0u);
         const int v2 = (int)__dp4a(c2, c2, 0u), v3 = (int)__dp4a(c3, c3, 0u);
         int t0 = 0, t1 = 0;
-#pragma unroll 2
+#pragma unroll 4
         for (int i = 0; i < 16; i += 2) {
             const uint32_t u = px(i), q = px(i + 1);
             int m = v0 - 2 * (int)__dp4a(u, c0, 0u), n = v0 - 2 * (int)__dp4a(q, c0, 0u);
-            m = min(m, v1 - 2 * (int)__dp4a(u, c1, 0u));
-            n = min(n, v1 - 2 * (int)__dp4a(q, c1, 0u));
+            m = min(m, (int)__dp4a(u, c1, 0u) * kNeg2 + v1);
+            n = min(n, (int)__dp4a(q, c1, 0u) * kNeg2 + v1);
             m = min(m, v2 - 2 * (int)__dp4a(u, c2, 0u));
             n = min(n, v2 - 2 * (int)__dp4a(q, c2, 0u));
             if (K != K_T3) {
-                m = min(m, v3 - 2 * (int)__dp4a(u, c3, 0u));
-                n = min(n, v3 - 2 * (int)__dp4a(q, c3, 0u));
+                m = min(m, (int)__dp4a(u, c3, 0u) * kNeg2 + v3);
+                n = min(n, (int)__dp4a(q, c3, 0u) * kNeg2 + v3);
             }
             t0 += m;
             t1 += n;
@@ -435,7 +440,6 @@ template <int IT> __device__ __forceinline__ R refine_ls_any(int K, R r, const M
     }
 }
 
-// RefineBlockCF<M> (BC1Encoder.cpp:877-928): the reference's loop as written
 // Ascending sort of 16 keys in registers: Batcher's odd-even merge network (63
 // compare-exchanges, each an unsigned min and max).
 __device__ __forceinline__ void sort16(uint32_t k[16]) {
@@ -488,7 +492,8 @@ __device__ __forceinline__ bool cf_same_trials(bool four, const R &r, int start,
     return same;
 }
 
-// With ORDER, *order_out receives the texel order of the input (rank k -> texel in nibble k).
+// RefineBlockCF<M> (BC1Encoder.cpp:877-928): the reference's loop as written. With ORDER,
+// *order_out receives the texel order of the input (rank k -> texel in nibble k).
 template <int IT, int K, bool ORDER = false>
 __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool exhaustive, int pp_sum, uint64_t *order_out = nullptr) {
     constexpr bool four = !kind_three(K);
@@ -1054,7 +1059,8 @@ __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__
         if (!__any_sync(0xffffffffu, active)) break;
         if (!active) continue;
         bool done = false;
-        if ((int)(i & 31) != forbidden) {
+        if ((int)(i & 31) == forbidden) i++;  // skipped by the reference without a stop test
+        if (i < rounds) {
             const uint16_t vx = s_vox[i & 15];
             const int ddr = ((int)((unsigned)vx << 30)) >> 30, ddg = ((int)((unsigned)vx << 28)) >> 30;
             const int ddb = ((int)((unsigned)vx << 26)) >> 30;
@@ -1071,8 +1077,8 @@ __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__
                 moved = true;
             }
             if (i - prev > 32) done = true;
+            i++;
         }
-        i++;
         if (i >= rounds) done = true;
         if (done) {
             if (moved) r.sel = tpb::find_selectors<IT, K>(r.lo, r.hi).x;
