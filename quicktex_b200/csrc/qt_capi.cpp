@@ -315,10 +315,16 @@ int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h,
     const size_t texel_bytes = texel_row * (size_t)h, blocks_bytes = block_row * (size_t)bh;
     const size_t per_brow = 4 * texel_row + block_row;
     // ~8 MB of texels per band, and at least min_band_blocks blocks (a launch that large
-    // runs the BC1 EndpointSearch as its own refill pass)
+    // runs the BC1 EndpointSearch as its own refill pass). Settings that pass min_band_blocks
+    // are compute-heavy: their kernels outlast the copies, so after a first band that starts
+    // the pipeline each band is twice the last, which keeps the uploads ahead of the kernels
+    // with few bands (each band's multi-pass launch ends with a tail of idle lanes).
     const size_t by_bytes = std::max<size_t>(1, (size_t(8) << 20) / per_brow);
-    const int rows_per_band = (int)std::max<size_t>(by_bytes, (size_t)((min_band_blocks + bw - 1) / bw));
-    const int nbands = (bh + rows_per_band - 1) / rows_per_band;
+    const int rows_first = (int)std::max<size_t>(by_bytes, (size_t)((min_band_blocks + bw - 1) / bw));
+    std::vector<int> cut(1, 0);  // band k covers block rows [cut[k], cut[k + 1])
+    for (long rows = rows_first; cut.back() < bh; rows = min_band_blocks > 0 ? 2 * rows : rows)
+        cut.push_back((int)std::min<long>(bh, (long)cut.back() + rows));
+    const int nbands = (int)cut.size() - 1;
     const bool ragged = (h & 3) != 0;
     const size_t in_bytes = encode ? texel_bytes : blocks_bytes, out_bytes = encode ? blocks_bytes : texel_bytes;
     if (nbands < 2 || (!encode && ragged))
@@ -335,7 +341,7 @@ int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h,
     cudaError_t e = cudaSuccess;
     // uploads and kernels
     for (int k = 0; k < nbands && e == cudaSuccess && rc == QT_OK; k++) {
-        const int r0 = k * rows_per_band, r1 = std::min(bh, r0 + rows_per_band);
+        const int r0 = cut[k], r1 = cut[k + 1];
         cudaStream_t s = st[k & 1];
         size_t off, len;
         if (encode) {
@@ -355,7 +361,7 @@ int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h,
     }
     // downloads
     for (int k = 0; k < nbands && e == cudaSuccess && rc == QT_OK; k++) {
-        const int r0 = k * rows_per_band, r1 = std::min(bh, r0 + rows_per_band);
+        const int r0 = cut[k], r1 = cut[k + 1];
         size_t off, len;
         if (encode) {
             off = (size_t)r0 * block_row;
