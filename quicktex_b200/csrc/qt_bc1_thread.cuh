@@ -76,6 +76,16 @@ __device__ __noinline__ M metrics(bool ignore_black) {
     return m;
 }
 
+// Check2's projected selector (BC1Encoder.cpp:725-727) is trunc(fl(fl(dd * f) + 0.5)) clamped to
+// [1, 3], dd = (p - c0).axis an exact integer, f = fl(4 / den). Rounding is monotone, so the selector
+// is >= s exactly when dd reaches the smallest integer with fl(fl(dd * f) + 0.5) >= s. Over every
+// |axis|^2 in [0, 3 * 255^2] that integer is ceil(fl(fl(s - 0.5) * fl(den / 4))) or one more
+// (checked exhaustively), so one evaluation of the rounded expression finds it.
+__device__ __forceinline__ int check2_threshold(float f, float quarter_den, float s) {
+    const int est = __float2int_ru(__fmul_rn(__fadd_rn(s, -0.5f), quarter_den));
+    return est + (int)!(__fadd_rn(__fmul_rn(__int2float_rn(est), f), 0.5f) >= s);
+}
+
 // FindSelectors<M>(error_mode), BC1Encoder.cpp:679-779; K is one of the group kernel's kinds
 template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, int hi) {
     const Pal P = make_pal<IT>(lo, hi, kind_three(K));
@@ -202,18 +212,20 @@ template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo,
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
         int t = 0;
         if (K == K_F4_CHECK2) {
-            const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
+            const float den = __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f);
+            const float f = __fdiv_rn(4.0f, den), quarter = __fmul_rn(den, 0.25f);
             const int dbase = P.r0 * ar + P.g0 * ag + P.b0 * ab;
+            // selector >= 2 (>= 3) exactly when p.axis - c0.axis reaches the threshold
+            const int u2 = check2_threshold(f, quarter, 2.0f) + dbase, u3 = check2_threshold(f, quarter, 3.0f) + dbase;
 #pragma unroll 4
             for (int i = 0; i < 16; i++) {
                 const uint32_t u = px(i);  // the palette words' byte 3 is 0: alpha drops out of dp4a
                 const int d0 = (int)__dp4a(u, c0, 0u), d1 = (int)__dp4a(u, c1, 0u);
                 const int d2 = (int)__dp4a(u, c2, 0u), d3 = (int)__dp4a(u, c3, 0u);
-                // |dd * f + 0.5| stays far inside int range (f <= 4 whenever the axis is non-zero)
-                const int sl = clampi(__float2int_rz(__fadd_rn(__fmul_rn(__int2float_rn(d3 - d0 - dbase), f), 0.5f)), 1, 3);
-                const bool one = sl == 1, two = sl == 2;
-                const int ea = one ? v0 - 2 * d0 : two ? v1 - 2 * d1 : v2 - 2 * d2;
-                const int eb = one ? v1 - 2 * d1 : two ? v2 - 2 * d2 : v3 - 2 * d3;
+                const int pd = d3 - d0;
+                const bool two = pd >= u2, three = pd >= u3;
+                const int ea = three ? v2 - 2 * d2 : two ? v1 - 2 * d1 : v0 - 2 * d0;
+                const int eb = three ? v3 - 2 * d3 : two ? v2 - 2 * d2 : v1 - 2 * d1;
                 t += min(ea, eb);
             }
         } else {
