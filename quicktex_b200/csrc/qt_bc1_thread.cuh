@@ -118,20 +118,22 @@ template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, in
         }
     } else if (K == K_F4_CHECK2) {
         const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
-        const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
+        const float den = __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f);
+        const float f = __fdiv_rn(4.0f, den), quarter = __fmul_rn(den, 0.25f);
         const int dbase = P.r0 * ar + P.g0 * ag + P.b0 * ab;
+        // the projected selector is >= 2 (>= 3) exactly when p.axis - c0.axis reaches the threshold
+        const int u2 = check2_threshold(f, quarter, 2.0f) + dbase, u3 = check2_threshold(f, quarter, 3.0f) + dbase;
 #pragma unroll 4
         for (int i = 0; i < 16; i++) {
             const uint32_t v = px(i), u = v & 0x00FFFFFFu;
             const int p0 = (int)__dp4a(v, c0, 0u), p1 = (int)__dp4a(v, c1, 0u);
             const int p2 = (int)__dp4a(v, c2, 0u), p3 = (int)__dp4a(v, c3, 0u);
-            const int dd = p3 - p0 - dbase;  // (p - c0).axis, exact
-            // |dd * f + 0.5| stays far inside int range (f <= 4 whenever the axis is non-zero)
-            const int sl = clampi(__float2int_rz(__fadd_rn(__fmul_rn(__int2float_rn(dd), f), 0.5f)), 1, 3);
+            const int pd = p3 - p0;  // p.axis
+            const bool two = pd >= u2, three = pd >= u3;
+            const int sl = three ? 3 : two ? 2 : 1;
             // the two candidates sl-1 and sl
-            const bool one = sl == 1, two = sl == 2;
-            const int e0 = one ? v0 - 2 * p0 : two ? v1 - 2 * p1 : v2 - 2 * p2;
-            const int e1 = one ? v1 - 2 * p1 : two ? v2 - 2 * p2 : v3 - 2 * p3;
+            const int e0 = three ? v2 - 2 * p2 : two ? v1 - 2 * p1 : v0 - 2 * p0;
+            const int e1 = three ? v3 - 2 * p3 : two ? v2 - 2 * p2 : v1 - 2 * p1;
             int s = sl, e = e1;
             if (e0 == e1) {
                 if (s == 1) s = 0;
