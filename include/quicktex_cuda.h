@@ -116,8 +116,10 @@ int qt_bc3_encode_device(const uint8_t *rgba, int width, int height, const qt_bc
 /* No reference counterpart: the number of kernels one qt_bc1_encode_device or
  * qt_bc3_encode_device call on a width x height texture launches on the current
  * device with these params (1 = the encoder; 2 = a split pass that writes the solid
- * blocks, then the encoder; 3 = split, encoder, then EndpointSearch as its own pass).
- * The host entry points launch this per band. params->color_mode is not checked. */
+ * blocks, then the encoder; 4 = split, encoder, EndpointSearch as its own pass, then a
+ * pass that finishes the searches that moved the endpoints; 5 = the same with the
+ * second cluster-fit pass of level 18 as its own pass). The host entry points launch
+ * this per band. params->color_mode is not checked. */
 int qt_bc1_encode_kernels(int width, int height, const qt_bc1_params *params, int *kernels);
 
 /* BC4Encoder(channel)::Encode -> EncodeBlock (BC4Encoder.cpp:30-71). */

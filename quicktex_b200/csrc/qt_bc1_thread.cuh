@@ -871,6 +871,15 @@ struct SearchQueues {
     long cap;
 };
 
+// Searches that moved the endpoints, finished by k_bc1_finish: the block, its final endpoints
+// and colour mode. Their selectors come from FindSelectors on the final endpoints
+// (BC1Encoder.cpp:994-995); done inside the refill loop, that would run with one lane of the
+// warp active.
+struct FinishQueue {
+    uint32_t *count;
+    uint32_t *b, *lohi, *mode;  // [cap] each
+};
+
 // Blocks whose EncodeBlock continues in k_bc1_cf2 after the first four-colour cluster-fit
 // pass (one entry per block: its index, the result after the first pass, the endpoints
 // before refinement). Entries that run the second pass fill the arrays from the front,
@@ -1033,15 +1042,30 @@ __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_cf2(const uint8_t *__r
 template <int IT, int K>
 __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__ rgba, int w, int h, int bw,
                                              unsigned rounds, uint8_t *__restrict__ out, int bc3, int aligned,
-                                             const SearchQueues &q) {
+                                             const SearchQueues &q, const FinishQueue &f) {
     const int lane = threadIdx.x & 31;
     const uint32_t total = q.count[qq];
-    bool active = false, drained = false, moved = false;
+    bool active = false, drained = false, moved = false, pending = false;
     long b = 0;
     tpb::R r = tpb::rinit();
     int forbidden = -1, pp = 0;
     unsigned prev = 0, i = 0;
     for (;;) {
+        // a search that moved the endpoints, ended in the last step, goes to the finish queue
+        // (warp-aggregated, all lanes converged here) before the lane takes its next entry
+        const uint32_t fin = __ballot_sync(0xffffffffu, pending);
+        if (fin) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(f.count, (uint32_t)__popc(fin));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (pending) {
+                const uint32_t slot = base + __popc(fin & ((1u << lane) - 1));
+                f.b[slot] = (uint32_t)b;
+                f.lohi[slot] = pack_lohi(r);
+                f.mode[slot] = (uint32_t)r.mode;
+                pending = false;
+            }
+        }
         const uint32_t need = __ballot_sync(0xffffffffu, !active && !drained);
         if (need) {
             uint32_t base = 0;
@@ -1095,10 +1119,13 @@ __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__
         }
         if (i >= rounds) done = true;
         if (done) {
-            if (moved) r.sel = tpb::find_selectors<IT, K>(r.lo, r.hi).x;
-            const uint2 blk = tpb::write(r);
-            if (bc3) reinterpret_cast<uint2 *>(out)[2 * b + 1] = blk;  // the colour half of the 16-byte block
-            else reinterpret_cast<uint2 *>(out)[b] = blk;
+            if (moved) {
+                pending = true;  // selectors and block from k_bc1_finish
+            } else {  // the queued selectors belong to these endpoints
+                const uint2 blk = tpb::write(r);
+                if (bc3) reinterpret_cast<uint2 *>(out)[2 * b + 1] = blk;  // the colour half of the 16-byte block
+                else reinterpret_cast<uint2 *>(out)[b] = blk;
+            }
             active = false;
         }
     }
@@ -1107,15 +1134,41 @@ __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__
 template <int IT>
 __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_search(const uint8_t *__restrict__ rgba, int w, int h, int bw,
                                                                    qt_bc1_params p, uint8_t *__restrict__ out, int bc3,
-                                                                   int aligned, SearchQueues q) {
+                                                                   int aligned, SearchQueues q, FinishQueue f) {
     load_tables_smem();
     const unsigned rounds = p.search_rounds;
     switch (p.error_mode) {  // four-colour searches use the encoder's error mode (kind_for)
-        case EM_NONE: search_queue<IT, K_F4_NONE>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;
-        case EM_FASTER: search_queue<IT, K_F4_FASTER>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;
-        case EM_CHECK2: search_queue<IT, K_F4_CHECK2>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;
-        default: search_queue<IT, K_F4_FULL>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q); break;
+        case EM_NONE: search_queue<IT, K_F4_NONE>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q, f); break;
+        case EM_FASTER: search_queue<IT, K_F4_FASTER>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q, f); break;
+        case EM_CHECK2: search_queue<IT, K_F4_CHECK2>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q, f); break;
+        default: search_queue<IT, K_F4_FULL>(0, rgba, w, h, bw, rounds, out, bc3, aligned, q, f); break;
     }
-    search_queue<IT, K_T3>(1, rgba, w, h, bw, rounds, out, bc3, aligned, q);
-    search_queue<IT, K_TB>(2, rgba, w, h, bw, rounds, out, bc3, aligned, q);
+    search_queue<IT, K_T3>(1, rgba, w, h, bw, rounds, out, bc3, aligned, q, f);
+    search_queue<IT, K_TB>(2, rgba, w, h, bw, rounds, out, bc3, aligned, q, f);
+}
+
+// The searches that moved the endpoints: FindSelectors on the final endpoints (BC1Encoder.cpp:994-995)
+// and WriteBlock, one entry per thread. The search kernel appends its queues in order, so a warp's
+// entries share a colour mode except where one mode's entries end.
+template <int IT>
+__global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_finish(const uint8_t *__restrict__ rgba, int w, int h, int bw,
+                                                                   qt_bc1_params p, uint8_t *__restrict__ out, int bc3,
+                                                                   int aligned, FinishQueue f) {
+    load_tables_smem();
+    const long end = (long)*f.count, stride = (long)gridDim.x * blockDim.x;
+    for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < end; i += stride) {
+        const long b = (long)f.b[i];
+        uint32_t v[16];
+        stage_block(rgba, w, h, bw, b, aligned, v);
+        tpb::R r = tpb::rinit();
+        const uint32_t lh = f.lohi[i];
+        r.lo = (int)(lh & 0xFFFF);
+        r.hi = (int)(lh >> 16);
+        r.mode = (int)f.mode[i];
+        const int Md = r.mode == CM_THREE ? CM_THREE : (r.mode == CM_TB ? CM_TB : CM_FOUR);
+        r.sel = tpb::fs_any<IT>(kind_for(Md, Md == CM_FOUR ? p.error_mode : EM_FULL), r.lo, r.hi).x;
+        const uint2 blk = tpb::write(r);
+        if (bc3) reinterpret_cast<uint2 *>(out)[2 * b + 1] = blk;  // the colour half of the 16-byte block
+        else reinterpret_cast<uint2 *>(out)[b] = blk;
+    }
 }

@@ -1582,7 +1582,7 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
         // and the second four-colour cluster-fit pass, when there is one, runs in its own pass
         // for the blocks where it can change the result
         const bool cf2 = defer && cf2_pass(p);
-        const size_t words = 64 + (size_t)n + (defer ? 15 * (size_t)n : 0) + (cf2 ? 6 * (size_t)n : 0);
+        const size_t words = 64 + (size_t)n + (defer ? 18 * (size_t)n : 0) + (cf2 ? 6 * (size_t)n : 0);
         uint32_t *scratch = nullptr;
         cudaError_t e = scratch_alloc((void **)&scratch, words * sizeof(uint32_t), s);
         if (e != cudaSuccess) return (int)e;
@@ -1599,9 +1599,14 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
             q.err = qb + 6 * (size_t)n;
             q.sel = qb + 9 * (size_t)n;
             q.mode = qb + 12 * (size_t)n;
+            FinishQueue fq;  // searches that moved the endpoints
+            fq.count = scratch + 16;
+            fq.b = qb + 15 * (size_t)n;
+            fq.lohi = fq.b + (size_t)n;
+            fq.mode = fq.b + 2 * (size_t)n;
             Cf2Queue c{};
             if (cf2) {
-                uint32_t *cb = qb + 15 * (size_t)n;
+                uint32_t *cb = qb + 18 * (size_t)n;
                 c.count = scratch + 8;
                 c.b = cb;
                 c.lohi = cb + (size_t)n;
@@ -1618,7 +1623,8 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
     k_bc1_split<I><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count);                      \
     k_bc1_defer<I><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, list, count, q, c);                    \
     if (cf2) k_bc1_cf2<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, c, q);                    \
-    k_bc1_search<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, q);
+    k_bc1_search<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, q, fq);                       \
+    k_bc1_finish<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, fq);
                 case IT_IDEAL: QT_DEFER(IT_IDEAL) break;
                 case IT_ROUND: QT_DEFER(IT_ROUND) break;
                 case IT_NVIDIA: QT_DEFER(IT_NVIDIA) break;
@@ -1665,7 +1671,7 @@ int bc1_encode_kernels(long n, const qt_bc1_params &p) {
     if (n <= 0) return 0;
     if (bc1_mapping() != 0 || n < kSplitMinBlocks || n > 0xFFFFFFFFL) return 1;
     if (p.search_rounds == 0 || n < defer_min_blocks()) return 2;
-    return cf2_pass(p) ? 4 : 3;
+    return cf2_pass(p) ? 5 : 4;  // split, encoder, (second cluster-fit pass,) search, finish
 }
 
 int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3, void *stream) {

@@ -62,11 +62,12 @@ def test_bc3_deferred_search_matches_oracle(oracle_lib):
 
 @pytest.mark.parametrize("mode,interp", [(0x04, 0), (0x03, 2), (0x13, 3)])
 def test_bc1_level18_whole_texture_matches_oracle(oracle_lib, mode, interp):
-    """Every block of a 2048^2 texture at level 18, through all four passes (split, encoder,
-    the second cluster-fit pass for the blocks it can change, search), against the oracle."""
+    """Every block of a 2048^2 texture at level 18, through all five passes (split, encoder,
+    the second cluster-fit pass for the blocks it can change, search, and the selectors of the
+    searches that moved), against the oracle."""
     img = np.ascontiguousarray(syn.block_mix(SIDE, SIDE, workload=14, stream=18 + mode + interp))
     p = capi.params_for_level(18, mode, interp)
-    assert capi.bc1_encode_kernels(SIDE, SIDE, p) == 4
+    assert capi.bc1_encode_kernels(SIDE, SIDE, p) == 5
     out = _device_encode(capi.bc1_encode_device, img, p, 8)
     exp = oracle_lib.bc1_encode(img, SIDE, SIDE, BC1Params(level=18, color_mode=mode, interpolator=interp))
     if out != exp:
@@ -85,9 +86,10 @@ def test_bc3_level18_whole_texture_matches_oracle(oracle_lib):
 
 def test_encode_kernel_count():
     """qt_bc1_encode_kernels reports the passes one device call launches: the encoder alone on
-    small textures, the split pass first from 16384 blocks, the search pass on top of that for
-    levels with EndpointSearch once the texture holds two searches per resident lane, and the
-    second cluster-fit pass as its own kernel at levels with two of them (level 18)."""
+    small textures, the split pass first from 16384 blocks, the search pass and the pass that
+    finishes the searches that moved on top of that for levels with EndpointSearch once the
+    texture holds two searches per resident lane, and the second cluster-fit pass as its own
+    kernel at levels with two of them (level 18)."""
     import torch
 
     sms = torch.cuda.get_device_properties(0).multi_processor_count
@@ -97,10 +99,10 @@ def test_encode_kernel_count():
     assert capi.bc1_encode_kernels(508, 508, p18) == 1  # 127^2 = 16129 blocks
     assert capi.bc1_encode_kernels(512, 512, p18) == 2  # 16384 blocks
     assert capi.bc1_encode_kernels(side_defer, side_defer, p10) == 2
-    assert capi.bc1_encode_kernels(side_defer, side_defer, p18) == 4
-    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(13)) == 3
-    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(17)) == 3
-    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(18)) == 4
+    assert capi.bc1_encode_kernels(side_defer, side_defer, p18) == 5
+    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(13)) == 4
+    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(17)) == 4
+    assert capi.bc1_encode_kernels(SIDE, SIDE, capi.params_for_level(18)) == 5
     with pytest.raises(capi.QtError) as e:
         capi.bc1_encode_kernels(0, 64, p18)
     assert e.value.code == 1
