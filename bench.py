@@ -74,11 +74,11 @@ CONFIG = {
 }
 
 
-# DRAM bytes per block of a level-18 encode call (split, encoder, second cluster-fit pass, search),
-# the setting class that holds ~80% of the step: the ncu capture summarised in
-# profiles/k_bc1_L18_2048sq_pipeline.md (dram__bytes_read.sum + dram__bytes_write.sum of the four
-# kernels = 77,088,512 B for 262,144 blocks). Each pass re-reads the block's texels.
-BC1_DRAM_BYTES_PER_BLOCK = (16792832 + 18020864 + 1280 + 20707584 + 21565952) / 262144
+# DRAM bytes per block of a level-18 encode call (split, encoder, second cluster-fit pass, search,
+# finish), the setting class that holds ~80% of the step: the ncu capture summarised in
+# profiles/k_bc1_L18_2048sq_pipeline.md (dram__bytes_read.sum + dram__bytes_write.sum of the five
+# kernels = 92,672,768 B for 262,144 blocks). Each pass re-reads the block's texels.
+BC1_DRAM_BYTES_PER_BLOCK = (16793088 + 18020864 + 2048 + 20707584 + 21563904 + 15585280) / 262144
 
 
 def measure_hbm_paths(dev, stream, side: int = 16384, reps: int = 5):
@@ -353,10 +353,11 @@ def run_ours(args, world, rank, local):
         "roofline": {
             "bound": "fp32_issue", "achieved": achieved_exec, "peak": peak_tops, "unit": "Tlane-op/s",
             "frac": achieved_exec / peak_tops, "traffic": BC1_DRAM_BYTES_PER_BLOCK * NB,
-            "traffic_source": "ncu dram bytes of the four kernels of one 2048^2 level-18 call, per block, "
+            "traffic_source": "ncu dram bytes of the five kernels of one 2048^2 level-18 call, per block, "
                               "times this texture's blocks",
-            "kernel": "BC1 encode call: qtk::k_bc1_split, then qtk::k_bc1_thread, or qtk::k_bc1_defer + "
-                      "qtk::k_bc1_search for settings with EndpointSearch (all settings)",
+            "kernel": "BC1 encode call: qtk::k_bc1_split, then qtk::k_bc1_thread, or qtk::k_bc1_defer (+ "
+                      "qtk::k_bc1_cf2) + qtk::k_bc1_search + qtk::k_bc1_finish for settings with EndpointSearch "
+                      "(all settings)",
             "work": "10 lane-ops x oracle-counted candidate evaluations per block, less those in second "
                     "cluster-fit passes that repeat the first pass's trials (skipped here with identical output)",
             "achieved_reference_work": achieved, "frac_reference_work": achieved / peak_tops,
