@@ -864,6 +864,10 @@ __global__ void __launch_bounds__(256) k_bc1_split(const uint8_t *__restrict__ r
 // k_bc1_search runs one search round per step in every lane: a lane whose
 // search has stopped writes its block and takes the next queued one.
 // ---------------------------------------------------------------------------
+// idle lanes a search warp gathers before it refills them (measured: 4 → +3.1%, 8-16 → +3.5%,
+// 24 → +2.5% at level 18 over refilling every lane as soon as it is idle)
+constexpr int kRefillBatch = 8;
+
 struct SearchQueues {
     uint32_t *count;  // [3] entries per queue
     uint32_t *head;   // [3] next entry to take
@@ -1066,7 +1070,10 @@ __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__
                 pending = false;
             }
         }
-        const uint32_t need = __ballot_sync(0xffffffffu, !active && !drained);
+        uint32_t need = __ballot_sync(0xffffffffu, !active && !drained);
+        // A refill (queue entry, texels) runs with only the refilled lanes active, so it waits for
+        // kRefillBatch idle lanes, unless no lane is searching
+        if (__popc(need) < kRefillBatch && __any_sync(0xffffffffu, active)) need = 0;
         if (need) {
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(q.head + qq, (uint32_t)__popc(need));
