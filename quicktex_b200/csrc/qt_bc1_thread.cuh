@@ -1049,32 +1049,38 @@ __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__
                                              const SearchQueues &q, const FinishQueue &f) {
     const int lane = threadIdx.x & 31;
     const uint32_t total = q.count[qq];
-    bool active = false, drained = false, moved = false, pending = false;
+    bool active = false, drained = false, moved = false, pending = false, pending_write = false;
     long b = 0;
     tpb::R r = tpb::rinit();
     int forbidden = -1, pp = 0;
     unsigned prev = 0, i = 0;
     for (;;) {
-        // a search that moved the endpoints, ended in the last step, goes to the finish queue
-        // (warp-aggregated, all lanes converged here) before the lane takes its next entry
-        const uint32_t fin = __ballot_sync(0xffffffffu, pending);
-        if (fin) {
-            uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(f.count, (uint32_t)__popc(fin));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (pending) {
-                const uint32_t slot = base + __popc(fin & ((1u << lane) - 1));
-                f.b[slot] = (uint32_t)b;
-                f.lohi[slot] = pack_lohi(r);
-                f.mode[slot] = (uint32_t)r.mode;
-                pending = false;
-            }
-        }
         uint32_t need = __ballot_sync(0xffffffffu, !active && !drained);
         // A refill (queue entry, texels) runs with only the refilled lanes active, so it waits for
-        // kRefillBatch idle lanes, unless no lane is searching
+        // kRefillBatch idle lanes, unless no lane is searching. The lanes' finished searches are
+        // settled in the same batch: those that moved the endpoints go to the finish queue
+        // (warp-aggregated), the others are written.
         if (__popc(need) < kRefillBatch && __any_sync(0xffffffffu, active)) need = 0;
         if (need) {
+            const uint32_t fin = __ballot_sync(0xffffffffu, pending);
+            if (fin) {
+                uint32_t fbase = 0;
+                if (lane == 0) fbase = atomicAdd(f.count, (uint32_t)__popc(fin));
+                fbase = __shfl_sync(0xffffffffu, fbase, 0);
+                if (pending) {
+                    const uint32_t slot = fbase + __popc(fin & ((1u << lane) - 1));
+                    f.b[slot] = (uint32_t)b;
+                    f.lohi[slot] = pack_lohi(r);
+                    f.mode[slot] = (uint32_t)r.mode;
+                    pending = false;
+                }
+            }
+            if (pending_write) {  // the queued selectors belong to these endpoints
+                const uint2 blk = tpb::write(r);
+                if (bc3) reinterpret_cast<uint2 *>(out)[2 * b + 1] = blk;  // the colour half of the 16-byte block
+                else reinterpret_cast<uint2 *>(out)[b] = blk;
+                pending_write = false;
+            }
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(q.head + qq, (uint32_t)__popc(need));
             base = __shfl_sync(0xffffffffu, base, 0);
@@ -1125,14 +1131,9 @@ __device__ __forceinline__ void search_queue(int qq, const uint8_t *__restrict__
             i++;
         }
         if (i >= rounds) done = true;
-        if (done) {
-            if (moved) {
-                pending = true;  // selectors and block from k_bc1_finish
-            } else {  // the queued selectors belong to these endpoints
-                const uint2 blk = tpb::write(r);
-                if (bc3) reinterpret_cast<uint2 *>(out)[2 * b + 1] = blk;  // the colour half of the 16-byte block
-                else reinterpret_cast<uint2 *>(out)[b] = blk;
-            }
+        if (done) {  // settled at the lane's next refill
+            if (moved) pending = true;  // selectors and block from k_bc1_finish
+            else pending_write = true;
             active = false;
         }
     }
