@@ -77,8 +77,8 @@ CONFIG = {
 # DRAM bytes per block of a level-18 encode call (split, encoder, second cluster-fit pass, search,
 # finish), the setting class that holds ~80% of the step: the ncu capture summarised in
 # profiles/k_bc1_L18_2048sq_pipeline.md (dram__bytes_read.sum + dram__bytes_write.sum of the five
-# kernels = 92,672,768 B for 262,144 blocks). Each pass re-reads the block's texels.
-BC1_DRAM_BYTES_PER_BLOCK = (16793088 + 18020864 + 2048 + 20707584 + 21563904 + 15585280) / 262144
+# kernels = 92,676,096 B for 262,144 blocks). Each pass re-reads the block's texels.
+BC1_DRAM_BYTES_PER_BLOCK = (16792832 + 18021376 + 2560 + 20707584 + 21565952 + 15585792) / 262144
 
 
 def measure_hbm_paths(dev, stream, side: int = 16384, reps: int = 5):
