@@ -80,3 +80,31 @@ def test_banded_decode_equals_device(w, h):
             capi.check(L.qt_bc5_decode_host(bp, w, h, 2, 0, hp))
             capi.check(L.qt_bc5_decode_device(dbp, w, h, 2, 0, dp, sp))
         assert np.array_equal(out_h, d_out.cpu().numpy()), (fmt, w, h)
+
+
+@pytest.mark.parametrize("w,h", [(2048, 2049), (2900, 2701)])
+def test_banded_search_encode_equals_device(w, h):
+    """Settings with EndpointSearch cut the texture into bands of at least the deferred-search
+    threshold, each twice the last: 2048x2049 gives two bands, 2900x2701 three. Both have a ragged
+    bottom edge, whose last band wraps to rows of the first (on the other stream for two bands)."""
+    import torch
+
+    L = capi.lib()
+    img = np.ascontiguousarray(syn.alpha_mix(w, h, workload=14, stream=w * 7 + h)[:h, :w])
+    d_in = _dev(img)
+    nb = ((w + 3) // 4) * ((h + 3) // 4)
+    s = torch.cuda.current_stream()
+    p18 = capi.params_for_level(18, capi.THREE_COLOR, 2)
+    p13 = capi.params_for_level(13)
+    cases = [
+        ("bc1 L18", 8, lambda src, dst: L.qt_bc1_encode_host(src, w, h, ctypes.byref(p18), dst),
+         lambda src, dst: L.qt_bc1_encode_device(src, w, h, ctypes.byref(p18), dst, capi._vp(s.cuda_stream))),
+        ("bc3 L13", 16, lambda src, dst: L.qt_bc3_encode_host(src, w, h, ctypes.byref(p13), dst),
+         lambda src, dst: L.qt_bc3_encode_device(src, w, h, ctypes.byref(p13), dst, capi._vp(s.cuda_stream))),
+    ]
+    for name, bsz, host_fn, dev_fn in cases:
+        out_h = np.empty(nb * bsz, np.uint8)
+        capi.check(host_fn(capi._vp(img.ctypes.data), capi._vp(out_h.ctypes.data)))
+        d_out = torch.empty(nb * bsz, dtype=torch.uint8, device="cuda")
+        capi.check(dev_fn(capi._vp(d_in.data_ptr()), capi._vp(d_out.data_ptr())))
+        assert np.array_equal(out_h, d_out.cpu().numpy()), (name, w, h)
