@@ -76,7 +76,7 @@ __device__ __noinline__ M metrics(bool ignore_black) {
     return m;
 }
 
-// Check2's projected selector (BC1Encoder.cpp:725-727) is trunc(fl(fl(dd * f) + 0.5)) clamped to
+// Check2's projected selector (BC1Encoder.cpp:723-729) is trunc(fl(fl(dd * f) + 0.5)) clamped to
 // [1, 3], dd = (p - c0).axis an exact integer, f = fl(4 / den). Rounding is monotone, so the selector
 // is >= s exactly when dd reaches the smallest integer with fl(fl(dd * f) + 0.5) >= s. Over every
 // |axis|^2 in [0, 3 * 255^2] that integer is ceil(fl(fl(s - 0.5) * fl(den / 4))) or one more
@@ -876,9 +876,10 @@ struct SearchQueues {
 };
 
 // Searches that moved the endpoints, finished by k_bc1_finish: the block, its final endpoints
-// and colour mode. Their selectors come from FindSelectors on the final endpoints
-// (BC1Encoder.cpp:994-995); done inside the refill loop, that would run with one lane of the
-// warp active.
+// and colour mode. The reference keeps the selectors of the last accepted trial, which
+// FindSelectors computed from those endpoints (BC1Encoder.cpp:974-990); the search rounds here
+// compute errors only, so the selectors are computed once at the end. Done inside the refill loop,
+// that would run with one lane of the warp active.
 struct FinishQueue {
     uint32_t *count;
     uint32_t *b, *lohi, *mode;  // [cap] each
@@ -1155,8 +1156,9 @@ __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_search(const uint8_t *
     search_queue<IT, K_TB>(2, rgba, w, h, bw, rounds, out, bc3, aligned, q, f);
 }
 
-// The searches that moved the endpoints: FindSelectors on the final endpoints (BC1Encoder.cpp:994-995)
-// and WriteBlock, one entry per thread. The search kernel appends its queues in order, so a warp's
+// The searches that moved the endpoints: FindSelectors on the final endpoints (the selectors the
+// reference kept from the last accepted trial, BC1Encoder.cpp:974-990) and WriteBlock, one entry
+// per thread. The search kernel appends its queues in order, so a warp's
 // entries share a colour mode except where one mode's entries end.
 template <int IT>
 __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_finish(const uint8_t *__restrict__ rgba, int w, int h, int bw,

@@ -1,7 +1,7 @@
 """The Check2 selector thresholds of the BC1 trial error loop (quicktex_b200/csrc/qt_bc1_thread.cuh,
 check2_threshold), checked exhaustively on the CPU in IEEE float32.
 
-FindSelectors' Check2 mode (BC1Encoder.cpp:725-727) projects each texel onto the palette axis and
+FindSelectors' Check2 mode (BC1Encoder.cpp:723-729) projects each texel onto the palette axis and
 takes sl = clamp(trunc(fl(fl(dd * f) + 0.5)), 1, 3), with dd = (p - c0).axis an exact integer and
 f = fl(4 / fl(|axis|^2 + 0.00000125)). The encoder instead compares dd with two integer
 thresholds per trial: the smallest dd with fl(fl(dd * f) + 0.5) >= s, for s = 2 and 3. It finds
