@@ -106,3 +106,24 @@ def test_encode_kernel_count():
     with pytest.raises(capi.QtError) as e:
         capi.bc1_encode_kernels(0, 64, p18)
     assert e.value.code == 1
+
+
+@pytest.mark.parametrize("side,level,mode", [(256, 18, 0x04), (2048, 10, 0x04), (2048, 17, 0x03), (2048, 18, 0x13)])
+def test_encode_kernel_count_matches_launches(side, level, mode):
+    """The kernels one qt_bc1_encode_device call launches, as the CUDA profiler records them, are the
+    number qt_bc1_encode_kernels reports (the figure bench.py counts launches with)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+
+    img = np.ascontiguousarray(syn.block_mix(side, side, workload=14, stream=side + level))
+    p = capi.params_for_level(level, mode, 0)
+    d_in = torch.from_numpy(img.reshape(-1).copy()).cuda()
+    d_out = torch.empty((side // 4) ** 2 * 8, dtype=torch.uint8, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    capi.bc1_encode_device(d_in.data_ptr(), side, side, p, d_out.data_ptr(), stream)  # warm-up
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        capi.bc1_encode_device(d_in.data_ptr(), side, side, p, d_out.data_ptr(), stream)
+        torch.cuda.synchronize()
+    launched = [e.name for e in prof.events() if "k_bc1_" in e.name]
+    assert len(launched) == capi.bc1_encode_kernels(side, side, p), launched
