@@ -232,7 +232,7 @@ def cpu_reference_sample(img: np.ndarray, repeats: int = 1):
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
-    import quicktex_b200.synth as syn
+    import workloads as syn
 
     img = syn.block_mix(W, H)
     vals = []
@@ -256,7 +256,7 @@ def run_reference_arm(args, world, rank):
 def run_ours(args, world, rank, local):
     import torch
 
-    import quicktex_b200.synth as syn
+    import workloads as syn
     from quicktex_b200 import capi
 
     dev = torch.device("cuda", local)
@@ -399,7 +399,7 @@ def measure_batched(args, dev, world):
     with the upload and download of all textures inside the timed region."""
     import torch
 
-    import quicktex_b200.synth as syn
+    import workloads as syn
     from quicktex_b200.batch import Arena, Batch, Job, run_plain, run_plain_host
 
     from quicktex_b200.shard import block_cost, max_over_ranks, shard
@@ -519,7 +519,7 @@ def measure_dds(args, dev):
     import torch
 
     import quicktex_b200 as qt
-    import quicktex_b200.synth as syn
+    import workloads as syn
     from PIL import Image
 
     from quicktex_b200 import dds, image_utils
@@ -585,7 +585,7 @@ def measure_serving(args, dev):
     server (16 GiB device budget); latency = arrival -> result bytes on the host."""
     import torch
 
-    import quicktex_b200.synth as syn
+    import workloads as syn
     from quicktex_b200.batch import Job, run_jobs
     from quicktex_b200.serve import Server, latency_stats
 

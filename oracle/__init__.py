@@ -72,16 +72,15 @@ class BC1Params:
         return (ctypes.c_int * 10)(*[-1 if v is None else int(v) for v in vals])
 
 
-def build(force: bool = False, with_ref: Optional[bool] = None) -> None:
-    """Compile the checkers (``make -C oracle``). The reference build runs only
-    where the reference tree exists."""
-    ref_root = os.environ.get("QT_REFERENCE_ROOT", "/root/reference")
+def build(force: bool = False, ref_root: Optional[str] = None) -> None:
+    """Compile the checkers (``make -C oracle``). The reference checker is built
+    only when ``ref_root`` (else ``QT_REFERENCE_ROOT`` from the environment)
+    names a reference source tree."""
+    ref_root = ref_root or os.environ.get("QT_REFERENCE_ROOT")
     targets = ["oracle"]
-    if with_ref is None:
-        with_ref = os.path.isdir(os.path.join(ref_root, "quicktex"))
-    if with_ref:
+    if ref_root and os.path.isdir(os.path.join(ref_root, "quicktex")):
         targets.append("ref")
-    cmd = ["make", "-C", HERE, f"REF={ref_root}"] + (["-B"] if force else []) + targets
+    cmd = ["make", "-C", HERE] + ([f"REF={ref_root}"] if "ref" in targets else []) + (["-B"] if force else []) + targets
     subprocess.run(cmd, check=True, stdout=subprocess.DEVNULL)
 
 

@@ -21,7 +21,10 @@ and writes them in this package's own layout (little endian):
   4352    969*128*2       u16 best4[969][128]   ranked candidate orderings per start ordering
   252416  153*32*2        u16 best3[153][32]
 
-Usage:  python gen_order_tables.py [REFERENCE_ROOT]   (default /root/reference)
+Usage:  python oracle/gen_order_tables.py REFERENCE_ROOT
+
+(REFERENCE_ROOT is the root of the reference source tree; QT_REFERENCE_ROOT
+in the environment is used when the argument is omitted.)
 """
 
 from __future__ import annotations
@@ -33,7 +36,8 @@ import sys
 
 import numpy as np
 
-OUT = os.path.join(os.path.dirname(os.path.abspath(__file__)), "bc1_order_tables.bin")
+OUT = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "quicktex_b200", "data",
+                   "bc1_order_tables.bin")
 
 N4, N3, B4, B3 = 969, 153, 128, 32
 OFF_ORDERS4 = 8
@@ -103,7 +107,9 @@ def load(path: str = OUT) -> dict[str, np.ndarray]:
 
 
 if __name__ == "__main__":
-    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("QT_REFERENCE_ROOT")
+    if not root:
+        raise SystemExit("usage: python oracle/gen_order_tables.py REFERENCE_ROOT (or set QT_REFERENCE_ROOT)")
     data = pack(extract(root))
     with open(OUT, "wb") as f:
         f.write(data)

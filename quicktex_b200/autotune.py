@@ -16,12 +16,19 @@ from __future__ import annotations
 import argparse
 import json
 import os
+import sys
 import time
 
 import numpy as np
 
-from . import synth
 from .batch import Arena, Batch, Job, TUNING_PATH
+
+# The tuner runs in the source tree: its inputs are the seeded workload textures of
+# workloads.py at the repository root (the generator the benchmark uses too).
+_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if _ROOT not in sys.path:
+    sys.path.insert(0, _ROOT)
+import workloads as synth  # noqa: E402
 
 TILES = (32, 64, 128, 256, 512, 1024, 2048, 4096)
 LEVELS = (0, 5, 10, 18)

@@ -4,7 +4,8 @@ Markers
   gpu   needs a CUDA device (a B200); everything else runs on CPU.
 
 The checkers (oracle/) are built on demand: the C restatement always, the
-compiled reference only where its source tree exists.
+compiled reference only where QT_REFERENCE_ROOT names its source tree (a
+checker built beforehand, e.g. by the package build, is used as it is).
 """
 
 import os
@@ -26,7 +27,7 @@ def oracle_lib():
     import oracle
 
     if not os.path.exists(oracle.ORACLE_SO):
-        oracle.build(with_ref=False)
+        oracle.build()
     return oracle.Oracle()
 
 
@@ -36,7 +37,7 @@ def reference_lib():
 
     if not oracle.reference_available():
         try:
-            oracle.build(with_ref=True)
+            oracle.build(ref_root=os.environ.get("QT_REFERENCE_ROOT"))
         except Exception:
             pass
     if not oracle.reference_available():

@@ -16,7 +16,7 @@ def image(name: str):
     from PIL import Image
 
     sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__)))))
-    import quicktex_b200.synth as syn
+    import workloads as syn
 
     c = CASES[name]
     w, h = c["size"]

@@ -3,7 +3,8 @@
 ``make -C oracle pymod``), for the seeded cases of dds_cases.py, plus the sha256
 of every level the reference's ``dds.read(...).decode_all()`` returns.
 
-    make -C oracle pymod && python tests/golden/make_dds_golden.py
+    make -C oracle pymod REF=<reference root> &&
+        QT_REFERENCE_ROOT=<reference root> python tests/golden/make_dds_golden.py
 
 Only runs where the reference source tree exists. Writes nothing there: it is
 imported with bytecode caching off.
@@ -19,10 +20,12 @@ import sys
 sys.dont_write_bytecode = True
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF = os.environ.get("QT_REFERENCE", "/root/reference")
+REF = os.environ.get("QT_REFERENCE_ROOT", "")  # root of the reference source tree (required)
 
 
 def main():
+    if not REF:
+        raise SystemExit("set QT_REFERENCE_ROOT to the root of the reference source tree")
     sys.path[:0] = [os.path.join(ROOT, "oracle", "_ref"), REF, HERE]
     import quicktex
     import quicktex.dds as rdds

@@ -1,9 +1,9 @@
 """Generate the committed golden fixtures under tests/golden/.
 
 Run where the reference source tree exists (it builds and runs the unmodified
-reference, oracle/_ref/libqtref.so):
+reference, oracle/_ref/libqtref.so), with QT_REFERENCE_ROOT naming its root:
 
-    python tests/golden/make_golden.py [--skip-full | --ce-only]
+    QT_REFERENCE_ROOT=<reference root> python tests/golden/make_golden.py [--skip-full | --ce-only]
 
 Writes
   kat.json         the reference's own known-answer vectors: the 4x4 PNG
@@ -42,10 +42,11 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
 import oracle  # noqa: E402
-import quicktex_b200.synth as syn  # noqa: E402
+import workloads as syn  # noqa: E402
 from oracle import BC1Params  # noqa: E402
 
-REF_IMAGES = os.path.join(os.environ.get("QT_REFERENCE_ROOT", "/root/reference"), "tests", "images")
+REF_ROOT = os.environ.get("QT_REFERENCE_ROOT")  # root of the reference source tree (required)
+REF_IMAGES = os.path.join(REF_ROOT or "", "tests", "images")
 MODES = {"four": 0x04, "three": 0x03, "three_black": 0x13}
 INTERPS = {"ideal": 0, "round": 1, "nvidia": 2, "amd": 3}
 
@@ -98,7 +99,7 @@ def write_ce_counts(ce: dict, rep: dict) -> None:
 
 def ce_only() -> None:
     """ce_counts.json from the oracle alone (the counts need no reference run)."""
-    oracle.build(with_ref=False)
+    oracle.build()
     orc = oracle.Oracle()
     orc.set_threads(os.cpu_count())
     img = syn.block_mix(4096, 4096)
@@ -123,7 +124,9 @@ def main():
         ce_only()
         return
 
-    oracle.build(with_ref=True)
+    if not REF_ROOT:
+        raise SystemExit("set QT_REFERENCE_ROOT to the root of the reference source tree")
+    oracle.build(ref_root=REF_ROOT)
     ref, orc = oracle.Reference(), oracle.Oracle()
     ref.set_threads(os.cpu_count())
     orc.set_threads(os.cpu_count())

@@ -6,7 +6,7 @@ modes and interpolators, sizes 1..300 including non-multiples of 4."""
 import numpy as np
 import pytest
 
-import quicktex_b200.synth as syn
+import workloads as syn
 from oracle import BC1Params
 from quicktex_b200 import capi
 from quicktex_b200.batch import Batch, Job, run_jobs, run_plain, Arena

@@ -11,7 +11,7 @@ offset."""
 import numpy as np
 import pytest
 
-import quicktex_b200.synth as syn
+import workloads as syn
 from oracle import BC1Params
 from quicktex_b200 import capi
 

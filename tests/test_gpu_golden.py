@@ -17,7 +17,7 @@ import numpy as np
 import pytest
 
 import quicktex_b200 as qt
-import quicktex_b200.synth as syn
+import workloads as syn
 from quicktex_b200 import capi
 
 pytestmark = pytest.mark.gpu

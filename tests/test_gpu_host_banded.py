@@ -9,7 +9,7 @@ import ctypes
 import numpy as np
 import pytest
 
-import quicktex_b200.synth as syn
+import workloads as syn
 from quicktex_b200 import capi
 
 pytestmark = pytest.mark.gpu

@@ -9,7 +9,7 @@ padding on encode, wrapped overwrite on decode).
 import numpy as np
 import pytest
 
-import quicktex_b200.synth as syn
+import workloads as syn
 from oracle import BC1Params
 from quicktex_b200 import capi
 

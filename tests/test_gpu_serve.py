@@ -7,7 +7,7 @@ import time
 import numpy as np
 import pytest
 
-import quicktex_b200.synth as syn
+import workloads as syn
 from quicktex_b200.batch import Job, run_jobs
 from quicktex_b200.serve import Server, latency_stats
 

@@ -15,7 +15,7 @@ import os
 import numpy as np
 import pytest
 
-import quicktex_b200.synth as syn
+import workloads as syn
 from oracle import BC1Params
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")

@@ -7,7 +7,7 @@ import socket
 import pytest
 import torch.multiprocessing as mp
 
-import quicktex_b200.synth as syn
+import workloads as syn
 from quicktex_b200.shard import block_cost, max_over_ranks, shard
 
 

@@ -14,7 +14,7 @@ import ctypes
 import numpy as np
 import pytest
 
-import quicktex_b200.synth as syn
+import workloads as syn
 from quicktex_b200 import capi
 from quicktex_b200.batch import Arena, BatchItem, Job, run_jobs
 
