@@ -107,9 +107,18 @@ extern "C" int qt_batch_run_noalloc(const qt_batch_item *items, size_t n, void *
     }
     if (n == 0) return QT_OK;
 
-    // descriptors; tiles coarsened (x2 at a time) until they fit the fixed queue
+    // every item is validated before its sizes are used: widths and heights are positive and
+    // each texture's block count fits the 32-bit tile fields (as qt_batch_run requires)
+    for (size_t i = 0; i < n; i++) {
+        if (int rc = check_item(items[i])) return rc;
+        const uint64_t nb = (uint64_t)((items[i].width + 3) / 4) * (uint64_t)((items[i].height + 3) / 4);
+        if (nb > 0xFFFFFFFFull) return qtk::set_error(QT_ERR_ARG, "Texture too large");
+    }
+    // tiles coarsened (x2 at a time) until they fit the fixed queue; every item needs at least
+    // one tile and n <= QT_NOALLOC_MAX_ITEMS < QT_NOALLOC_MAX_TILES, so a scale of 2^32 (one tile
+    // per item) always fits and the loop ends by then
     uint64_t scale = 1;
-    for (;;) {
+    for (int round = 0; round <= 32; round++) {
         uint64_t tiles = 0;
         for (size_t i = 0; i < n; i++) {
             uint32_t tb;
@@ -125,7 +134,6 @@ extern "C" int qt_batch_run_noalloc(const qt_batch_item *items, size_t n, void *
     uint32_t nt = 0;
     for (size_t i = 0; i < n; i++) {
         const qt_batch_item &it = items[i];
-        if (int rc = check_item(it)) return rc;
         qtk::BatchItemDev &d = h_items[i];
         d.src = it.src;
         d.dst = it.dst;
@@ -146,6 +154,7 @@ extern "C" int qt_batch_run_noalloc(const qt_batch_item *items, size_t n, void *
         const uint64_t t = std::max<uint64_t>(1, tb * scale);
         const uint64_t nb = (uint64_t)d.bw * d.bh;
         for (uint64_t s0 = 0; s0 < nb; s0 += t) {
+            if (nt >= QT_NOALLOC_MAX_TILES) return qtk::set_error(QT_ERR_ARG, "qt_batch_run_noalloc: tile queue full");
             const uint32_t cnt = (uint32_t)std::min<uint64_t>(t, nb - s0);
             // pad carries the tile's cost for the ordering below; the kernel ignores it
             h_tiles[nt++] = {(uint32_t)i, (uint32_t)s0, cnt, (uint32_t)std::min(4.0e9f, c * (float)cnt)};
