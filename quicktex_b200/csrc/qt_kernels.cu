@@ -1,24 +1,12 @@
-// qt_kernels.cu — sm_100a kernels of the S3TC encode/decode path.
+// qt_kernels.cu — sm_100a kernels of the S3TC encode/decode path and their
+// launchers.
 //
-// Mapping. BC1 (and the colour half of BC3) runs one 4x4 block per group of
-// 16 lanes (two blocks per warp). Each phase of the reference encoder
-// (BC1Encoder::EncodeBlock, BC1Encoder.cpp:261-342) picks its own lane
-// mapping:
-//   * texel-parallel  (lane = texel): metrics, FindEndpoints, FindSelectors,
-//     RefineEndpointsLS(pixels). Every sum the reference accumulates over texels
-//     is integer-valued (in int or in float below 2^24), so warp reductions
-//     (redux.sync) give the reference's exact values in any order.
-//   * ordering-parallel (lane = cluster-fit ordering): RefineBlockCF. All
-//     orderings start from the same `orig` result, so the reference's
-//     sequential "keep if strictly better, stop at zero error" loop equals an
-//     argmin over (error, ordering index).
-//   * round-parallel (lane = search round): EndpointSearch. Rounds between two
-//     improvements all start from the same result, so 16 consecutive rounds are
-//     evaluated speculatively and the first improving one (or the stop rule)
-//     decides, exactly as the sequential loop would.
-// The reference's FindSelectors early exits never change an accepted result
-// (every exit bound is >= the later acceptance bound), so full errors are
-// computed instead.
+// Mapping. Every kernel runs one 4x4 block per thread. BC1 (and the colour
+// half of BC3) runs the reference encoder (BC1Encoder::EncodeBlock,
+// BC1Encoder.cpp:261-342) sequentially per thread, in its order; those
+// kernels are in qt_bc1_thread.cuh, included below. The reference's
+// FindSelectors early exits never change an accepted result (every exit bound
+// is >= the later acceptance bound), so full errors are computed instead.
 //
 // Floating point. Every operation whose rounding matters is written with an
 // explicit round-to-nearest intrinsic (__fadd_rn, __fmul_rn, __fdiv_rn), in
@@ -27,7 +15,8 @@
 // result is an integer below 2^24, i.e. exact.
 //
 // BC4/BC5 encode and all decoders are HBM-bound: one thread per block,
-// 16-byte row loads/stores where the texture is 4-aligned.
+// 16-byte row loads/stores where the texture is 4-aligned. The persistent
+// batch kernel (k_batch) runs any mix of them from a device work queue.
 
 #include <cuda_runtime.h>
 
@@ -83,8 +72,6 @@ constexpr int CM_INCOMPLETE = 0x00, CM_THREE = 0x03, CM_FOUR = 0x04, CM_TB = 0x1
 constexpr int EM_NONE = 0, EM_FASTER = 1, EM_CHECK2 = 2, EM_FULL = 3;
 constexpr int EP_LS = 0, EP_BB = 1, EP_BBINT = 2, EP_PCA = 3;
 constexpr int IT_IDEAL = 0, IT_ROUND = 1, IT_NVIDIA = 2, IT_AMD = 3;
-
-constexpr int kGroupsPerCta = 8;  // 16-lane groups per 128-thread CTA
 
 // BC4 selector for each threshold count (BC4Encoder.cpp:46 Levels {1,7,6,5,4,3,2,0}), 3 bits each
 constexpr uint32_t kBC4Levels = 1u | (7u << 3) | (6u << 6) | (5u << 9) | (4u << 12) | (3u << 15) | (2u << 18) | (0u << 21);
@@ -198,34 +185,10 @@ template <int IT> __device__ __forceinline__ Pal make_pal(int lo, int hi, bool t
 }
 
 // ---------------------------------------------------------------------------
-// per-CTA shared state of the BC1 kernel. File scope, so that the phase
-// functions below (kept __noinline__: one copy each, a small instruction
-// working set per launch) reach the block being encoded without passing it.
+// per-CTA shared copies of small constant tables (read by every BC1 kernel)
 // ---------------------------------------------------------------------------
 __shared__ float s_mid5[32], s_mid6[64];
 __shared__ uint16_t s_vox[16];
-__shared__ uint32_t s_px[kGroupsPerCta][16];      // the block's texels, RGBA8
-__shared__ float4 s_pf[kGroupsPerCta][16];        // (r, g, b, r^2+g^2+b^2) as exact floats
-__shared__ int s_sum[kGroupsPerCta][17 * 3];       // cluster-fit prefix sums
-__shared__ uint16_t s_row[kGroupsPerCta][128];     // BestOrders row of the current cluster fit
-__shared__ int s_met[kGroupsPerCta][2][16];        // metrics: [0] all texels, [1] ignoring black
-__shared__ int s_pp[kGroupsPerCta];                // sum over the block of r^2 + g^2 + b^2
-
-// metric slots
-constexpr int MT_MN = 0, MT_MX = 3, MT_AV = 6, MT_SUM = 9, MT_GREY = 12, MT_BLACK = 13;
-
-struct Grp {
-    unsigned gm;  // the group's 16 lanes within the warp
-    int lane;     // texel index in phases that map lanes to texels
-    int g;        // group index within the CTA
-};
-__device__ __forceinline__ Grp grp() {
-    Grp G;
-    G.lane = threadIdx.x & 15;
-    G.g = threadIdx.x >> 4;
-    G.gm = 0xFFFFu << (threadIdx.x & 16);
-    return G;
-}
 
 struct Res {  // EncodeResults (BC1Encoder.h:147-153); endpoints packed 5:6:5
     int lo, hi;
@@ -233,24 +196,6 @@ struct Res {  // EncodeResults (BC1Encoder.h:147-153); endpoints packed 5:6:5
     int mode;
     uint32_t err;
 };
-
-__device__ __forceinline__ Res res_init() {
-    Res r;
-    r.lo = r.hi = 0;
-    r.sel = 0;
-    r.mode = CM_INCOMPLETE;
-    r.err = UINT_MAX;
-    return r;
-}
-
-struct SelErr {
-    uint32_t sel, err;
-};
-
-__device__ __forceinline__ unsigned gsum(unsigned m, unsigned v) { return __reduce_add_sync(m, v); }
-__device__ __forceinline__ unsigned gmin(unsigned m, unsigned v) { return __reduce_min_sync(m, v); }
-__device__ __forceinline__ unsigned gmax(unsigned m, unsigned v) { return __reduce_max_sync(m, v); }
-__device__ __forceinline__ unsigned gor(unsigned m, unsigned v) { return __reduce_or_sync(m, v); }
 
 // Selector-search kinds: the (colour mode, error mode) pairs FindSelectors is
 // ever called with. Three-colour searches are always ErrorMode::Full
@@ -260,647 +205,16 @@ __host__ __device__ constexpr bool kind_three(int k) { return k >= K_T3; }
 __host__ __device__ constexpr int kind_mode(int k) { return k == K_T3 ? CM_THREE : (k == K_TB ? CM_TB : CM_FOUR); }
 __device__ __forceinline__ int kind_for(int M, int em) { return M == CM_THREE ? K_T3 : (M == CM_TB ? K_TB : em); }
 
-// ColorBlock::GetMetrics (ColorBlock.h:88-117), into s_met[g][which]
-__device__ __noinline__ void get_metrics(int which, bool ignore_black) {
-    const Grp G = grp();
-    const uint32_t v = s_px[G.g][G.lane];
-    const int p[3] = {(int)(v & 0xFF), (int)((v >> 8) & 0xFF), (int)((v >> 16) & 0xFF)};
-    const bool blk = (p[0] | p[1] | p[2]) < 4;
-    const bool has_black = __any_sync(G.gm, blk);
-    const bool inc = !(ignore_black && blk);
-    const bool grey = __all_sync(G.gm, !inc || (p[0] == p[1] && p[0] == p[2]));
-    const int total = __popc(__ballot_sync(G.gm, inc) & G.gm);
-    int *M = s_met[G.g][which];
-#pragma unroll
-    for (int c = 0; c < 3; c++) {
-        const int mn = (int)gmin(G.gm, inc ? p[c] : 255), mx = (int)gmax(G.gm, inc ? p[c] : 0);
-        const int sm = (int)gsum(G.gm, inc ? p[c] : 0);
-        if (G.lane == 0) {
-            M[MT_MN + c] = mn;
-            M[MT_MX + c] = mx;
-            M[MT_SUM + c] = sm;
-            M[MT_AV + c] = total > 0 ? (sm + total / 2) / total : 0;
-        }
-    }
-    if (G.lane == 0) {
-        M[MT_GREY] = grey;
-        M[MT_BLACK] = has_black;
-    }
-    __syncwarp(G.gm);
-}
-
-// ---------------------------------------------------------------------------
-// FindSelectors<M>(error_mode), texel-parallel (BC1Encoder.cpp:679-779)
-// ---------------------------------------------------------------------------
-template <int IT, int K> __device__ __noinline__ SelErr fs_tp(int lo, int hi) {
-    const Grp G = grp();
-    const uint32_t v = s_px[G.g][G.lane];
-    const int pr = v & 0xFF, pg = (v >> 8) & 0xFF, pb = (v >> 16) & 0xFF;
-    const Pal P = make_pal<IT>(lo, hi, kind_three(K));
-    int s;
-    unsigned e;
-    if (K == K_F4_NONE || K == K_F4_FASTER) {
-        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
-        const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
-        const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
-        const int t0 = d0 + d1, t1 = d1 + d2, t2 = d2 + d3;
-        const int dot = 2 * ar * pr + 2 * ag * pg + 2 * ab * pb;
-        s = 3 - ((dot <= t0) + (dot < t1) + (dot < t2));
-        e = K == K_F4_FASTER ? sq3(pr - sel4(P.r0, P.r1, P.r2, P.r3, s), pg - sel4(P.g0, P.g1, P.g2, P.g3, s),
-                                   pb - sel4(P.b0, P.b1, P.b2, P.b3, s))
-                             : 0u;
-    } else if (K == K_F4_CHECK2) {
-        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
-        const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
-        const int dd = (pr - P.r0) * ar + (pg - P.g0) * ag + (pb - P.b0) * ab;
-        const float sf = __fadd_rn(__fmul_rn(__int2float_rn(dd), f), 0.5f);
-        const int sl = clampi(f2i_x86(sf), 1, 3);
-        const unsigned e0 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - pr, sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - pg,
-                                sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - pb);
-        const unsigned e1 = sq3(sel4(P.r0, P.r1, P.r2, P.r3, sl) - pr, sel4(P.g0, P.g1, P.g2, P.g3, sl) - pg,
-                                sel4(P.b0, P.b1, P.b2, P.b3, sl) - pb);
-        s = sl;
-        e = e1;
-        if (e0 == e1) {
-            if (s == 1) s = 0;  // prefer the endpoint (:736-738)
-        } else if (e0 < e) {
-            s = sl - 1;
-            e = e0;
-        }
-    } else {
-        const unsigned e0 = sq3(P.r0 - pr, P.g0 - pg, P.b0 - pb), e1 = sq3(P.r1 - pr, P.g1 - pg, P.b1 - pb);
-        const unsigned e2 = sq3(P.r2 - pr, P.g2 - pg, P.b2 - pb);
-        s = 0;
-        e = e0;
-        if (e1 < e) { e = e1; s = 1; }
-        if (e2 < e) { e = e2; s = 2; }
-        if (K != K_T3) {
-            const unsigned e3 = sq3(P.r3 - pr, P.g3 - pg, P.b3 - pb);
-            if (e3 <= e) { e = e3; s = 3; }  // ties prefer selector 3 (:762)
-        }
-    }
-    SelErr o;
-    o.err = gsum(G.gm, e);
-    o.sel = gor(G.gm, (unsigned)s << (2 * G.lane));
-    return o;
-}
-
-template <int IT> __device__ __forceinline__ SelErr fs_any(int K, int lo, int hi) {
-    switch (K) {
-        case K_F4_NONE: return fs_tp<IT, K_F4_NONE>(lo, hi);
-        case K_F4_FASTER: return fs_tp<IT, K_F4_FASTER>(lo, hi);
-        case K_F4_CHECK2: return fs_tp<IT, K_F4_CHECK2>(lo, hi);
-        case K_F4_FULL: return fs_tp<IT, K_F4_FULL>(lo, hi);
-        case K_T3: return fs_tp<IT, K_T3>(lo, hi);
-        default: return fs_tp<IT, K_TB>(lo, hi);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// lane-serial block error: one lane evaluates all 16 texels for its own
-// endpoints (error only; the winner's selectors come from fs_tp)
-// ---------------------------------------------------------------------------
-template <int IT, int K> __device__ __forceinline__ float block_err(const float4 *pf, int lo, int hi) {
-    const Pal P = make_pal<IT>(lo, hi, kind_three(K));
-    float tot = 0.0f;
-    if (K == K_F4_FULL || K == K_T3 || K == K_TB) {
-        // sum_t min_j |p_t - c_j|^2 = sum_t |p_t|^2 + sum_t min_j (|c_j|^2 - 2 p_t.c_j), in exact integers:
-        // p.c by one dp4a on the packed texel (the colour's alpha byte is 0), the first sum is per block
-        const uint32_t *px = s_px[grp().g];
-        const uint32_t c0 = P.r0 | (P.g0 << 8) | (P.b0 << 16), c1 = P.r1 | (P.g1 << 8) | (P.b1 << 16);
-        const uint32_t c2 = P.r2 | (P.g2 << 8) | (P.b2 << 16), c3 = P.r3 | (P.g3 << 8) | (P.b3 << 16);
-        const int v0 = (int)sq3(P.r0, P.g0, P.b0), v1 = (int)sq3(P.r1, P.g1, P.b1);
-        const int v2 = (int)sq3(P.r2, P.g2, P.b2), v3 = (int)sq3(P.r3, P.g3, P.b3);
-        int t0 = 0, t1 = 0;
-#pragma unroll 2
-        for (int i = 0; i < 16; i += 2) {
-            const uint32_t u = px[i], q = px[i + 1];
-            int m = v0 - 2 * (int)__dp4a(u, c0, 0u), n = v0 - 2 * (int)__dp4a(q, c0, 0u);
-            m = min(m, v1 - 2 * (int)__dp4a(u, c1, 0u));
-            n = min(n, v1 - 2 * (int)__dp4a(q, c1, 0u));
-            m = min(m, v2 - 2 * (int)__dp4a(u, c2, 0u));
-            n = min(n, v2 - 2 * (int)__dp4a(q, c2, 0u));
-            if (K != K_T3) {
-                m = min(m, v3 - 2 * (int)__dp4a(u, c3, 0u));
-                n = min(n, v3 - 2 * (int)__dp4a(q, c3, 0u));
-            }
-            t0 += m;
-            t1 += n;
-        }
-        tot = (float)(s_pp[grp().g] + t0 + t1);
-    } else if (K == K_F4_FASTER) {
-        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
-        const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
-        const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
-        const float t0 = (float)(d0 + d1), t1 = (float)(d1 + d2), t2 = (float)(d2 + d3);
-        const float a2r = 2.0f * ar, a2g = 2.0f * ag, a2b = 2.0f * ab;
-#pragma unroll 4
-        for (int i = 0; i < 16; i++) {
-            const float4 p = pf[i];
-            const float dot = fmaf(p.z, a2b, fmaf(p.y, a2g, p.x * a2r));
-            const int s = 3 - ((int)(dot <= t0) + (int)(dot < t1) + (int)(dot < t2));  // selector = 3 - level
-            const float dr = p.x - (float)sel4(P.r0, P.r1, P.r2, P.r3, s);
-            const float dg = p.y - (float)sel4(P.g0, P.g1, P.g2, P.g3, s);
-            const float db = p.z - (float)sel4(P.b0, P.b1, P.b2, P.b3, s);
-            tot += fmaf(db, db, fmaf(dg, dg, dr * dr));
-        }
-    } else if (K == K_F4_CHECK2) {
-        const int ar = P.r3 - P.r0, ag = P.g3 - P.g0, ab = P.b3 - P.b0;
-        const float f = __fdiv_rn(4.0f, __fadd_rn(__uint2float_rn(sq3(ar, ag, ab)), .00000125f));
-        const float far_ = (float)ar, fag = (float)ag, fab = (float)ab;
-        const float c0r = (float)P.r0, c0g = (float)P.g0, c0b = (float)P.b0;
-#pragma unroll 4
-        for (int i = 0; i < 16; i++) {
-            const float4 p = pf[i];
-            const float dd = fmaf(p.z - c0b, fab, fmaf(p.y - c0g, fag, (p.x - c0r) * far_));
-            const float sf = __fadd_rn(__fmul_rn(dd, f), 0.5f);
-            const int sl = clampi(f2i_x86(sf), 1, 3);
-            const float ar0 = (float)sel4(P.r0, P.r1, P.r2, P.r3, sl - 1) - p.x;
-            const float ag0 = (float)sel4(P.g0, P.g1, P.g2, P.g3, sl - 1) - p.y;
-            const float ab0 = (float)sel4(P.b0, P.b1, P.b2, P.b3, sl - 1) - p.z;
-            const float ar1 = (float)sel4(P.r0, P.r1, P.r2, P.r3, sl) - p.x;
-            const float ag1 = (float)sel4(P.g0, P.g1, P.g2, P.g3, sl) - p.y;
-            const float ab1 = (float)sel4(P.b0, P.b1, P.b2, P.b3, sl) - p.z;
-            tot += fminf(fmaf(ab0, ab0, fmaf(ag0, ag0, ar0 * ar0)), fmaf(ab1, ab1, fmaf(ag1, ag1, ar1 * ar1)));
-        }
-    }
-    return tot;
-}
-
-// ---------------------------------------------------------------------------
-// FindEndpointsSingleColor(result, pixels, color, is_3color), texel-parallel
-// (BC1Encoder.cpp:443-471): the error is taken against colors[2] of the
-// endpoints held BEFORE the table lookup, over RGBA (palette alpha 255).
-// ---------------------------------------------------------------------------
-struct SC {
-    int lo, hi;
-    uint32_t err;
-};
-
-template <int IT> __device__ __noinline__ SC single_color_px(int stale_lo, int stale_hi, bool is3, int which) {
-    const Grp G = grp();
-    const uint32_t v = s_px[G.g][G.lane];
-    const Pal P = make_pal<IT>(stale_lo, stale_hi, is3);  // colors[2] is internal index 1 in both orders
-    const int dr = (int)(v & 0xFF) - P.r1, dg = (int)((v >> 8) & 0xFF) - P.g1, db = (int)((v >> 16) & 0xFF) - P.b1;
-    const int da = (int)(v >> 24) - 255;
-    SC o;
-    o.err = gsum(G.gm, (unsigned)(dr * dr + dg * dg + db * db + da * da));
-    const int *M = s_met[G.g][which];
-    const uint32_t mr = g_tab.match5[IT][M[MT_AV]], mg = g_tab.match6[IT][M[MT_AV + 1]], mb = g_tab.match5[IT][M[MT_AV + 2]];
-    o.lo = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
-    o.hi = eppack(mr & 0xFF, mg & 0xFF, mb & 0xFF);
-    return o;
-}
-
-// ---------------------------------------------------------------------------
-// FindEndpoints (BC1Encoder.cpp:473-677), texel-parallel
-// ---------------------------------------------------------------------------
+// Vector4::Dot (Vector4.h:53-57) in the reference's rounding: sum from 0, left to right
 __device__ __forceinline__ float fdot4_rn(float a0, float a1, float a2, float a3, float b0, float b1, float b2, float b3) {
-    // Vector4::Dot (Vector4.h:53-57): sum from 0, left to right
     float s = __fadd_rn(0.0f, __fmul_rn(a0, b0));
     s = __fadd_rn(s, __fmul_rn(a1, b1));
     s = __fadd_rn(s, __fmul_rn(a2, b2));
     return __fadd_rn(s, __fmul_rn(a3, b3));
 }
 
-__device__ __noinline__ int2 find_endpoints(int mode, bool ignore_black, int power_iters, int which) {
-    const Grp G = grp();
-    const uint32_t v = s_px[G.g][G.lane];
-    const int pr = v & 0xFF, pg = (v >> 8) & 0xFF, pb = (v >> 16) & 0xFF;
-    const int *M = s_met[G.g][which];
-    const int mn[3] = {M[MT_MN], M[MT_MN + 1], M[MT_MN + 2]}, mx[3] = {M[MT_MX], M[MT_MX + 1], M[MT_MX + 2]};
-    const int av[3] = {M[MT_AV], M[MT_AV + 1], M[MT_AV + 2]};
-    int lo, hi;
-    if (M[MT_GREY]) {  // :474-494
-        const int fr = (int)(s_px[G.g][0] & 0xFF);
-        if (mx[0] - mn[0] < 2) {
-            lo = hi = eppack(s8to5(fr), s8to6(fr), s8to5(fr));
-        } else {
-            lo = eppack(s8to5(mn[0]), s8to6(mn[0]), s8to5(mn[0]));
-            hi = eppack(s8to5(mx[0]), s8to6(mx[0]), s8to5(mx[0]));
-        }
-    } else if (mode == EP_LS) {  // :495-552
-        const int d0 = mx[0] - mn[0], d1 = mx[1] - mn[1], d2 = mx[2] - mn[2];
-        const int c0 = (d0 >= d1 && d0 >= d2) ? 0 : ((d1 >= d2 && d1 >= d0) ? 1 : 2);  // Color::MaxChannelRGB
-        const int p[3] = {pr, pg, pb};
-        const int px0 = c0 == 0 ? pr : (c0 == 1 ? pg : pb);
-        unsigned sxy[3];
-#pragma unroll
-        for (int c = 0; c < 3; c++) sxy[c] = gsum(G.gm, (unsigned)(px0 * p[c]));  // zero-initialised (:510 is not)
-        float l[3] = {0.f, 0.f, 0.f}, h[3] = {0.f, 0.f, 0.f};
-        const float mn0 = (float)(c0 == 0 ? mn[0] : (c0 == 1 ? mn[1] : mn[2]));
-        const unsigned sum_x = (unsigned)M[MT_SUM + c0], sum_xx = c0 == 0 ? sxy[0] : (c0 == 1 ? sxy[1] : sxy[2]);
-#pragma unroll
-        for (int c = 0; c < 3; c++)
-            if (c == c0) l[c] = h[c] = mn0;
-        const float den = __fsub_rn(__uint2float_rn(16u * sum_xx), __uint2float_rn(sum_x * sum_x));
-        if (fabsf(den) > 1e-8f) {
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                if (c == c0) continue;
-                const unsigned sum_y = (unsigned)M[MT_SUM + c], sum_xy = sxy[c];
-                const float a = __fdiv_rn(__uint2float_rn((16u * sum_xy) - (sum_x * sum_y)), den);
-                const float b = __fdiv_rn(__uint2float_rn((sum_xx * sum_y) - (sum_xy * sum_x)), den);
-                l[c] = __fadd_rn(b, __fmul_rn(a, mn0));
-                h[c] = __fadd_rn(b, __fmul_rn(a, mn0));
-            }
-        }
-#pragma unroll
-        for (int c = 0; c < 3; c++) {
-            const float inset = __fdiv_rn(__fsub_rn(h[c], l[c]), 16.0f);
-            l[c] = __fdiv_rn(__fadd_rn(l[c], inset), 255.0f);
-            h[c] = __fdiv_rn(__fsub_rn(h[c], inset), 255.0f);
-        }
-        lo = precise_round565(l[0], l[1], l[2], s_mid5, s_mid6);
-        hi = precise_round565(h[0], h[1], h[2], s_mid5, s_mid6);
-    } else if (mode == EP_BB || mode == EP_BBINT) {  // :553-605
-        const int b = pb - av[2];
-        const int cxz = (int)gsum(G.gm, (unsigned)(b * pr - av[0]));  // b * r - avg.r, as written (:572)
-        const int cyz = (int)gsum(G.gm, (unsigned)(b * pg - av[1]));
-        if (mode == EP_BB) {
-            const float bias = __fdiv_rn(8.0f, 255.0f);
-            float l[3], h[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                l[c] = __fdiv_rn((float)mn[c], 255.0f);
-                h[c] = __fdiv_rn((float)mx[c], 255.0f);
-                const float inset = __fdiv_rn(__fsub_rn(__fsub_rn(h[c], l[c]), bias), 16.0f);
-                l[c] = __fadd_rn(l[c], inset);
-                h[c] = __fsub_rn(h[c], inset);
-            }
-            if (cxz < 0) { const float t = l[0]; l[0] = h[0]; h[0] = t; }
-            if (cyz < 0) { const float t = l[1]; l[1] = h[1]; h[1] = t; }
-            lo = precise_round565(l[0], l[1], l[2], s_mid5, s_mid6);
-            hi = precise_round565(h[0], h[1], h[2], s_mid5, s_mid6);
-        } else {
-            int a[3], z[3];
-#pragma unroll
-            for (int c = 0; c < 3; c++) {
-                const int inset = ((mx[c] - mn[c]) - 8) >> 4;
-                a[c] = clamp255(mn[c] + inset);
-                z[c] = clamp255(mx[c] - inset);
-            }
-            if (cxz < 0) { const int t = a[0]; a[0] = z[0]; z[0] = t; }
-            if (cyz < 0) { const int t = a[1]; a[1] = z[1]; z[1] = t; }
-            lo = eppack(s8to5(a[0]), s8to6(a[1]), s8to5(a[2]));
-            hi = eppack(s8to5(z[0]), s8to6(z[1]), s8to5(z[2]));
-        }
-    } else {  // PCA, :606-674
-        const bool blk = (pr | pg | pb) < 4;
-        const bool inc = !(ignore_black && blk);
-        const int dr = pr - av[0], dg = pg - av[1], db = pb - av[2];
-        // covariance from identity, accumulated over included texels: exact integers
-        const int s00 = (int)gsum(G.gm, inc ? (unsigned)(dr * dr) : 0u);
-        const int s01 = (int)gsum(G.gm, inc ? (unsigned)(dr * dg) : 0u);
-        const int s02 = (int)gsum(G.gm, inc ? (unsigned)(dr * db) : 0u);
-        const int s11 = (int)gsum(G.gm, inc ? (unsigned)(dg * dg) : 0u);
-        const int s12 = (int)gsum(G.gm, inc ? (unsigned)(dg * db) : 0u);
-        const int s22 = (int)gsum(G.gm, inc ? (unsigned)(db * db) : 0u);
-        const float k255 = 255.0f;
-        const float c00 = __fdiv_rn((float)(1 + s00), k255), c01 = __fdiv_rn((float)s01, k255);
-        const float c02 = __fdiv_rn((float)s02, k255), c11 = __fdiv_rn((float)(1 + s11), k255);
-        const float c12 = __fdiv_rn((float)s12, k255), c22 = __fdiv_rn((float)(1 + s22), k255);
-        const float c33 = __fdiv_rn(1.0f, k255), z = __fdiv_rn(0.0f, k255);
-        float d0 = __fsub_rn((float)mx[0], (float)mn[0]);
-        float d1 = __fsub_rn((float)mx[1], (float)mn[1]);
-        float d2 = __fsub_rn((float)mx[2], (float)mn[2]);
-        float d3 = __fsub_rn(0.0f, 0.0f);
-        if (c02 < 0) d0 = -d0;
-        if (c12 < 0) d1 = -d1;
-        for (int it = 0; it < power_iters; it++) {  // Matrix4x4 * Vector4 (Matrix4x4.cpp:33-39), mirrored rows
-            const float n0 = fdot4_rn(d0, d1, d2, d3, c00, c01, c02, z);
-            const float n1 = fdot4_rn(d0, d1, d2, d3, c01, c11, c12, z);
-            const float n2 = fdot4_rn(d0, d1, d2, d3, c02, c12, c22, z);
-            const float n3 = fdot4_rn(d0, d1, d2, d3, z, z, z, c33);
-            d0 = n0; d1 = n1; d2 = n2; d3 = n3;
-        }
-        float k = 0.0f;  // Vector4::MaxAbs(3)
-        if (fabsf(d0) > k) k = fabsf(d0);
-        if (fabsf(d1) > k) k = fabsf(d1);
-        if (fabsf(d2) > k) k = fabsf(d2);
-        float a0 = 306.0f, a1 = 601.0f, a2 = 117.0f, a3 = 0.0f;
-        if (k >= 2) {
-            const float s = __fdiv_rn(2048.0f, k);
-            a0 = __fmul_rn(d0, s); a1 = __fmul_rn(d1, s); a2 = __fmul_rn(d2, s); a3 = __fmul_rn(d3, s);
-        }
-        a0 = __fmul_rn(a0, 16.0f); a1 = __fmul_rn(a1, 16.0f); a2 = __fmul_rn(a2, 16.0f); a3 = __fmul_rn(a3, 16.0f);
-        const float dot = fdot4_rn((float)pr, (float)pg, (float)pb, 0.0f, a0, a1, a2, a3);
-        // first index of the maximum / minimum (strict > / < scan, :654-670)
-        float vmax = inc ? dot : -INFINITY, vmin = inc ? dot : INFINITY;
-        int imax = G.lane, imin = G.lane;
-#pragma unroll
-        for (int off = 8; off >= 1; off >>= 1) {
-            const float ov = __shfl_xor_sync(G.gm, vmax, off, 16);
-            const int oi = __shfl_xor_sync(G.gm, imax, off, 16);
-            if (ov > vmax || (ov == vmax && oi < imax)) { vmax = ov; imax = oi; }
-            const float ow = __shfl_xor_sync(G.gm, vmin, off, 16);
-            const int oj = __shfl_xor_sync(G.gm, imin, off, 16);
-            if (ow < vmin || (ow == vmin && oj < imin)) { vmin = ow; imin = oj; }
-        }
-        const uint32_t pmin = s_px[G.g][imin], pmax = s_px[G.g][imax];
-        lo = eppack(s8to5(pmin & 0xFF), s8to6((pmin >> 8) & 0xFF), s8to5((pmin >> 16) & 0xFF));
-        hi = eppack(s8to5(pmax & 0xFF), s8to6((pmax >> 8) & 0xFF), s8to5((pmax >> 16) & 0xFF));
-    }
-    return make_int2(lo, hi);
-}
-
-// ---------------------------------------------------------------------------
-// RefineBlockLS<M> (BC1Encoder.cpp:852-875) with
-// RefineEndpointsLS<FourColor>(result, pixels, metrics) (:781-825). Only the
-// FourColor instantiation of the latter is ever called (:860): no texel is
-// skipped and the 4-colour weights apply to every colour mode.
-// ---------------------------------------------------------------------------
-template <int IT, int K> __device__ __noinline__ Res refine_ls(Res r, int passes, int which) {
-    const Grp G = grp();
-    const uint32_t v = s_px[G.g][G.lane];
-    const int pr = v & 0xFF, pg = (v >> 8) & 0xFF, pb = (v >> 16) & 0xFF;
-    const int *M = s_met[G.g][which];
-    for (int pass = 0; pass < passes; pass++) {
-        Res t = r;
-        const int s = (t.sel >> (2 * G.lane)) & 3;
-        const int n1 = __popc(__ballot_sync(G.gm, s == 1) & G.gm), n2 = __popc(__ballot_sync(G.gm, s == 2) & G.gm);
-        const int n3 = __popc(__ballot_sync(G.gm, s == 3) & G.gm), n0 = 16 - n1 - n2 - n3;
-        // sum of OrderTable<4>::Weights[sel] = {s^2, s(3-s), s(3-s), (3-s)^2}: exact small integers
-        float m0 = (float)(n1 + 4 * n2 + 9 * n3), m1 = (float)(2 * n1 + 2 * n2), m2 = m1, m3 = (float)(9 * n0 + 4 * n1 + n2);
-        const float q00r = (float)(int)gsum(G.gm, (unsigned)(pr * s));
-        const float q00g = (float)(int)gsum(G.gm, (unsigned)(pg * s));
-        const float q00b = (float)(int)gsum(G.gm, (unsigned)(pb * s));
-        const float det = __fsub_rn(__fmul_rn(m0, m3), __fmul_rn(m1, m2));
-        if (fabsf(det) < 1e-8f) {  // not multicolour: FindEndpointsSingleColor on the average
-            const SC sc = single_color_px<IT>(t.lo, t.hi, K != K_F4_NONE && kind_three(K), which);
-            t.lo = sc.lo;
-            t.hi = sc.hi;
-            t.err = sc.err;
-            t.sel = 0x55555555u;
-            t.mode = kind_three(K) ? CM_THREE : CM_FOUR;
-        } else {
-            const float tt = m0; m0 = m3; m3 = tt;
-            m1 = -m1;
-            m2 = -m2;
-            const float sc = __fdiv_rn(__fdiv_rn(3.0f, 255.0f), det);
-            m0 = __fmul_rn(m0, sc); m1 = __fmul_rn(m1, sc); m2 = __fmul_rn(m2, sc); m3 = __fmul_rn(m3, sc);
-            const float q10r = (float)(M[MT_SUM] * 3) - q00r, q10g = (float)(M[MT_SUM + 1] * 3) - q00g;
-            const float q10b = (float)(M[MT_SUM + 2] * 3) - q00b;
-            t.lo = precise_round565(__fadd_rn(__fmul_rn(m0, q00r), __fmul_rn(m1, q10r)),
-                                    __fadd_rn(__fmul_rn(m0, q00g), __fmul_rn(m1, q10g)),
-                                    __fadd_rn(__fmul_rn(m0, q00b), __fmul_rn(m1, q10b)), s_mid5, s_mid6);
-            t.hi = precise_round565(__fadd_rn(__fmul_rn(m2, q00r), __fmul_rn(m3, q10r)),
-                                    __fadd_rn(__fmul_rn(m2, q00g), __fmul_rn(m3, q10g)),
-                                    __fadd_rn(__fmul_rn(m2, q00b), __fmul_rn(m3, q10b)), s_mid5, s_mid6);
-            const SelErr se = fs_tp<IT, K>(t.lo, t.hi);
-            t.sel = se.sel;
-            t.err = se.err;
-            t.mode = kind_mode(K);
-        }
-        if (t.lo == r.lo && t.hi == r.hi) break;
-        if (K == K_F4_NONE || t.err < r.err) r = t;
-        else break;
-    }
-    return r;
-}
-
-template <int IT> __device__ __forceinline__ Res refine_ls_any(int K, Res r, int passes, int which) {
-    switch (K) {
-        case K_F4_NONE: return refine_ls<IT, K_F4_NONE>(r, passes, which);
-        case K_F4_FASTER: return refine_ls<IT, K_F4_FASTER>(r, passes, which);
-        case K_F4_CHECK2: return refine_ls<IT, K_F4_CHECK2>(r, passes, which);
-        case K_F4_FULL: return refine_ls<IT, K_F4_FULL>(r, passes, which);
-        case K_T3: return refine_ls<IT, K_T3>(r, passes, which);
-        default: return refine_ls<IT, K_TB>(r, passes, which);
-    }
-}
-
 __device__ __forceinline__ bool is_single_hash(bool four, int h) {
     return four ? (h == 15 || h == 700 || h == 753 || h == 515) : (h == 12 || h == 15 || h == 89);
-}
-
-// RefineEndpointsLS<M>(result, sums, matrix, hash) (BC1Encoder.cpp:827-850):
-// q10 = sums at the ordering's cumulative selector counts (exact integers)
-__device__ __forceinline__ int2 ls_from_sums(const int *S, float4 f, uint32_t o, bool four) {
-    const int l1 = o & 0xFF, l2 = l1 + ((o >> 8) & 0xFF), l3 = l2 + ((o >> 16) & 0xFF);
-    int qr = S[3 * l1] + S[3 * l2], qg = S[3 * l1 + 1] + S[3 * l2 + 1], qb = S[3 * l1 + 2] + S[3 * l2 + 2];
-    if (four) {
-        qr += S[3 * l3];
-        qg += S[3 * l3 + 1];
-        qb += S[3 * l3 + 2];
-    }
-    const float denom = four ? 3.0f : 2.0f;
-    const float fr = (float)qr, fg = (float)qg, fb = (float)qb;
-    const float q0r = (float)S[48] * denom - fr, q0g = (float)S[49] * denom - fg, q0b = (float)S[50] * denom - fb;
-    const int lo = precise_round565(__fadd_rn(__fmul_rn(f.x, q0r), __fmul_rn(f.y, fr)),
-                                    __fadd_rn(__fmul_rn(f.x, q0g), __fmul_rn(f.y, fg)),
-                                    __fadd_rn(__fmul_rn(f.x, q0b), __fmul_rn(f.y, fb)), s_mid5, s_mid6);
-    const int hi = precise_round565(__fadd_rn(__fmul_rn(f.z, q0r), __fmul_rn(f.w, fr)),
-                                    __fadd_rn(__fmul_rn(f.z, q0g), __fmul_rn(f.w, fg)),
-                                    __fadd_rn(__fmul_rn(f.z, q0b), __fmul_rn(f.w, fb)), s_mid5, s_mid6);
-    return make_int2(lo, hi);
-}
-
-// ---------------------------------------------------------------------------
-// RefineBlockCF<M> (BC1Encoder.cpp:877-928)
-// ---------------------------------------------------------------------------
-template <int IT, int K> __device__ __noinline__ Res refine_cf(Res r, unsigned orderings, bool exhaustive, int which) {
-    constexpr bool four = !kind_three(K);
-    constexpr int M = kind_mode(K);
-    const Grp G = grp();
-    const Res orig = r;
-    // Histogram of the selectors -> start ordering (OrderTable::GetHash, OrderTable.h:91-104)
-    const uint32_t w = orig.sel;
-    const int n1 = __popc(w & ~(w >> 1) & 0x55555555u), n2 = __popc(~w & (w >> 1) & 0x55555555u);
-    const int n3 = __popc(w & (w >> 1) & 0x55555555u), n0 = 16 - n1 - n2 - n3;
-    int start;
-    if (four) {  // SingleColorHashes (OrderTable.cpp:43-44), looked up by bin
-        start = n0 == 16 ? 15 : n1 == 16 ? 700 : n2 == 16 ? 753 : n3 == 16 ? 515 : (int)g_tab.hash4[n0 | (n1 << 4) | (n2 << 8)];
-    } else {
-        start = n0 == 16 ? 12 : n1 == 16 ? 15 : n2 == 16 ? 89 : (int)g_tab.hash3[n0 | (n1 << 4)];
-    }
-    const unsigned total = exhaustive ? (four ? 969u : 153u) : orderings;
-    uint16_t *row = s_row[G.g];
-    if (!exhaustive) {  // stage the BestOrders row (8 or 2 entries per lane)
-        const uint16_t *src = four ? g_tab.best4 + start * 128 : g_tab.best3 + start * 32;
-        for (unsigned q = G.lane; q < total; q += 16) row[q] = src[q] & 0x7FFF;  // without the single-colour flag
-    }
-    // projection onto high - low, sort, prefix sums (:891-909); all values exact integers
-    const uint32_t v = s_px[G.g][G.lane];
-    const int pr = v & 0xFF, pg = (v >> 8) & 0xFF, pb = (v >> 16) & 0xFF;
-    const int axr = s5to8(epr(orig.hi)) - s5to8(epr(orig.lo));
-    const int axg = s6to8(epg(orig.hi)) - s6to8(epg(orig.lo));
-    const int axb = s5to8(epb(orig.hi)) - s5to8(epb(orig.lo));
-    const uint32_t key = ((uint32_t)(0x1000000 + pr * axr + pg * axg + pb * axb) << 4) | (uint32_t)G.lane;
-    int rank = 0;  // keys are distinct (the texel index is in the low bits)
-#pragma unroll
-    for (int i = 0; i < 16; i++) rank += __shfl_sync(G.gm, key, i, 16) < key;
-    int sr = 0, sg = 0, sb = 0;  // sum of the texels ranked at or below this lane's position
-#pragma unroll 4
-    for (int j = 0; j < 16; j++) {
-        if (__shfl_sync(G.gm, rank, j, 16) <= G.lane) {
-            const uint32_t u = s_px[G.g][j];
-            sr += u & 0xFF;
-            sg += (u >> 8) & 0xFF;
-            sb += (u >> 16) & 0xFF;
-        }
-    }
-    int *S = s_sum[G.g];
-    S[3 * (G.lane + 1) + 0] = sr;
-    S[3 * (G.lane + 1) + 1] = sg;
-    S[3 * (G.lane + 1) + 2] = sb;
-    if (G.lane == 0) S[0] = S[1] = S[2] = 0;
-    __syncwarp(G.gm);
-
-    // the single-colour trial is the same for every single-colour ordering of this call
-    const SC sc = single_color_px<IT>(orig.lo, orig.hi, !four, which);
-
-    if (total <= 4) {
-        // few orderings: evaluate them in sequence, texel-parallel (the reference's loop as written)
-        for (unsigned q = 0; q < total; q++) {
-            const int th = exhaustive ? (int)q : (int)row[q];
-            Res t;
-            if (is_single_hash(four, th)) {
-                t.lo = sc.lo;
-                t.hi = sc.hi;
-                t.err = sc.err;
-                t.sel = 0x55555555u;
-            } else {
-                const int2 e = ls_from_sums(S, four ? g_tab.factors4[th] : g_tab.factors3[th],
-                                            four ? g_tab.orders4[th] : g_tab.orders3[th], four);
-                t.lo = e.x;
-                t.hi = e.y;
-                const SelErr se = fs_tp<IT, K>(t.lo, t.hi);
-                t.sel = se.sel;
-                t.err = se.err;
-            }
-            t.mode = M;
-            if (t.err < r.err) r = t;
-            if (t.err == 0) break;
-        }
-    } else {
-        // ordering-parallel: lane l evaluates orderings l, l+16, ...; argmin over (error, index)
-        const float4 *pf = s_pf[G.g];
-        float best = INFINITY;
-        int bq = 0x7FFF, blo = 0, bhi = 0;
-        unsigned q = G.lane;
-        int th = 0;
-        float4 f = make_float4(0.f, 0.f, 0.f, 0.f);
-        uint32_t o = 0;
-        if (q < total) {
-            th = exhaustive ? (int)q : (int)row[q];
-            f = four ? g_tab.factors4[th] : g_tab.factors3[th];
-            o = four ? g_tab.orders4[th] : g_tab.orders3[th];
-        }
-        for (; q < total; q += 16) {
-            // prefetch the next ordering's table entries while this one is evaluated
-            const unsigned qn = q + 16;
-            int thn = 0;
-            float4 fn = f;
-            uint32_t on = o;
-            if (qn < total) {
-                thn = exhaustive ? (int)qn : (int)row[qn];
-                fn = four ? g_tab.factors4[thn] : g_tab.factors3[thn];
-                on = four ? g_tab.orders4[thn] : g_tab.orders3[thn];
-            }
-            int lo, hi;
-            float e;
-            if (is_single_hash(four, th)) {
-                lo = sc.lo;
-                hi = sc.hi;
-                e = (float)sc.err;
-            } else {
-                const int2 ep = ls_from_sums(S, f, o, four);
-                lo = ep.x;
-                hi = ep.y;
-                e = block_err<IT, K>(pf, lo, hi);
-            }
-            if (e < best) {
-                best = e;
-                bq = (int)q;
-                blo = lo;
-                bhi = hi;
-            }
-            th = thn;
-            f = fn;
-            o = on;
-        }
-        const uint32_t be = best == INFINITY ? UINT_MAX : (uint32_t)best;
-        const uint32_t min_e = gmin(G.gm, be);
-        const uint32_t min_q = gmin(G.gm, be == min_e ? (uint32_t)bq : 0xFFFFu);
-        if (min_e < orig.err) {
-            const int wl = (int)(min_q & 15);
-            r.lo = __shfl_sync(G.gm, blo, wl, 16);
-            r.hi = __shfl_sync(G.gm, bhi, wl, 16);
-            r.err = min_e;
-            r.mode = M;
-            const int wth = exhaustive ? (int)min_q : (int)row[min_q];
-            r.sel = is_single_hash(four, wth) ? 0x55555555u : fs_tp<IT, K>(r.lo, r.hi).sel;
-        }
-    }
-    __syncwarp(G.gm);  // s_sum and s_row are rewritten by the next call
-    return r;
-}
-
-template <int IT> __device__ __forceinline__ Res refine_cf_any(int K, Res r, unsigned orderings, bool exhaustive, int which) {
-    switch (K) {
-        case K_F4_NONE: return refine_cf<IT, K_F4_NONE>(r, orderings, exhaustive, which);
-        case K_F4_FASTER: return refine_cf<IT, K_F4_FASTER>(r, orderings, exhaustive, which);
-        case K_F4_CHECK2: return refine_cf<IT, K_F4_CHECK2>(r, orderings, exhaustive, which);
-        case K_F4_FULL: return refine_cf<IT, K_F4_FULL>(r, orderings, exhaustive, which);
-        default: return refine_cf<IT, K_T3>(r, orderings, exhaustive, which);
-    }
-}
-
-// ---------------------------------------------------------------------------
-// EndpointSearch (BC1Encoder.cpp:930-996), round-parallel speculation
-// ---------------------------------------------------------------------------
-template <int IT, int K> __device__ __noinline__ Res endpoint_search(Res r, unsigned rounds) {
-    const Grp G = grp();
-    const float4 *pf = s_pf[G.g];
-    const unsigned sh = (G.gm & 0xFFFFu) ? 0 : 16;
-    unsigned prev = 0, i0 = 0;
-    int forbidden = -1;
-    bool moved = false;
-    while (i0 < rounds) {
-        const unsigned i = i0 + (unsigned)G.lane;
-        const bool active = i < rounds && (int)(i & 31) != forbidden;
-        const uint16_t vx = s_vox[i & 15];
-        const int ddr = ((int)((unsigned)vx << 30)) >> 30, ddg = ((int)((unsigned)vx << 28)) >> 30;
-        const int ddb = ((int)((unsigned)vx << 26)) >> 30;
-        int lo = r.lo, hi = r.hi;
-        if (i & 16) lo = eppack(clampi(epr(lo) + ddr, 0, 31), clampi(epg(lo) + ddg, 0, 63), clampi(epb(lo) + ddb, 0, 31));
-        else hi = eppack(clampi(epr(hi) + ddr, 0, 31), clampi(epg(hi) + ddg, 0, 63), clampi(epb(hi) + ddb, 0, 31));
-        float e = INFINITY;
-        if (active) e = block_err<IT, K>(pf, lo, hi);
-        const bool improve = active && e < (float)r.err;
-        const bool stop = active && (i - prev > 32);
-        const unsigned bi = (__ballot_sync(G.gm, improve) >> sh) & 0xFFFFu;
-        const unsigned bs = (__ballot_sync(G.gm, stop) >> sh) & 0xFFFFu;
-        const int fi = bi ? __ffs(bi) - 1 : 16, fs = bs ? __ffs(bs) - 1 : 16;
-        if (bi && fi <= fs) {  // the first improving round is accepted
-            const unsigned j = i0 + (unsigned)fi;
-            r.lo = __shfl_sync(G.gm, lo, fi, 16);
-            r.hi = __shfl_sync(G.gm, hi, fi, 16);
-            r.err = (uint32_t)__shfl_sync(G.gm, e, fi, 16);
-            forbidden = (int)((s_vox[j & 15] >> 8) & 15) | (int)(j & 16);
-            prev = j;
-            i0 = j + 1;
-            moved = true;
-        } else if (bs) {  // that round did not improve and i - prev > 32: stop
-            break;
-        } else {
-            i0 += 16;
-        }
-    }
-    if (moved) r.sel = fs_tp<IT, K>(r.lo, r.hi).sel;  // selectors of the accepted endpoints
-    return r;
-}
-
-template <int IT> __device__ __forceinline__ Res endpoint_search_any(int K, Res r, unsigned rounds) {
-    switch (K) {
-        case K_F4_NONE: return endpoint_search<IT, K_F4_NONE>(r, rounds);
-        case K_F4_FASTER: return endpoint_search<IT, K_F4_FASTER>(r, rounds);
-        case K_F4_CHECK2: return endpoint_search<IT, K_F4_CHECK2>(r, rounds);
-        case K_F4_FULL: return endpoint_search<IT, K_F4_FULL>(r, rounds);
-        case K_T3: return endpoint_search<IT, K_T3>(r, rounds);
-        default: return endpoint_search<IT, K_TB>(r, rounds);
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -952,136 +266,6 @@ __device__ __forceinline__ uint2 write_block(const Res &r) {
 #pragma unroll
     for (int i = 0; i < 16; i++) sel |= ((lut >> (2 * ((r.sel >> (2 * i)) & 3))) & 3) << (2 * i);
     return make_uint2((uint32_t)ep0 | ((uint32_t)ep1 << 16), sel);
-}
-
-// ---------------------------------------------------------------------------
-// BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342) for the group's block
-// ---------------------------------------------------------------------------
-template <int IT> __device__ __forceinline__ uint2 encode_bc1_group(const Grp &G, const qt_bc1_params &p, int color_mode) {
-    if (__all_sync(G.gm, s_px[G.g][G.lane] == s_px[G.g][0])) return write_block_solid<IT>(s_px[G.g][0]);
-
-    get_metrics(0, false);
-    const bool has_black = s_met[G.g][0][MT_BLACK] != 0;
-    const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
-    bool needs_err = use_likely;
-    needs_err |= color_mode == CM_THREE;
-    needs_err |= (color_mode == CM_TB) && has_black;
-    needs_err |= p.error_mode != EM_NONE;
-    needs_err |= p.search_rounds > 0;
-    const int em = needs_err ? p.error_mode : EM_NONE;
-    const int ls_passes = p.two_ls_passes ? 2 : 1, cf_passes = p.two_cf_passes ? 2 : 1;
-    const int ep_passes = (needs_err && p.two_ep_passes) ? 2 : 1;
-    const int k4 = kind_for(CM_FOUR, em);
-
-    Res orig = res_init(), res = res_init();
-    for (int round = 0; round < ep_passes; round++) {
-        const int2 ep = find_endpoints(round == 1 ? EP_BB : p.endpoint_mode, false, (int)p.power_iterations, 0);
-        Res to = res_init();
-        to.lo = ep.x;
-        to.hi = ep.y;
-        Res tr = to;
-        const SelErr se = fs_any<IT>(k4, tr.lo, tr.hi);
-        tr.sel = se.sel;
-        tr.err = se.err;
-        tr.mode = CM_FOUR;
-        tr = refine_ls_any<IT>(k4, tr, ls_passes, 0);
-        if (!needs_err || tr.err < res.err) {
-            res = tr;
-            orig = to;
-        }
-    }
-    if (res.err > 0 && use_likely)
-        for (int it = 0; it < cf_passes; it++) res = refine_cf_any<IT>(kind_for(CM_FOUR, p.error_mode), res, p.orderings4, p.exhaustive, 0);
-
-    if (res.err > 0 && (color_mode & CM_THREE)) {
-        Res t = orig;
-        const SelErr se = fs_tp<IT, K_T3>(t.lo, t.hi);
-        t.sel = se.sel;
-        t.err = se.err;
-        t.mode = CM_THREE;
-        t = refine_ls<IT, K_T3>(t, ls_passes, 0);
-        if (t.err > 0 && use_likely)
-            for (int it = 0; it < cf_passes; it++) t = refine_cf<IT, K_T3>(t, p.orderings3, p.exhaustive, 0);
-        if (t.err < res.err) res = t;
-    }
-
-    if (res.err > 0 && color_mode == CM_TB && has_black) {
-        const int *M0 = s_met[G.g][0];
-        if (!((M0[MT_MX] | M0[MT_MX + 1] | M0[MT_MX + 2]) < 4)) {
-            get_metrics(1, true);
-            const int2 ep = find_endpoints(EP_PCA, true, (int)p.power_iterations, 1);
-            Res t = res_init();
-            t.lo = ep.x;
-            t.hi = ep.y;
-            const SelErr se = fs_tp<IT, K_TB>(t.lo, t.hi);
-            t.sel = se.sel;
-            t.err = se.err;
-            t.mode = CM_TB;
-            t = refine_ls<IT, K_TB>(t, ls_passes, 1);
-            if (t.err < res.err) res = t;
-        }
-    }
-
-    if (res.err > 0 && p.search_rounds > 0) {
-        const int M = res.mode == CM_THREE ? CM_THREE : (res.mode == CM_TB ? CM_TB : CM_FOUR);
-        res = endpoint_search_any<IT>(kind_for(M, M == CM_FOUR ? p.error_mode : EM_FULL), res, p.search_rounds);
-    }
-    return write_block(res);
-}
-
-// BC4Encoder::EncodeBlock (BC4Encoder.cpp:30-71) for the group's block; returns the 8 bytes
-__device__ __forceinline__ uint2 encode_bc4_group(const Grp &G, int ch) {
-    const int v = (int)((s_px[G.g][G.lane] >> (8 * ch)) & 0xFF);
-    const int mn = (int)gmin(G.gm, (unsigned)v), mx = (int)gmax(G.gm, (unsigned)v);
-    if (mn == mx) return make_uint2((uint32_t)mn | ((uint32_t)mn << 8), 0u);
-    const int bias = 4 - mn * 14, delta = mx - mn, x = v * 14;
-    int lvl = 0;
-#pragma unroll
-    for (int c = 0; c < 7; c++) lvl += x >= delta * (1 + 2 * c) - bias;
-    const uint32_t s = (kBC4Levels >> (3 * lvl)) & 7u;
-    const int bit = 3 * G.lane;
-    const uint32_t lo = gor(G.gm, bit < 32 ? s << bit : 0u);
-    const uint32_t hi = gor(G.gm, bit >= 32 ? s << (bit - 32) : (bit + 3 > 32 ? s >> (32 - bit) : 0u));
-    // bytes: a0=max, a1=min, then 48 selector bits little endian
-    return make_uint2((uint32_t)mx | ((uint32_t)mn << 8) | (lo << 16), (lo >> 16) | (hi << 16));
-}
-
-// ---------------------------------------------------------------------------
-// BC1 / BC3 encode kernel: one block per 16-lane group, grid-stride
-// ---------------------------------------------------------------------------
-template <int IT>
-__global__ void __launch_bounds__(128, 6) k_bc1_encode(const uint8_t *__restrict__ rgba, int w, int h, int bw, long b_begin,
-                                                       long nblocks, qt_bc1_params p, uint8_t *__restrict__ out, int bc3) {
-    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
-        if (i < 32) s_mid5[i] = c_mid5[i];
-        s_mid6[i] = c_mid6[i];
-        if (i < 16) s_vox[i] = c_voxels[i];
-    }
-    __syncthreads();
-    const Grp G = grp();
-    const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
-
-    for (long b = b_begin + (long)blockIdx.x * kGroupsPerCta + G.g; b < nblocks; b += (long)gridDim.x * kGroupsPerCta) {
-        const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
-        int sx = bx * 4 + (G.lane & 3), sy = by * 4 + (G.lane >> 2);
-        if (sx >= w) sx %= w;  // RawTexture::GetBlock wraps at the edges (Texture.h:105-108)
-        if (sy >= h) sy %= h;
-        const uint32_t v = *reinterpret_cast<const uint32_t *>(rgba + ((size_t)sy * w + sx) * 4);
-        const float fr = (float)(v & 0xFF), fg = (float)((v >> 8) & 0xFF), fb = (float)((v >> 16) & 0xFF);
-        s_px[G.g][G.lane] = v;
-        s_pf[G.g][G.lane] = make_float4(fr, fg, fb, fr * fr + fg * fg + fb * fb);
-        const unsigned pp = gsum(G.gm, sq3((int)(v & 0xFF), (int)((v >> 8) & 0xFF), (int)((v >> 16) & 0xFF)));
-        if (G.lane == 0) s_pp[G.g] = (int)pp;
-        __syncwarp(G.gm);
-        const uint2 blk = encode_bc1_group<IT>(G, p, color_mode);
-        if (bc3) {
-            const uint2 a = encode_bc4_group(G, 3);
-            if (G.lane == 0) reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
-        } else if (G.lane == 0) {
-            reinterpret_cast<uint2 *>(out)[b] = blk;
-        }
-        __syncwarp(G.gm);
-    }
 }
 
 // ---------------------------------------------------------------------------
@@ -1533,17 +717,6 @@ int upload_tables(int device) {
     return (int)e;
 }
 
-// BC1 mapping: 0 = one block per thread, 1 = one block per 16-lane group.
-// QT_BC1_MAPPING=thread|group overrides the default for comparison runs.
-static int bc1_mapping() {
-    static int m = -1;
-    if (m < 0) {
-        const char *e = getenv("QT_BC1_MAPPING");
-        m = (e && e[0] == 'g') ? 1 : 0;
-    }
-    return m;
-}
-
 // below this many blocks the split pass costs more than idle solid lanes do
 constexpr long kSplitMinBlocks = 16384;
 
@@ -1561,7 +734,7 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
     const long n = b_end - b_begin;
     if (n <= 0) return 0;
     cudaStream_t s = (cudaStream_t)stream;
-    if (bc1_mapping() == 0) {
+    {
         const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
         const int g = grid_for(n, tpb::kThreads);
         if (n < kSplitMinBlocks || n > 0xFFFFFFFFL) {
@@ -1657,19 +830,11 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
         scratch_free(scratch, s);
         return (int)e;
     }
-    const int grid = grid_for(n, kGroupsPerCta);
-    switch (p.interpolator) {
-        case IT_IDEAL: k_bc1_encode<IT_IDEAL><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
-        case IT_ROUND: k_bc1_encode<IT_ROUND><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
-        case IT_NVIDIA: k_bc1_encode<IT_NVIDIA><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
-        default: k_bc1_encode<IT_AMD><<<grid, 128, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3); break;
-    }
-    return (int)cudaGetLastError();
 }
 
 int bc1_encode_kernels(long n, const qt_bc1_params &p) {
     if (n <= 0) return 0;
-    if (bc1_mapping() != 0 || n < kSplitMinBlocks || n > 0xFFFFFFFFL) return 1;
+    if (n < kSplitMinBlocks || n > 0xFFFFFFFFL) return 1;
     if (p.search_rounds == 0 || n < defer_min_blocks()) return 2;
     return cf2_pass(p) ? 5 : 4;  // split, encoder, (second cluster-fit pass,) search, finish
 }
