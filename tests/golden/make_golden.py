@@ -13,7 +13,13 @@ Writes
                    full size (512^2 BC1 L5 encode+decode; 4096^2 BC1 at levels
                    {0,10,18} x 3 colour modes x 4 interpolators; 8192^2 BC3 L5,
                    BC5, BC4 channels {0,1,3} and their decodes), plus a 512^2
-                   sweep of every level 0-19. Each entry also records the
+                   sweep of every level 0-19, and the adversarial hazard
+                   corpus (workloads.hazard_mix: greyscale, all-black solid,
+                   near-black, 3-colour+black, RGB-uniform with varying alpha,
+                   extreme two-colour and solid blocks) for BC1 at every level
+                   x colour mode x interpolator and BC3 at every level x
+                   interpolator (--hazard-only adds just these to the existing
+                   file). Each entry also records the
                    sha256 of its input so a mismatch in the generator is caught
                    before the codec is blamed. Every hash is cross-checked
                    against the oracle restatement (qt_oracle.c) before writing.
@@ -115,10 +121,35 @@ def ce_only() -> None:
     write_ce_counts(ce, rep)
 
 
+def hazard_entry(ref, orc) -> dict:
+    """Reference hashes of the adversarial hazard corpus: BC1 at every level x colour mode x
+    interpolator, BC3 at every level x interpolator. The LeastSquares endpoint mode (level 1) is
+    left out for every interpolator: the reference reads an uninitialised array there
+    (BC1Encoder.cpp:510), and on this corpus its output differs from a zero-initialised copy of
+    itself on a few blocks for each interpolator, so no implementation can be pinned to it."""
+    img = syn.hazard_mix()
+    h, w = img.shape[:2]
+    bc1, bc3 = {}, {}
+    for L in range(20):
+        if oracle.Reference().level_params(L, 0x04)[1] == 0:
+            continue
+        for iname, it in INTERPS.items():
+            p = BC1Params(level=L, interpolator=it)
+            bc3[f"L{L}_{iname}"] = checked(f"hazard bc3 L{L} {iname}", ref.bc3_encode(img, w, h, p),
+                                           orc.bc3_encode(img, w, h, p))
+            for mn, m in MODES.items():
+                p = BC1Params(level=L, color_mode=m, interpolator=it)
+                bc1[f"L{L}_{mn}_{iname}"] = checked(f"hazard L{L} {mn} {iname}", ref.bc1_encode(img, w, h, p),
+                                                    orc.bc1_encode(img, w, h, p))
+    return {"input": {"gen": "hazard_mix", "w": w, "h": h, "sha256": sha(img), "counts": syn.hazard_counts(img)},
+            "bc1": bc1, "bc3": bc3}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--skip-full", action="store_true", help="only the 512^2 cases")
     ap.add_argument("--ce-only", action="store_true", help="only ce_counts.json, from the oracle")
+    ap.add_argument("--hazard-only", action="store_true", help="only the hazard corpus, added to ref_hashes.json")
     args = ap.parse_args()
     if args.ce_only:
         ce_only()
@@ -130,6 +161,14 @@ def main():
     ref, orc = oracle.Reference(), oracle.Oracle()
     ref.set_threads(os.cpu_count())
     orc.set_threads(os.cpu_count())
+
+    if args.hazard_only:
+        path = os.path.join(HERE, "ref_hashes.json")
+        hashes = json.load(open(path))
+        hashes["hazard_mix"] = hazard_entry(ref, orc)
+        with open(path, "w") as f:
+            json.dump(hashes, f, indent=1)
+        return
 
     with open(os.path.join(HERE, "kat.json"), "w") as f:
         json.dump(kat(), f, indent=1)
@@ -158,6 +197,7 @@ def main():
                 sweep[f"L{L}_{mn}_{iname}"] = checked(f"sweep L{L}", ref.bc1_encode(img, 512, 512, p), orc.bc1_encode(img, 512, 512, p))
     hashes["mix_512_sweep"] = {"input": {"gen": "block_mix", "w": 512, "h": 512, "workload": 2, "stream": 1,
                                          "sha256": sha(img)}, "bc1": sweep}
+    hashes["hazard_mix"] = hazard_entry(ref, orc)
     print(f"512 cases done in {time.time() - t0:.0f}s", flush=True)
 
     ce, rep = {}, {}

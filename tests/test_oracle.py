@@ -103,6 +103,25 @@ def test_oracle_matches_reference_hashes_512(oracle_lib):
             assert sha(got) == h, key
 
 
+def test_oracle_matches_reference_hashes_hazards(oracle_lib):
+    """A slice of the adversarial hazard corpus (all settings: tests/golden/make_golden.py)."""
+    entry = json.load(open(HASHES_PATH))["hazard_mix"]
+    img = syn.hazard_mix()
+    assert sha(img) == entry["input"]["sha256"]
+    assert syn.hazard_counts(img) == entry["input"]["counts"]
+    h, w = img.shape[:2]
+    for key, digest in entry["bc1"].items():
+        level, interp = int(key.split("_")[0][1:]), key.rsplit("_", 1)[1]
+        mode = key[len(key.split("_")[0]) + 1:-(len(interp) + 1)]
+        if level in (0, 2, 5, 9, 13) or (level == 18 and interp in ("ideal", "nvidia")):
+            got = oracle_lib.bc1_encode(img, w, h, BC1Params(level=level, color_mode=MODES[mode], interpolator=INTERPS[interp]))
+            assert sha(got) == digest, key
+    for key in ("L0_ideal", "L5_amd", "L10_round", "L18_nvidia"):
+        level, interp = int(key.split("_")[0][1:]), key.split("_")[1]
+        got = oracle_lib.bc3_encode(img, w, h, BC1Params(level=level, interpolator=INTERPS[interp]))
+        assert sha(got) == entry["bc3"][key], key
+
+
 def test_oracle_matches_reference_live(oracle_lib, reference_lib):
     """Live comparison with the compiled reference on fresh seeded inputs (every level,
     mode and interpolator; LeastSquares x Nvidia excluded: the reference reads

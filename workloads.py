@@ -18,6 +18,11 @@ sizes and value distributions of the reference benchmark plan:
 * ``mixed_batch``      many textures with log-uniform sizes in [4, 2048],
                        25% forced to a non-multiple of 4, formats
                        BC1:BC3:BC4:BC5 = 4:3:2:1, levels uniform in {0,5,10,18}.
+* ``hazard_mix``       adversarial blocks aimed at the encoder's rarely taken
+                       branches (greyscale, all-black solid, near-black texels,
+                       three-colour+black, RGB-uniform blocks with varying alpha,
+                       extreme two-colour and solid blocks); ``hazard_counts``
+                       counts the blocks that reach each branch.
 
 All arrays are ``uint8`` of shape ``(h, w, 4)``, row-major RGBA.
 """
@@ -214,3 +219,122 @@ class MixedBatchPools:
         y0 = int(self.rng.integers(0, self.side - item.height + 1))
         x0 = int(self.rng.integers(0, self.side - item.width + 1))
         return np.ascontiguousarray(pool[y0:y0 + item.height, x0:x0 + item.width])
+
+
+# ---------------------------------------------------------------------------
+# adversarial blocks for the encoder's rarely taken branches
+# ---------------------------------------------------------------------------
+HAZARD_CLASSES = ("grey_narrow", "grey_wide", "black_solid", "near_black_mix", "near_black_edge", "grey_plus_black",
+                  "rgb_uniform_alpha", "two_colour_extreme", "solid_extreme", "dark_solid")
+_EXTREMES = np.array([0, 1, 2, 3, 4, 5, 7, 8, 127, 128, 250, 253, 254, 255])
+
+
+def _hazard_blocks(rng: np.random.Generator, cls: np.ndarray) -> np.ndarray:
+    """(n, 16, 4) uint8 RGBA blocks; block k drawn from HAZARD_CLASSES[cls[k]]."""
+    n = len(cls)
+    out = np.empty((n, 16, 4), np.uint8)
+    out[..., 3] = 255
+    for k, name in enumerate(HAZARD_CLASSES):
+        idx = np.nonzero(cls == k)[0]
+        m = len(idx)
+        if m == 0:
+            continue
+        b = np.empty((m, 16, 4), np.int64)
+        b[..., 3] = 255
+        if name == "grey_narrow":  # greyscale, two adjacent levels: max.r - min.r == 1 (< 2), never solid
+            base = rng.integers(0, 255, m)
+            v = base[:, None] + rng.integers(0, 2, (m, 16))
+            v[:, 0], v[:, 1] = base, base + 1
+            b[..., 0] = b[..., 1] = b[..., 2] = v
+        elif name == "grey_wide":  # greyscale spanning >= 2 levels
+            lo = rng.integers(0, 250, m)[:, None]
+            hi = np.minimum(255, lo + 2 + rng.integers(0, 120, m)[:, None])
+            v = lo + np.floor(rng.random((m, 16)) * (hi - lo + 1)).astype(np.int64)
+            v[:, 3], v[:, 12] = lo[:, 0], hi[:, 0]
+            b[..., 0] = b[..., 1] = b[..., 2] = v
+        elif name == "black_solid":  # every texel (0, 0, 0, a)
+            b[..., :3] = 0
+            b[..., 3] = np.where(rng.random(m) < 0.25, rng.integers(0, 256, m), 255)[:, None]
+        elif name == "near_black_mix":  # (r|g|b) < 4 texels among bright ones: the 3-colour+black trial
+            dark = rng.integers(0, 4, (m, 16, 3))
+            bright = rng.integers(0, 256, (m, 16, 3))
+            bright[:, 0] = np.maximum(bright[:, 0], 64)
+            is_dark = rng.random((m, 16)) < rng.uniform(0.15, 0.7, m)[:, None]
+            is_dark[:, 0], is_dark[:, 1] = True, False
+            b[..., :3] = np.where(is_dark[..., None], dark, bright)
+        elif name == "near_black_edge":  # channels straddling the (r|g|b) < 4 rule: 0..7
+            b[..., :3] = rng.integers(0, 8, (m, 16, 3))
+            b[:, 0, :3] = rng.integers(0, 4, (m, 3))
+            b[:, 1, :3] = [4, 0, 0]
+        elif name == "grey_plus_black":  # greyscale bright texels plus black ones, texel (0,0) black
+            lo = rng.integers(4, 200, m)[:, None]
+            v = lo + rng.integers(0, rng.integers(1, 56, m)[:, None] + 1, (m, 16))
+            v = np.minimum(v, 255)
+            b[..., 0] = b[..., 1] = b[..., 2] = v
+            is_dark = rng.random((m, 16)) < 0.4
+            is_dark[:, 0], is_dark[:, 1] = True, False
+            b[..., :3] = np.where(is_dark[..., None], rng.integers(0, 4, (m, 16, 3)), b[..., :3])
+        elif name == "rgb_uniform_alpha":  # one RGB colour, alpha varying: not a solid block
+            b[..., :3] = rng.integers(0, 256, (m, 1, 3))
+            b[..., 3] = rng.integers(0, 256, (m, 16))
+            b[:, 0, 3], b[:, 1, 3] = 0, 255
+        elif name == "two_colour_extreme":  # two colours from extreme channel values, random partition
+            c = _EXTREMES[rng.integers(0, len(_EXTREMES), (m, 2, 3))]
+            c[:, 1, 0] = np.where((c[:, 0] == c[:, 1]).all(1), 255 - c[:, 0, 0], c[:, 1, 0])
+            sel = rng.random((m, 16)) < rng.uniform(0.1, 0.9, m)[:, None]
+            sel[:, 0], sel[:, 1] = False, True
+            b[..., :3] = np.where(sel[..., None], c[:, 1][:, None, :], c[:, 0][:, None, :])
+        elif name == "solid_extreme":  # solid blocks of extreme channel values
+            b[..., :3] = _EXTREMES[rng.integers(0, len(_EXTREMES), (m, 1, 3))]
+        elif name == "dark_solid":  # solid, not black, small channels
+            c = rng.integers(0, 8, (m, 1, 3))
+            c[:, 0, 2] = np.where((c[:, 0] == 0).all(1), 1, c[:, 0, 2])
+            b[..., :3] = c
+        out[idx] = np.clip(b, 0, 255).astype(np.uint8)
+    return out
+
+
+def hazard_mix(w: int = 512, h: int = 384, workload: int = 11, stream: int = 0) -> np.ndarray:
+    """RGBA8 texture of adversarial blocks: classes of HAZARD_CLASSES in equal shares
+    (round-robin over a seeded permutation of the block positions)."""
+    rng = rng_for(workload, stream)
+    bw, bh = (w + 3) // 4, (h + 3) // 4
+    n = bw * bh
+    cls = (rng.permutation(n) % len(HAZARD_CLASSES)).astype(np.int64)
+    return _blocks_to_image(_hazard_blocks(rng, cls), bw, bh, w, h)
+
+
+def hazard_counts(img: np.ndarray) -> dict:
+    """Blocks of a block-aligned RGBA8 texture that reach each rarely taken branch of
+    BC1Encoder::EncodeBlock (BC1Encoder.cpp:261-342):
+
+      grey_narrow     greyscale, not solid, max.r - min.r < 2 (FindEndpoints :476-484)
+      grey_wide       greyscale, not solid, max.r - min.r >= 2 (:485-493)
+      black_solid     solid with r = g = b = 0 (WriteBlockSolid's all-black rule, :349-353)
+      tcb_trial       has_black and not max.IsBlack(): the 3-colour+black trial (:327)
+      near_black      holds a texel with (r|g|b) in {3, 4}, either side of IsBlack (Color.h:82)
+      grey_ignoring_black  greyscale over its non-black texels but with a black one:
+                      the greyscale branch inside the 3-colour+black trial
+      rgb_uniform_alpha_varies  one RGB colour, not solid (IsSingleColor compares RGBA)
+    """
+    hh, ww = img.shape[:2]
+    bl = img.reshape(hh // 4, 4, ww // 4, 4, 4).transpose(0, 2, 1, 3, 4).reshape(-1, 16, 4).astype(np.int64)
+    rgb = bl[..., :3]
+    solid = (bl == bl[:, :1]).all((1, 2))
+    grey = ((rgb[..., 0] == rgb[..., 1]) & (rgb[..., 0] == rgb[..., 2])).all(1)
+    rng_r = rgb[..., 0].max(1) - rgb[..., 0].min(1)
+    ored = rgb[..., 0] | rgb[..., 1] | rgb[..., 2]
+    is_black = ored < 4
+    mx = rgb.max(1)
+    max_black = (mx[:, 0] | mx[:, 1] | mx[:, 2]) < 4
+    nb_grey = np.where(is_black, True, (rgb[..., 0] == rgb[..., 1]) & (rgb[..., 0] == rgb[..., 2])).all(1)
+    rgb_uni = (rgb == rgb[:, :1]).all((1, 2))
+    return {
+        "grey_narrow": int((grey & ~solid & (rng_r < 2)).sum()),
+        "grey_wide": int((grey & ~solid & (rng_r >= 2)).sum()),
+        "black_solid": int((solid & (ored[:, 0] == 0)).sum()),
+        "tcb_trial": int((~solid & is_black.any(1) & ~max_black).sum()),
+        "near_black": int((~solid & ((ored == 3) | (ored == 4)).any(1)).sum()),
+        "grey_ignoring_black": int((~solid & ~grey & nb_grey & is_black.any(1) & ~max_black).sum()),
+        "rgb_uniform_alpha_varies": int((rgb_uni & ~solid).sum()),
+    }
