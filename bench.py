@@ -207,33 +207,50 @@ def barrier(world: int):
         dist.barrier()
 
 
-def cpu_reference_sample(img: np.ndarray, repeats: int = 1):
-    """The reference encoder (as shipped: BlockEncoder::Encode with OpenMP) on a
-    512x512 crop for each of the 36 settings. Returns (Mblocks/s, seconds, cores, kind)."""
+def cpu_reference_sample(img: np.ndarray, mode: int = 0, threads: int = 0, side: int = 512):
+    """The reference encoder on a side x side crop for each of the 36 settings, encode only
+    (encoder and input built beforehand). mode 0: its own Encode as shipped (BlockEncoder::Encode,
+    OpenMP over block rows for BC1); mode 1: OpenMP over EncodeBlock. Returns
+    (Mblocks/s, seconds, threads, kind)."""
     import oracle
 
-    crop = np.ascontiguousarray(img[:512, :512])
-    if oracle.reference_available():
-        lib, kind = oracle.Reference(), "reference"
-    else:
-        lib, kind = oracle.Oracle(), "port"
-    cores = os.cpu_count() or 1
-    lib.set_threads(cores)
-    blocks = 0
+    crop = np.ascontiguousarray(img[:side, :side])
+    cores = threads or os.cpu_count() or 1
+    if not oracle.reference_available():
+        raise RuntimeError("the compiled reference (oracle/_ref/libqtref.so) is not built")
+    ref = oracle.Reference()
+    ref.set_threads(cores)
+    secs = 0.0
     t0 = time.perf_counter()
-    for _ in range(repeats):
-        for L, _mn, m, _in, it in SETTINGS:
-            lib.bc1_encode(crop, 512, 512, oracle.BC1Params(level=L, color_mode=m, interpolator=it), mode=0)
-            blocks += 128 * 128
-    dt = time.perf_counter() - t0
-    return blocks / dt / 1e6, dt, cores, kind
+    for L, _mn, m, _in, it in SETTINGS:
+        secs += ref.time_encode(1, crop, side, side, oracle.BC1Params(level=L, color_mode=m, interpolator=it),
+                                mode=mode, reps=1)
+    wall = time.perf_counter() - t0
+    ref.set_threads(os.cpu_count() or 1)
+    return (side // 4) ** 2 * len(SETTINGS) / secs / 1e6, wall, cores, "reference"
+
+
+def cpu_sweep_figures(img: np.ndarray) -> dict:
+    """The other two CPU figures of the reference's timing plan for the sweep: OpenMP over
+    EncodeBlock on the same 512x512 crops, and one thread on 128x128 crops."""
+    omp, t1, cores, _ = cpu_reference_sample(img, mode=1)
+    one, t2, _, _ = cpu_reference_sample(img, mode=1, threads=1, side=128)
+    return {"omp_over_blocks": omp, "single_thread": one, "unit": "Mblocks/s", "cores": cores, "kind": "reference",
+            "sample": "36 settings on 512x512 crops (one thread: 128x128 crops); encode only",
+            "cpu_seconds": t1 + t2}
 
 
 def run_reference_arm(args, world, rank):
     if rank != 0:
         return
+    import oracle
     import workloads as syn
 
+    if not oracle.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "the compiled reference (oracle/_ref/libqtref.so, "
+                                                             "built by oracle/Makefile from the reference sources) "
+                                                             "is missing"}), flush=True)
+        return
     img = syn.block_mix(W, H)
     vals = []
     for i in range(args.warmup + args.steps):
@@ -241,7 +258,8 @@ def run_reference_arm(args, world, rank):
         if i >= args.warmup:
             vals.append(v)
     value = float(np.mean(vals))
-    sample = "512x512 crop (16,384 blocks) of the workload texture for each of the 36 settings per step"
+    sample = ("512x512 crop (16,384 blocks) of the workload texture for each of the 36 settings per step; "
+              "the reference's own Encode as shipped (OpenMP over block rows), encode only")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "Mblocks/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 36 * 16384 / value / 1e3,
@@ -383,12 +401,236 @@ def run_ours(args, world, rank, local):
         line["serve"] = measure_serving(args, dev)
     if not args.no_dds and world == 1:
         line["dds"] = measure_dds(args, dev)
+    if not args.no_configs and world == 1:
+        line["config_bc1_512_L5"] = measure_config1(dev, stream, flush)
+        line["config_bc3_bc4_bc5_8192"] = measure_config3(dev, stream)
     if world == 1 and rank == 0 and not args.no_cpu:
         v, dt, cores, kind = cpu_reference_sample(img)
         line["cpu_baseline"] = {"value": v, "unit": "Mblocks/s", "cores": cores, "kind": kind,
-                                "sample": f"512x512 crop x 36 settings, as-shipped OpenMP encode, {dt:.1f} s"}
+                                "sample": f"512x512 crop x 36 settings, the reference's own Encode as shipped "
+                                          f"(OpenMP), encode only, {dt:.1f} s"}
+        line["cpu_figures"] = cpu_sweep_figures(img)
     if rank == 0:
         print(json.dumps(line), flush=True)
+
+
+GOLDEN_HASHES = os.path.join(ROOT, "tests", "golden", "ref_hashes.json")
+
+
+def _sha(b) -> str:
+    import hashlib
+
+    return hashlib.sha256(bytes(b)).hexdigest()
+
+
+def _timed_each(fn, stream, reps: int, flush=None) -> float:
+    """Median CUDA-event time (ms) of `fn` on `stream` over `reps` runs, L2 flushed before each
+    run when `flush` (a device buffer larger than L2) is given."""
+    import torch
+
+    fn()
+    ts = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        b.synchronize()
+        ts.append(a.elapsed_time(b))
+    return float(np.median(ts))
+
+
+def _wall_each(fn, reps: int) -> float:
+    """Median wall time (ms) of `fn` (a call that returns with its result in host memory)."""
+    fn()
+    ts = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        fn()
+        ts.append(time.perf_counter() - t0)
+    return float(np.median(ts)) * 1e3
+
+
+def cpu_figures(fmt: int, img: np.ndarray, params=None, c0: int = 0, c1: int = 1, side: int = 0, single_side: int = 0,
+                decode_blocks=None, reps: int = 1) -> dict:
+    """The reference's CPU encoder (oracle/_ref, unmodified sources) three ways, as the reference's
+    timing plan asks: as shipped (its own Encode: OpenMP for BC1 only, serial for BC3/BC4/BC5),
+    OpenMP over EncodeBlock (the fair parallel figure), and one thread. Encode only (tables and
+    input built beforehand), best of `reps` after one untimed run, on a `side`^2 crop (single
+    thread: `single_side`^2). With `decode_blocks`, the same three for decoding them instead."""
+    import oracle
+
+    if not oracle.reference_available():
+        return {"unavailable": "compiled reference (oracle/_ref) not built"}
+    ref = oracle.Reference()
+    cores = os.cpu_count() or 1
+    params = params or oracle.BC1Params()
+    h, w = img.shape[:2]
+    side = side or min(w, h)
+    single_side = single_side or side
+
+    def rate(s, mode, threads):
+        ref.set_threads(threads)
+        nb = (s // 4) ** 2
+        if decode_blocks is not None:
+            bw = w // 4
+            blk = decode_blocks.reshape(h // 4, bw, -1)[: s // 4, : s // 4].reshape(-1)
+            t = ref.time_decode(fmt, np.ascontiguousarray(blk), s, s, params.interpolator, c0, c1, mode, reps)
+        else:
+            t = ref.time_encode(fmt, np.ascontiguousarray(img[:s, :s]), s, s, params, c0, c1, mode, reps)
+        return nb / t / 1e6
+
+    t0 = time.perf_counter()
+    out = {"as_shipped": rate(side, 0, cores), "omp_over_blocks": rate(side, 1, cores),
+           "single_thread": rate(single_side, 1, 1), "unit": "Mblocks/s", "cores": cores, "kind": "reference",
+           "sample": f"{side}x{side} crop ({(side // 4) ** 2} blocks); one thread on {single_side}x{single_side}"}
+    ref.set_threads(cores)
+    out["cpu_seconds"] = time.perf_counter() - t0
+    return out
+
+
+def measure_config1(dev, stream, flush, reps: int = 20):
+    """512x512 gradient + noise (10% solid blocks), BC1 level 5 four-colour Ideal encode, then
+    decode. Device-resident through the C-ABI (CUDA events, L2 flushed before each run), and end
+    to end through the drop-in Python API (BC1Encoder(5).encode(RawTexture) and
+    BC1Decoder().decode, whose texels live in pageable host memory), beside the reference's CPU
+    figures. Outputs are checked against the reference's committed digests."""
+    import torch
+
+    import quicktex_b200 as qt
+    import workloads as syn
+    from quicktex_b200 import capi
+    from quicktex_b200.s3tc.bc1 import BC1Decoder, BC1Encoder
+
+    side = 512
+    nb = (side // 4) ** 2
+    img = syn.gradient_noise(side, side)
+    golden = json.load(open(GOLDEN_HASHES))["gradient_512"]
+    d_in = torch.from_numpy(img.reshape(-1).copy()).to(dev)
+    d_blk = torch.empty(nb * 8, dtype=torch.uint8, device=dev)
+    d_dec = torch.empty(side * side * 4, dtype=torch.uint8, device=dev)
+    p = capi.params_for_level(5)
+    sp = stream.cuda_stream
+    enc_fn = lambda: capi.bc1_encode_device(d_in.data_ptr(), side, side, p, d_blk.data_ptr(), sp)  # noqa: E731
+    dec_fn = lambda: capi.bc1_decode_device(d_blk.data_ptr(), side, side, 0, False, d_dec.data_ptr(), sp)  # noqa: E731
+    enc_ms = _timed_each(enc_fn, stream, reps, flush)
+    dec_ms = _timed_each(dec_fn, stream, reps, flush)
+    torch.cuda.synchronize()
+    exact = (_sha(d_blk.cpu().numpy()) == golden["bc1_L5_four_ideal"] and
+             _sha(d_dec.cpu().numpy()) == golden["bc1_decode_ideal"])
+
+    tex = qt.RawTexture.frombytes(img.tobytes(), side, side)
+    enc, dec = BC1Encoder(5), BC1Decoder()
+    blocks = enc.encode(tex)
+    exact = exact and _sha(blocks.tobytes()) == golden["bc1_L5_four_ideal"]
+    e_enc = _wall_each(lambda: enc.encode(tex), reps)
+    e_dec = _wall_each(lambda: dec.decode(blocks), reps)
+    e_both = _wall_each(lambda: dec.decode(enc.encode(tex)), reps)
+    peaks, kind = load_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    cpu_enc = cpu_figures(1, img, reps=5)
+    cpu_dec = cpu_figures(1, img, decode_blocks=np.frombuffer(blocks.tobytes(), np.uint8), reps=5)
+    return {
+        "workload": "512x512 gradient + noise, 10% solid blocks; BC1 level 5 four-colour Ideal encode, then decode",
+        "blocks": nb,
+        "device": {"encode_mblocks_s": nb / enc_ms / 1e3, "decode_mblocks_s": nb / dec_ms / 1e3,
+                   "encode_decode_mblocks_s": nb / (enc_ms + dec_ms) / 1e3, "encode_ms": enc_ms, "decode_ms": dec_ms,
+                   "l2": "flushed before each run"},
+        "e2e_dropin": {"encode_mblocks_s": nb / e_enc / 1e3, "decode_mblocks_s": nb / e_dec / 1e3,
+                       "encode_decode_mblocks_s": nb / e_both / 1e3,
+                       "path": "BC1Encoder(5).encode(RawTexture) / BC1Decoder().decode: pageable host memory, "
+                               "copies and kernel launches inside the timed call"},
+        "roofline": {"bound": "hbm", "encode_gb_s": nb * 72 / enc_ms / 1e6, "decode_gb_s": nb * 72 / dec_ms / 1e6,
+                     "peak_gb_s": hbm, "encode_frac": nb * 72 / enc_ms / 1e6 / hbm,
+                     "decode_frac": nb * 72 / dec_ms / 1e6 / hbm, "peak_source": kind,
+                     "note": "1 MiB of texels: one launch of 256 CTAs, latency-bound, not bandwidth-bound"},
+        "cpu_encode": cpu_enc, "cpu_decode": cpu_dec,
+        "bit_exact_vs_reference": exact,
+    }
+
+
+def measure_config3(dev, stream, reps: int = 5):
+    """8192x8192: BC3 level 5 (Ideal) of the colour block mix with the alpha mix (binary
+    cutouts, ramps, noise), BC4 on channels 0, 1 and 3 of it, and BC5 (channels 0, 1) of the
+    normal map of a sum of 8 Gaussian bumps; each decoded back. Device-resident (256 MiB inputs,
+    larger than L2), CUDA events; BC3 and BC5 encode also end to end through the drop-in Python
+    API from pageable memory. Outputs checked against the reference's committed digests."""
+    import torch
+
+    import quicktex_b200 as qt
+    import workloads as syn
+    from quicktex_b200 import capi
+    from quicktex_b200.s3tc.bc3 import BC3Encoder
+    from quicktex_b200.s3tc.bc5 import BC5Encoder
+
+    side = 8192
+    nb = (side // 4) ** 2
+    golden = json.load(open(GOLDEN_HASHES))
+    ga, gn = golden.get("alpha_8192", {}), golden.get("normal_8192", {})
+    peaks, kind = load_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    sp = stream.cuda_stream
+    L = capi.lib()
+    vp = capi._vp
+    res, exact = {}, {}
+    d_blk = torch.empty(nb * 16, dtype=torch.uint8, device=dev)
+    d_out = torch.empty(side * side * 4, dtype=torch.uint8, device=dev)
+
+    def leg(name, fn, nbytes, golden_key, golden_entry, out_tensor):
+        ms = _timed_each(fn, stream, reps)
+        torch.cuda.synchronize()
+        block_bytes = 16 if name.startswith(("bc3", "bc5")) else 8
+        n = nb * block_bytes if name.endswith("encode") else side * side * 4
+        exact[name] = _sha(out_tensor[:n].cpu().numpy()) == golden_entry.get(golden_key)
+        res[name] = {"ms": ms, "mblocks_s": nb / ms / 1e3, "gb_s": nbytes / ms / 1e6, "frac_of_hbm": nbytes / ms / 1e6 / hbm}
+
+    img = syn.alpha_mix(side, side)
+    d_in = torch.from_numpy(img.reshape(-1)).to(dev)
+    p5 = capi.params_for_level(5)
+    leg("bc3_L5_encode", lambda: capi.bc3_encode_device(d_in.data_ptr(), side, side, p5, d_blk.data_ptr(), sp),
+        nb * 80, "bc3_L5_ideal", ga, d_blk)
+    leg("bc3_decode", lambda: capi.check(L.qt_bc3_decode_device(vp(d_blk.data_ptr()), side, side, 0, vp(d_out.data_ptr()), vp(sp))),
+        nb * 80, "bc3_decode_ideal", ga, d_out)
+    for c in (0, 1, 3):
+        leg(f"bc4_ch{c}_encode", lambda c=c: capi.check(L.qt_bc4_encode_device(vp(d_in.data_ptr()), side, side, c, vp(d_blk.data_ptr()), vp(sp))),
+            nb * 72, f"bc4_ch{c}", ga, d_blk)
+        leg(f"bc4_ch{c}_decode", lambda c=c: capi.check(L.qt_bc4_decode_device(vp(d_blk.data_ptr()), side, side, c, vp(d_out.data_ptr()), vp(sp))),
+            nb * 72, f"bc4_decode_ch{c}", ga, d_out)
+    tex = qt.RawTexture.frombytes(img.tobytes(), side, side)
+    e3 = _wall_each(lambda: BC3Encoder(5).encode(tex), 2)
+    cpu3 = cpu_figures(3, img, capi_params_to_oracle(5), side=2048, single_side=512)
+    cpu4 = {c: cpu_figures(4, img, c0=c, side=2048, single_side=1024) for c in (0, 3)}
+    del tex, img
+
+    nm = syn.normal_map(side, side)
+    d_in.copy_(torch.from_numpy(nm.reshape(-1)))
+    leg("bc5_encode", lambda: capi.check(L.qt_bc5_encode_device(vp(d_in.data_ptr()), side, side, 0, 1, vp(d_blk.data_ptr()), vp(sp))),
+        nb * 80, "bc5_01", gn, d_blk)
+    leg("bc5_decode", lambda: capi.check(L.qt_bc5_decode_device(vp(d_blk.data_ptr()), side, side, 0, 1, vp(d_out.data_ptr()), vp(sp))),
+        nb * 80, "bc5_decode_01", gn, d_out)
+    tex = qt.RawTexture.frombytes(nm.tobytes(), side, side)
+    e5 = _wall_each(lambda: BC5Encoder(0, 1).encode(tex), 2)
+    cpu5 = cpu_figures(5, nm, c0=0, c1=1, side=2048, single_side=1024)
+    del tex, nm
+    return {
+        "workload": "8192x8192: BC3 level 5 Ideal and BC4 channels {0,1,3} of the block mix with the alpha mix; "
+                    "BC5 channels (0,1) of the Gaussian-bump normal map; and their decodes",
+        "blocks": nb, "device": res, "peak_gb_s": hbm, "peak_source": kind,
+        "algorithmic_bytes_per_block": {"bc3": 80, "bc5": 80, "bc4": 72},
+        "e2e_dropin": {"bc3_L5_encode_mblocks_s": nb / e3 / 1e3, "bc5_encode_mblocks_s": nb / e5 / 1e3,
+                       "path": "BC3Encoder(5) / BC5Encoder(0, 1).encode(RawTexture): pageable host memory, "
+                               "copies and kernels inside the timed call"},
+        "cpu": {"bc3_L5_encode": cpu3, "bc4_encode": cpu4, "bc5_encode": cpu5},
+        "bit_exact_vs_reference": exact,
+    }
+
+
+def capi_params_to_oracle(level: int, color_mode: int = 0x04, interpolator: int = 0):
+    import oracle
+
+    return oracle.BC1Params(level=level, color_mode=color_mode, interpolator=interpolator)
 
 
 def measure_batched(args, dev, world):
@@ -400,7 +642,7 @@ def measure_batched(args, dev, world):
     import torch
 
     import workloads as syn
-    from quicktex_b200.batch import Arena, Batch, Job, run_plain, run_plain_host
+    from quicktex_b200.batch import Arena, Batch, Job, run_plain, run_plain_host, run_plain_native
 
     from quicktex_b200.shard import block_cost, max_over_ranks, shard
 
@@ -440,12 +682,17 @@ def measure_batched(args, dev, world):
     torch.cuda.synchronize()
     out_persistent = arena.outputs()  # each texture's bytes (the alignment padding between them is not output)
     arena.d_out.zero_()
-    run_plain(citems, sptr)
+    run_plain_native(citems, sptr)
     torch.cuda.synchronize()
-    plain = timed(lambda: run_plain(citems, sptr), max(1, args.steps // 2))
+    plain = timed(lambda: run_plain_native(citems, sptr), max(1, args.steps // 2))
     arena.download()
     torch.cuda.synchronize()
     identical = out_persistent == arena.outputs()
+    arena.d_out.zero_()
+    plain_py = timed(lambda: run_plain(citems, sptr), max(1, args.steps // 4))
+    arena.download()
+    torch.cuda.synchronize()
+    identical = identical and out_persistent == arena.outputs()
 
     def e2e():
         arena.upload()
@@ -457,7 +704,7 @@ def measure_batched(args, dev, world):
     t0 = time.perf_counter()
     run_plain_host(arena)
     plain_e2e = (time.perf_counter() - t0) * 1e3
-    pm, qm, em = (max_over_ranks(float(np.median(x))) for x in (persistent, plain, e2e_ms))
+    pm, qm, em, ym = (max_over_ranks(float(np.median(x))) for x in (persistent, plain, e2e_ms, plain_py))
     plain_e2e = max_over_ranks(plain_e2e)
     ntiles = batch.last_tiles()
     batch.close()
@@ -469,11 +716,15 @@ def measure_batched(args, dev, world):
         "persistent_mblocks_s": all_blocks / (pm / 1e3) / 1e6,
         "plain_mblocks_s": all_blocks / (qm / 1e3) / 1e6,
         "persistent_over_plain": qm / pm,
+        "plain": "one single-texture device entry point call per texture from the library's C++ loop "
+                 "(qt_batch_run_plain)",
+        "plain_python_loop_mblocks_s": all_blocks / (ym / 1e3) / 1e6,
+        "persistent_over_plain_python_loop": ym / pm,
         "persistent_e2e_mblocks_s": all_blocks / (em / 1e3) / 1e6,
         "plain_e2e_mblocks_s": all_blocks / (plain_e2e / 1e3) / 1e6,
         "persistent_over_plain_e2e": plain_e2e / em,
         "e2e_h2d_bytes": arena.in_bytes, "e2e_d2h_bytes": arena.out_bytes,
-        "ms": {"persistent": pm, "plain": qm, "persistent_e2e": em, "plain_e2e": plain_e2e},
+        "ms": {"persistent": pm, "plain": qm, "plain_python_loop": ym, "persistent_e2e": em, "plain_e2e": plain_e2e},
         "tiles": ntiles,
         "launches_per_step": {"persistent": 1, "plain": len(jobs)},
         "outputs_identical": identical,
@@ -664,6 +915,7 @@ def main():
     ap.add_argument("--batch-count", type=int, default=10000, help="textures in the batched leg")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving leg")
     ap.add_argument("--no-dds", action="store_true", help="skip the mip-chain (DDS) leg")
+    ap.add_argument("--no-configs", action="store_true", help="skip the 512^2 BC1 and 8192^2 BC3/BC4/BC5 legs")
     ap.add_argument("--serve-pool", type=int, default=256, help="distinct request payloads")
     ap.add_argument("--serve-rates", type=float, nargs="+", default=[1000, 10000, 50000])
     ap.add_argument("--serve-seconds", type=float, nargs="+", default=[2.0, 2.0, 1.0])

@@ -196,6 +196,12 @@ int qt_batch_set_grid(qt_batch *b, int ctas_per_sm);
 int qt_batch_run(qt_batch *b, const qt_batch_item *items, size_t n, void *stream);
 /* Number of tiles the last qt_batch_run queued. */
 size_t qt_batch_last_tiles(const qt_batch *b);
+/* The launch model the batch replaces, for comparison: the same items, one
+ * single-texture device entry point call (qt_bc{1,3,4,5}_encode_device /
+ * _decode_device) per texture in a native loop, on `stream`. The reference's
+ * counterpart is one Encode/Decode call per texture (Encoder.h:36-56,
+ * Decoder.h:36-54). Same output bytes as qt_batch_run. */
+int qt_batch_run_plain(const qt_batch_item *items, size_t n, void *stream);
 /* Size the queue for up to `items` textures and `tiles` tiles now, so that later
  * runs within those limits never reallocate it (a reallocation waits for the
  * device and re-captures the graph). Never shrinks the queue. */

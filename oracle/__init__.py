@@ -204,6 +204,30 @@ class Reference(_Lib):
 
     def __init__(self, path: str = REF_SO):
         super().__init__(path)
+        self.lib.ref_time_encode.argtypes = [_i, _vp, _i, _i, _i, _i, _i, _i, _i, _i, _i]
+        self.lib.ref_time_encode.restype = ctypes.c_double
+        self.lib.ref_time_decode.argtypes = [_i, _vp, _i, _i, _i, _i, _i, _i, _i]
+        self.lib.ref_time_decode.restype = ctypes.c_double
+
+    # CPU baseline timing: seconds of the fastest of `reps` runs (after one untimed run) of one
+    # encode/decode, with the codec, its tables and the input built beforehand. mode 0: the
+    # reference's own Encode/Decode loop as shipped; mode 1: OpenMP over EncodeBlock/DecodeBlock.
+    def time_encode(self, fmt: int, rgba, w, h, params: BC1Params = BC1Params(), c0: int = 0, c1: int = 1,
+                    mode: int = 0, reps: int = 1) -> float:
+        src = _as_u8(rgba)
+        t = self.lib.ref_time_encode(fmt, _ptr(src), w, h, params.level, params.color_mode, params.interpolator,
+                                     c0, c1, mode, reps)
+        if t < 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return t
+
+    def time_decode(self, fmt: int, blocks, w, h, interp: int = IDEAL, c0: int = 0, c1: int = 1, mode: int = 0,
+                    reps: int = 1) -> float:
+        src = _as_u8(blocks)
+        t = self.lib.ref_time_decode(fmt, _ptr(src), w, h, interp, c0, c1, mode, reps)
+        if t < 0:
+            raise RuntimeError(self.lib.ref_last_error().decode())
+        return t
 
 
 class Oracle(_Lib):

@@ -97,6 +97,58 @@ template <typename Enc> void run_encode(const Enc &enc, const RawTexture &raw, u
     std::memcpy(out, t.Data(), t.NBytes());
 }
 
+// Seconds of the fastest of `reps` runs (after one untimed run) of one encode of `raw`: mode 0
+// the reference's own Encode, mode 1 OpenMP over EncodeBlock. Only the encode is timed: the
+// encoder, its tables and the input texture exist beforehand (the reference's CPU timing plan).
+template <typename Enc> double time_encode(const Enc &enc, const RawTexture &raw, int mode, int reps) {
+    using Tex = typename Enc::Texture;
+    double best = 1e30;
+    for (int r = 0; r <= reps; r++) {
+        const auto t0 = std::chrono::steady_clock::now();
+        if (mode == 0) {
+            Tex t = enc.Encode(raw);
+            (void)t;
+        } else {
+            Tex t(raw.Width(), raw.Height());
+            const int bx = t.BlocksX(), by = t.BlocksY();
+            const long n = (long)bx * by;
+#pragma omp parallel for schedule(dynamic, 64)
+            for (long i = 0; i < n; i++) {
+                int x = (int)(i % bx), y = (int)(i / bx);
+                t.SetBlock(x, y, enc.EncodeBlock(raw.GetBlock<4, 4>(x, y)));
+            }
+        }
+        const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (r > 0 && dt < best) best = dt;
+    }
+    return best;
+}
+
+// The same for one decode: mode 0 the reference's own (serial) Decode, mode 1 OpenMP over
+// DecodeBlock (block-aligned sizes only, so no two blocks write the same texel).
+template <typename Dec> double time_decode(const Dec &dec, const typename Dec::Texture &tex, int mode, int reps) {
+    double best = 1e30;
+    for (int r = 0; r <= reps; r++) {
+        const auto t0 = std::chrono::steady_clock::now();
+        if (mode == 0) {
+            RawTexture out = dec.Decode(tex);
+            (void)out;
+        } else {
+            RawTexture out(tex.Width(), tex.Height());
+            const int bx = tex.BlocksX(), by = tex.BlocksY();
+            const long n = (long)bx * by;
+#pragma omp parallel for schedule(dynamic, 256)
+            for (long i = 0; i < n; i++) {
+                int x = (int)(i % bx), y = (int)(i / bx);
+                out.SetBlock<4, 4>(x, y, dec.DecodeBlock(tex.GetBlock(x, y)));
+            }
+        }
+        const double dt = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (r > 0 && dt < best) best = dt;
+    }
+    return best;
+}
+
 template <typename F> int guarded(F &&f) {
     try {
         f();
@@ -207,6 +259,39 @@ int ref_bc5_decode(const uint8_t *blocks, int w, int h, int c0, int c1, uint8_t 
         RawTexture r = d.Decode(to_blocks<BC5Block>(blocks, w, h));
         std::memcpy(out, r.Data(), r.NBytes());
     });
+}
+
+// Timing (CPU baseline): seconds of the fastest of `reps` encodes of fmt (1, 3, 4, 5) on the
+// w x h texture; level/color_mode/interp apply to BC1 and BC3, c0/c1 to BC4 (c0) and BC5.
+// Returns a negative value on error (message in ref_last_error).
+double ref_time_encode(int fmt, const uint8_t *rgba, int w, int h, int level, int color_mode, int interp, int c0,
+                       int c1, int mode, int reps) {
+    double t = -1.0;
+    if (guarded([&] {
+            const RawTexture raw = to_raw(rgba, w, h);
+            if (fmt == 1) t = time_encode(BC1Encoder((unsigned)level, static_cast<BC1Encoder::ColorMode>(color_mode), make_interp(interp)), raw, mode, reps);
+            else if (fmt == 3) t = time_encode(BC3Encoder((unsigned)level, make_interp(interp)), raw, mode, reps);
+            else if (fmt == 4) t = time_encode(BC4Encoder((uint8_t)c0), raw, mode, reps);
+            else if (fmt == 5) t = time_encode(BC5Encoder((uint8_t)c0, (uint8_t)c1), raw, mode, reps);
+            else throw std::invalid_argument("format must be 1, 3, 4 or 5");
+        }))
+        return -1.0;
+    return t;
+}
+
+// The same for decoding `blocks` (BC1 with write_alpha = 0; BC3 with the given interpolator).
+double ref_time_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int c0, int c1, int mode, int reps) {
+    double t = -1.0;
+    if (guarded([&] {
+            if (mode == 1 && ((w & 3) || (h & 3))) throw std::invalid_argument("mode 1 needs block-aligned sizes");
+            if (fmt == 1) t = time_decode(BC1Decoder(false, make_interp(interp)), to_blocks<BC1Block>(blocks, w, h), mode, reps);
+            else if (fmt == 3) t = time_decode(BC3Decoder(make_interp(interp)), to_blocks<BC3Block>(blocks, w, h), mode, reps);
+            else if (fmt == 4) t = time_decode(BC4Decoder((uint8_t)c0), to_blocks<BC4Block>(blocks, w, h), mode, reps);
+            else if (fmt == 5) t = time_decode(BC5Decoder((uint8_t)c0, (uint8_t)c1), to_blocks<BC5Block>(blocks, w, h), mode, reps);
+            else throw std::invalid_argument("format must be 1, 3, 4 or 5");
+        }))
+        return -1.0;
+    return t;
 }
 
 }  // extern "C"

@@ -69,8 +69,9 @@ def _lib():
         L.qt_batch_last_tiles.restype = ctypes.c_size_t
         L.qt_batch_reserve.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
         L.qt_copy_async.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
+        L.qt_batch_run_plain.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_size_t, ctypes.c_void_p]
         for n in ("qt_batch_create", "qt_batch_destroy", "qt_batch_set_rules", "qt_batch_set_grid", "qt_batch_run",
-                  "qt_batch_reserve", "qt_copy_async"):
+                  "qt_batch_reserve", "qt_copy_async", "qt_batch_run_plain"):
             getattr(L, n).restype = ctypes.c_int
         _sigs_done = True
     return L
@@ -260,9 +261,19 @@ class Arena:
         return [ho[o:o + j.out_bytes].tobytes() for j, o in zip(self.jobs, self.out_off)]
 
 
+def run_plain_native(items: Sequence[BatchItem], stream: int = 0) -> None:
+    """The same work with one single-texture device entry point call per texture,
+    issued by the library's own C++ loop (``qt_batch_run_plain``): the launch model
+    the batch replaces, with no interpreter in the loop."""
+    L = _lib()
+    arr = (BatchItem * len(items))(*items)
+    capi.check(L.qt_batch_run_plain(arr, len(items), ctypes.c_void_p(stream)))
+
+
 def run_plain(items: Sequence[BatchItem], stream: int = 0) -> None:
     """The same work with one launch per texture through the single-texture
-    device entry points (the launch model the batch replaces)."""
+    device entry points, each called from Python (``run_plain_native`` issues the
+    same calls from C++)."""
     for it in items:
         f, p = it.format, ctypes.byref(it.params)
         src, dst, w, h, s = ctypes.c_void_p(it.src), ctypes.c_void_p(it.dst), it.width, it.height, ctypes.c_void_p(stream)

@@ -6,7 +6,8 @@ Outputs (next to this file, so they travel with the source tree):
   _quicktex.cpython-<ver>-<plat>.so          the pybind11 module, linked against the above
 
 Kernels are compiled for sm_100a only (``-gencode arch=compute_100a,code=sm_100a``),
-with -lineinfo for profiling. nvcc cross-compiles, so this runs on a machine
+with -lineinfo for profiling and -fmad=false (no float contraction, as the reference's
+x86-64 build has none). nvcc cross-compiles, so this runs on a machine
 without a GPU.
 
 Usage:  python quicktex_b200/build.py [--force]
@@ -38,7 +39,7 @@ KERNEL_SRCS = ["qt_kernels.cu", "qt_noalloc.cu", "qt_resize.cu"]
 HOST_SRCS = ["qt_capi.cpp", "qt_batch.cpp", "qt_server.cpp"]
 # every header a source may include: the kernels include qt_bc1_thread.cuh
 HEADERS = sorted(os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".h", ".cuh"))) + \
-    [os.path.join(INCLUDE, "quicktex_cuda.h")]
+    [os.path.join(INCLUDE, "quicktex_cuda.h"), os.path.abspath(__file__)]  # this recipe: its flags
 
 
 def _newer(out: str, deps: list[str]) -> bool:
@@ -78,8 +79,11 @@ def build(force: bool = False, verbose: bool = False) -> None:
         s = os.path.join(CSRC, src)
         o = os.path.join(BUILD, src + ".o")
         if force or not _newer(o, [s] + HEADERS):
-            cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-I" + INCLUDE, "-I" + CSRC,
-                   "-c", s, "-o", o]
+            # -fmad=false: no float multiply-add contraction anywhere, the reference's x86-64 SSE
+            # arithmetic (one rounding per operation) whether or not an expression is written with
+            # explicit round-to-nearest intrinsics
+            cmd = [NVCC, "-O3", "-std=c++17", *ARCH, "-lineinfo", "-fmad=false", "-Xcompiler", "-fPIC", "-I" + INCLUDE,
+                   "-I" + CSRC, "-c", s, "-o", o]
             if verbose:
                 cmd.insert(1, "-Xptxas=-v")
             _run(cmd)

@@ -336,4 +336,27 @@ int qt_batch_run(qt_batch *b, const qt_batch_item *items, size_t n, void *stream
     return QT_OK;
 }
 
+int qt_batch_run_plain(const qt_batch_item *items, size_t n, void *stream) {
+    if (n && !items) return qtk::set_error(QT_ERR_ARG, "items is NULL");
+    for (size_t i = 0; i < n; i++) {
+        const qt_batch_item &it = items[i];
+        if (int rc = check_item(it)) return rc;
+        const int w = it.width, h = it.height, f = it.format;
+        int rc;
+        if (it.op == QT_OP_ENCODE) {
+            rc = f == 1   ? qt_bc1_encode_device(it.src, w, h, &it.params, it.dst, stream)
+                 : f == 3 ? qt_bc3_encode_device(it.src, w, h, &it.params, it.dst, stream)
+                 : f == 4 ? qt_bc4_encode_device(it.src, w, h, it.chan0, it.dst, stream)
+                          : qt_bc5_encode_device(it.src, w, h, it.chan0, it.chan1, it.dst, stream);
+        } else {
+            rc = f == 1   ? qt_bc1_decode_device(it.src, w, h, it.interpolator, it.write_alpha, it.dst, stream)
+                 : f == 3 ? qt_bc3_decode_device(it.src, w, h, it.interpolator, it.dst, stream)
+                 : f == 4 ? qt_bc4_decode_device(it.src, w, h, it.chan0, it.dst, stream)
+                          : qt_bc5_decode_device(it.src, w, h, it.chan0, it.chan1, it.dst, stream);
+        }
+        if (rc) return rc;
+    }
+    return QT_OK;
+}
+
 }  // extern "C"

@@ -9,7 +9,7 @@ import pytest
 import workloads as syn
 from oracle import BC1Params
 from quicktex_b200 import capi
-from quicktex_b200.batch import Batch, Job, run_jobs, run_plain, Arena
+from quicktex_b200.batch import Batch, Job, run_jobs, run_plain, run_plain_native, Arena
 
 pytestmark = pytest.mark.gpu
 
@@ -86,6 +86,11 @@ def test_graph_replay_growth_and_plain_path():
         batched = arena.outputs()
         arena.d_out.zero_()
         run_plain(arena.items(), s.cuda_stream)
+        arena.download()
+        s.synchronize()
+        assert arena.outputs() == batched
+        arena.d_out.fill_(0xA5)
+        run_plain_native(arena.items(), s.cuda_stream)  # the same calls from the library's C++ loop
         arena.download()
         s.synchronize()
         assert arena.outputs() == batched
