@@ -191,6 +191,9 @@ int qt_batch_destroy(qt_batch *b);
 int qt_batch_set_rules(qt_batch *b, const qt_tile_rule *rules, size_t n);
 /* Persistent grid size in CTAs per SM (0 = the kernel's occupancy limit). */
 int qt_batch_set_grid(qt_batch *b, int ctas_per_sm);
+/* Threads per CTA of the persistent kernel: 32, 64 or 128 (the default). Work is
+ * claimed per warp, so the outputs do not depend on it. */
+int qt_batch_set_threads(qt_batch *b, int threads_per_cta);
 /* Enqueue one persistent launch over all items on `stream` (device buffers; the
  * call returns once the work is queued). */
 int qt_batch_run(qt_batch *b, const qt_batch_item *items, size_t n, void *stream);
@@ -260,9 +263,11 @@ int qt_server_create(int device, size_t memory_budget, int slots, size_t max_bat
                      qt_server **out);
 /* Runs every request already submitted to completion, then frees the server. */
 int qt_server_destroy(qt_server *s);
-/* Tuning rules / grid of every slot's queue (as qt_batch_set_rules / qt_batch_set_grid). */
+/* Tuning rules / grid / CTA size of every slot's queue (as qt_batch_set_rules,
+ * qt_batch_set_grid, qt_batch_set_threads). */
 int qt_server_set_rules(qt_server *s, const qt_tile_rule *rules, size_t n);
 int qt_server_set_grid(qt_server *s, int ctas_per_sm);
+int qt_server_set_threads(qt_server *s, int threads_per_cta);
 /* Queue n requests; tags[i] is reported with request i's completion. All or
  * nothing: an invalid request -> QT_ERR_ARG and none is queued. */
 int qt_server_submit(qt_server *s, const qt_batch_item *items, const uint64_t *tags, size_t n);

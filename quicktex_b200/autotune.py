@@ -5,8 +5,15 @@ through ``qt_batch_run`` with each candidate tile size (blocks per queue entry;
 a warp takes one entry at a time) and keeps the fastest; the measured time per
 block becomes the class's cost, which orders the queue heaviest-first. Levels
 not measured take the cost and tile of the nearest measured level. Finally it
-picks the persistent grid's CTAs per SM on a mixed batch. The result is the
-JSON table ``Batch`` loads by default (``data/batch_tuning.json``).
+picks the persistent grid on a mixed batch: threads per CTA (32, 64, 128)
+jointly with CTAs per SM. The result is the JSON table ``Batch`` and the
+serving loop load by default (``data/batch_tuning.json``).
+
+The kernel maps one 4x4 block to one thread, so two knobs of a sub-warp
+mapping have no counterpart here: each thread stages exactly its own block's
+16 texels in shared memory (a staging depth of one block per thread, fixed by
+the mapping), and each thread reads the cluster-fit ordering table row it
+needs straight from L1/L2 (there is no cooperative chunk of the table to size).
 
     python -m quicktex_b200.autotune [--out PATH] [--quick]
 """
@@ -31,6 +38,7 @@ if _ROOT not in sys.path:
 import workloads as synth  # noqa: E402
 
 TILES = (32, 64, 128, 256, 512, 1024, 2048, 4096)
+THREADS = (32, 64, 128)  # threads per CTA of the persistent kernel
 LEVELS = (0, 5, 10, 18)
 
 
@@ -110,20 +118,26 @@ def tune(device: int = 0, quick: bool = False) -> dict:
             near = min(ms, key=lambda x: (abs(x - L), -x))
             rules.append({"op": 0, "format": fmt, "level": L, "tile_blocks": ms[near]["tile_blocks"],
                           "cost_per_block": ms[near]["us_per_kblock"] / base})
-    # persistent grid size on a mixed batch
+    # persistent grid on a mixed batch: threads per CTA x resident warps per SM (4 to 16; the
+    # kernel's registers allow 16)
     items = synth.mixed_batch(300 if quick else 1500, workload=7)
     pools = synth.MixedBatchPools(workload=7, side=2048)
     mixed = Arena([Job.encode(i.fmt, pools.texture(i), i.width, i.height, level=i.level, channel=0) for i in items], device)
     mixed.upload()
     batch.set_rules(rules)
     grid = {}
-    for k in (1, 2, 3, 4):
-        batch.set_grid(k)
-        grid[k] = _time(batch, mixed)
-    best_k = min(grid, key=grid.get)
+    for threads in THREADS:
+        batch.set_threads(threads)
+        for warps in (4, 8, 12, 16):
+            k = warps * 32 // threads
+            batch.set_grid(k)
+            grid[f"{threads}x{k}"] = _time(batch, mixed)
+    best = min(grid, key=grid.get)
+    best_threads, best_k = (int(x) for x in best.split("x"))
     batch.close()
     return {"device": torch.cuda.get_device_name(device), "when": time.strftime("%Y-%m-%dT%H:%M:%SZ", time.gmtime()),
-            "ctas_per_sm": best_k, "grid_ms": grid, "measured": measured, "rules": rules}
+            "threads_per_cta": best_threads, "ctas_per_sm": best_k, "grid_ms": grid, "measured": measured,
+            "rules": rules}
 
 
 def main():
@@ -136,7 +150,7 @@ def main():
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     with open(args.out, "w") as f:
         json.dump(t, f, indent=1)
-    print(json.dumps({k: t[k] for k in ("device", "ctas_per_sm", "grid_ms")}))
+    print(json.dumps({k: t[k] for k in ("device", "threads_per_cta", "ctas_per_sm", "grid_ms")}))
     for m in t["measured"]:
         print(m)
 

@@ -64,13 +64,14 @@ def _lib():
         L.qt_batch_destroy.argtypes = [ctypes.c_void_p]
         L.qt_batch_set_rules.argtypes = [ctypes.c_void_p, ctypes.POINTER(TileRule), ctypes.c_size_t]
         L.qt_batch_set_grid.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.qt_batch_set_threads.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.qt_batch_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(BatchItem), ctypes.c_size_t, ctypes.c_void_p]
         L.qt_batch_last_tiles.argtypes = [ctypes.c_void_p]
         L.qt_batch_last_tiles.restype = ctypes.c_size_t
         L.qt_batch_reserve.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_size_t]
         L.qt_copy_async.argtypes = [ctypes.c_void_p, ctypes.c_size_t, ctypes.c_void_p]
         L.qt_batch_run_plain.argtypes = [ctypes.POINTER(BatchItem), ctypes.c_size_t, ctypes.c_void_p]
-        for n in ("qt_batch_create", "qt_batch_destroy", "qt_batch_set_rules", "qt_batch_set_grid", "qt_batch_run",
+        for n in ("qt_batch_create", "qt_batch_destroy", "qt_batch_set_rules", "qt_batch_set_grid", "qt_batch_set_threads", "qt_batch_run",
                   "qt_batch_reserve", "qt_copy_async", "qt_batch_run_plain"):
             getattr(L, n).restype = ctypes.c_int
         _sigs_done = True
@@ -101,6 +102,8 @@ class Batch:
     def apply_tuning(self, tuning: dict) -> None:
         rules = tuning.get("rules", [])
         self.set_rules(rules)
+        if tuning.get("threads_per_cta"):
+            self.set_threads(int(tuning["threads_per_cta"]))
         if tuning.get("ctas_per_sm"):
             self.set_grid(int(tuning["ctas_per_sm"]))
 
@@ -112,6 +115,10 @@ class Batch:
 
     def set_grid(self, ctas_per_sm: int) -> None:
         capi.check(_lib().qt_batch_set_grid(self.handle, ctas_per_sm))
+
+    def set_threads(self, threads_per_cta: int) -> None:
+        """Threads per CTA of the persistent kernel (32, 64 or 128)."""
+        capi.check(_lib().qt_batch_set_threads(self.handle, threads_per_cta))
 
     def reserve(self, items: int, tiles: int) -> None:
         """Size the queue now so runs within these limits never reallocate it."""

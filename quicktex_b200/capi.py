@@ -27,9 +27,10 @@ EXPORTS = (
     "qt_bc4_encode_host", "qt_bc4_encode_device", "qt_bc5_encode_host", "qt_bc5_encode_device",
     "qt_bc1_decode_host", "qt_bc1_decode_device", "qt_bc3_decode_host", "qt_bc3_decode_device",
     "qt_bc4_decode_host", "qt_bc4_decode_device", "qt_bc5_decode_host", "qt_bc5_decode_device",
-    "qt_batch_create", "qt_batch_destroy", "qt_batch_set_rules", "qt_batch_set_grid", "qt_batch_run",
+    "qt_batch_create", "qt_batch_destroy", "qt_batch_set_rules", "qt_batch_set_grid", "qt_batch_set_threads", "qt_batch_run",
     "qt_batch_last_tiles", "qt_batch_reserve", "qt_copy_async", "qt_batch_run_noalloc", "qt_batch_run_plain",
-    "qt_server_create", "qt_server_destroy", "qt_server_set_rules", "qt_server_set_grid", "qt_server_submit",
+    "qt_server_create", "qt_server_destroy", "qt_server_set_rules", "qt_server_set_grid", "qt_server_set_threads",
+    "qt_server_submit",
     "qt_server_poll", "qt_server_get_stats", "qt_server_clock",
     "qt_resize_bilinear_device", "qt_flip_swizzle_device", "qt_bc1_encode_kernels",
 )

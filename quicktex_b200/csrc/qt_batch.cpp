@@ -65,6 +65,7 @@ struct qt_batch {
     std::mutex mu;
     Rule rules[2 * 4 * kLevels];
     int ctas_per_sm = 0;
+    int threads = 128;  // per CTA of the persistent kernel
     size_t cap_items = 0, cap_tiles = 0, last_tiles = 0;
     qtk::BatchItemDev *d_items = nullptr, *h_items = nullptr;
     qtk::TileDev *d_tiles = nullptr, *h_tiles = nullptr;
@@ -227,6 +228,20 @@ int qt_batch_set_grid(qt_batch *b, int ctas_per_sm) {
     return QT_OK;
 }
 
+int qt_batch_set_threads(qt_batch *b, int threads_per_cta) {
+    if (!b || (threads_per_cta != 32 && threads_per_cta != 64 && threads_per_cta != 128))
+        return qtk::set_error(QT_ERR_ARG, "threads per CTA must be 32, 64 or 128");
+    std::lock_guard<std::mutex> lk(b->mu);
+    if (threads_per_cta != b->threads && b->exec) {
+        cudaGraphExecDestroy(b->exec);
+        cudaGraphDestroy(b->graph);
+        b->exec = nullptr;
+        b->graph = nullptr;
+    }
+    b->threads = threads_per_cta;
+    return QT_OK;
+}
+
 size_t qt_batch_last_tiles(const qt_batch *b) { return b ? b->last_tiles : 0; }
 
 int qt_copy_async(const qt_copy *copies, size_t n, void *stream) {
@@ -316,7 +331,7 @@ int qt_batch_run(qt_batch *b, const qt_batch_item *items, size_t n, void *stream
         const int grid = b->ctas_per_sm > 0 ? qtk::batch_sms() * b->ctas_per_sm : 0;
         if ((e = cudaStreamBeginCapture(b->capture, cudaStreamCaptureModeThreadLocal)) != cudaSuccess)
             return qtk::cuda_error((int)e, "graph capture");
-        const int lrc = qtk::launch_batch(b->d_items, b->d_tiles, b->d_ctl, grid, b->capture);
+        const int lrc = qtk::launch_batch(b->d_items, b->d_tiles, b->d_ctl, grid, b->threads, b->capture);
         cudaGraph_t g = nullptr;
         e = cudaStreamEndCapture(b->capture, &g);
         if (lrc != 0) {

@@ -50,7 +50,7 @@ __device__ __forceinline__ int cg(uint32_t v) { return (v >> 8) & 0xFF; }
 __device__ __forceinline__ int cb(uint32_t v) { return (v >> 16) & 0xFF; }
 __device__ __forceinline__ bool black(uint32_t v) { return (cr(v) | cg(v) | cb(v)) < 4; }
 
-__device__ __noinline__ M metrics(bool ignore_black) {
+__device__ __forceinline__ M metrics_body(bool ignore_black) {
     M m;
     m.mn[0] = m.mn[1] = m.mn[2] = 255;
     m.mx[0] = m.mx[1] = m.mx[2] = 0;
@@ -76,6 +76,17 @@ __device__ __noinline__ M metrics(bool ignore_black) {
     return m;
 }
 
+// Each phase exists twice: its body (__forceinline__, *_body) and a __noinline__ copy under the
+// plain name, one per template instance. The generic kernels call the copies, which keeps
+// their instruction working set small when one kernel serves every setting; the specialised
+// kernels (k_bc1_fast: one selector kind, no EndpointSearch) inline the bodies, which saves
+// the call overhead where the per-block work is small. INL picks one at compile time.
+__device__ __noinline__ M metrics(bool ignore_black) { return metrics_body(ignore_black); }
+template <bool INL> __device__ __forceinline__ M metrics_(bool ignore_black) {
+    if constexpr (INL) return metrics_body(ignore_black);
+    else return metrics(ignore_black);
+}
+
 // Check2's projected selector (BC1Encoder.cpp:723-729) is trunc(fl(fl(dd * f) + 0.5)) clamped to
 // [1, 3], dd = (p - c0).axis an exact integer, f = fl(4 / den). Rounding is monotone, so the selector
 // is >= s exactly when dd reaches the smallest integer with fl(fl(dd * f) + 0.5) >= s. Over every
@@ -87,7 +98,7 @@ __device__ __forceinline__ int check2_threshold(float f, float quarter_den, floa
 }
 
 // FindSelectors<M>(error_mode), BC1Encoder.cpp:679-779; K is one of the group kernel's kinds
-template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, int hi) {
+template <int IT, int K> __device__ __forceinline__ uint2 find_selectors_body(int lo, int hi) {
     const Pal P = make_pal<IT>(lo, hi, kind_three(K));
     // palette colours (internal order) as packed RGB words and their |c|^2: the error of texel p
     // against colour k is |p|^2 + v_k - 2 p.c_k, exact in integers (dp4a)
@@ -164,6 +175,14 @@ template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, in
         }
     }
     return make_uint2(sel, tot);
+}
+
+template <int IT, int K> __device__ __noinline__ uint2 find_selectors(int lo, int hi) {
+    return find_selectors_body<IT, K>(lo, hi);
+}
+template <int IT, int K, bool INL> __device__ __forceinline__ uint2 find_selectors_(int lo, int hi) {
+    if constexpr (INL) return find_selectors_body<IT, K>(lo, hi);
+    else return find_selectors<IT, K>(lo, hi);
 }
 
 template <int IT> __device__ __forceinline__ uint2 fs_any(int K, int lo, int hi) {
@@ -251,7 +270,7 @@ template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo,
 }
 
 // FindEndpointsSingleColor(result, pixels, color, is_3color) (BC1Encoder.cpp:458-471)
-template <int IT> __device__ __noinline__ R single_color(int stale_lo, int stale_hi, int ar, int ag, int ab, bool is3) {
+template <int IT> __device__ __forceinline__ R single_color_body(int stale_lo, int stale_hi, int ar, int ag, int ab, bool is3) {
     const Pal P = make_pal<IT>(stale_lo, stale_hi, is3);  // colors[2] is internal index 1
     uint32_t e = 0;
 #pragma unroll 4
@@ -270,8 +289,17 @@ template <int IT> __device__ __noinline__ R single_color(int stale_lo, int stale
     return r;
 }
 
+template <int IT> __device__ __noinline__ R single_color(int stale_lo, int stale_hi, int ar, int ag, int ab, bool is3) {
+    return single_color_body<IT>(stale_lo, stale_hi, ar, ag, ab, is3);
+}
+template <int IT, bool INL>
+__device__ __forceinline__ R single_color_(int stale_lo, int stale_hi, int ar, int ag, int ab, bool is3) {
+    if constexpr (INL) return single_color_body<IT>(stale_lo, stale_hi, ar, ag, ab, is3);
+    else return single_color<IT>(stale_lo, stale_hi, ar, ag, ab, is3);
+}
+
 // FindEndpoints (BC1Encoder.cpp:473-677)
-__device__ __noinline__ int2 find_endpoints(const M &m, int mode, bool ignore_black, int power_iters) {
+__device__ __forceinline__ int2 find_endpoints_body(const M &m, int mode, bool ignore_black, int power_iters) {
     int lo, hi;
     if (m.grey) {
         const int fr = cr(px(0));
@@ -401,8 +429,16 @@ __device__ __noinline__ int2 find_endpoints(const M &m, int mode, bool ignore_bl
     return make_int2(lo, hi);
 }
 
+__device__ __noinline__ int2 find_endpoints(const M &m, int mode, bool ignore_black, int power_iters) {
+    return find_endpoints_body(m, mode, ignore_black, power_iters);
+}
+template <bool INL> __device__ __forceinline__ int2 find_endpoints_(const M &m, int mode, bool ignore_black, int power_iters) {
+    if constexpr (INL) return find_endpoints_body(m, mode, ignore_black, power_iters);
+    else return find_endpoints(m, mode, ignore_black, power_iters);
+}
+
 // RefineBlockLS<M> with RefineEndpointsLS<FourColor>(pixels) (BC1Encoder.cpp:781-825, 852-875)
-template <int IT, int K> __device__ __noinline__ R refine_ls(R r, const M &m, int passes) {
+template <int IT, int K, bool INL> __device__ __forceinline__ R refine_ls_body(R r, const M &m, int passes) {
     for (int pass = 0; pass < passes; pass++) {
         R t = r;
         int q0r = 0, q0g = 0, q0b = 0, n1 = 0, n2 = 0, n3 = 0;
@@ -416,7 +452,7 @@ template <int IT, int K> __device__ __noinline__ R refine_ls(R r, const M &m, in
         float m0 = (float)(n1 + 4 * n2 + 9 * n3), m1 = (float)(2 * n1 + 2 * n2), m2 = m1, m3 = (float)(9 * n0 + 4 * n1 + n2);
         const float det = __fsub_rn(__fmul_rn(m0, m3), __fmul_rn(m1, m2));
         if (fabsf(det) < 1e-8f) {
-            t = single_color<IT>(t.lo, t.hi, m.av[0], m.av[1], m.av[2], kind_three(K));
+            t = single_color_<IT, INL>(t.lo, t.hi, m.av[0], m.av[1], m.av[2], kind_three(K));
         } else {
             const float tt = m0; m0 = m3; m3 = tt;
             m1 = -m1;
@@ -431,7 +467,7 @@ template <int IT, int K> __device__ __noinline__ R refine_ls(R r, const M &m, in
             t.hi = precise_round565(__fadd_rn(__fmul_rn(m2, f0r), __fmul_rn(m3, q10r)),
                                     __fadd_rn(__fmul_rn(m2, f0g), __fmul_rn(m3, q10g)),
                                     __fadd_rn(__fmul_rn(m2, f0b), __fmul_rn(m3, q10b)), s_mid5, s_mid6);
-            const uint2 se = find_selectors<IT, K>(t.lo, t.hi);
+            const uint2 se = find_selectors_<IT, K, INL>(t.lo, t.hi);
             t.sel = se.x;
             t.err = se.y;
             t.mode = kind_mode(K);
@@ -441,6 +477,14 @@ template <int IT, int K> __device__ __noinline__ R refine_ls(R r, const M &m, in
         else break;
     }
     return r;
+}
+
+template <int IT, int K> __device__ __noinline__ R refine_ls(R r, const M &m, int passes) {
+    return refine_ls_body<IT, K, false>(r, m, passes);
+}
+template <int IT, int K, bool INL> __device__ __forceinline__ R refine_ls_(R r, const M &m, int passes) {
+    if constexpr (INL) return refine_ls_body<IT, K, true>(r, m, passes);
+    else return refine_ls<IT, K>(r, m, passes);
 }
 
 template <int IT> __device__ __forceinline__ R refine_ls_any(int K, R r, const M &m, int passes) {
@@ -508,8 +552,8 @@ __device__ __forceinline__ bool cf_same_trials(bool four, const R &r, int start,
 
 // RefineBlockCF<M> (BC1Encoder.cpp:877-928): the reference's loop as written. With ORDER,
 // *order_out receives the texel order of the input (rank k -> texel in nibble k).
-template <int IT, int K, bool ORDER = false>
-__device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool exhaustive, int pp_sum, uint64_t *order_out = nullptr) {
+template <int IT, int K, bool ORDER, bool INL>
+__device__ __forceinline__ R refine_cf_body(R r, const M &m, unsigned orderings, bool exhaustive, int pp_sum, uint64_t *order_out) {
     constexpr bool four = !kind_three(K);
     const int tid = threadIdx.x;
     const R orig = r;
@@ -550,7 +594,7 @@ __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool ex
         R t;
         if (single) {
             if (!sc_done) {  // the same trial for every single-colour ordering of this call
-                sc = single_color<IT>(orig.lo, orig.hi, m.av[0], m.av[1], m.av[2], !four);
+                sc = single_color_<IT, INL>(orig.lo, orig.hi, m.av[0], m.av[1], m.av[2], !four);
                 sc.mode = kind_mode(K);
                 sc_done = true;
             }
@@ -582,8 +626,18 @@ __device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool ex
         }
         if (t.err == 0) break;
     }
-    if (from_ls) r.sel = find_selectors<IT, K>(r.lo, r.hi).x;  // selectors of the winning LS trial
+    if (from_ls) r.sel = find_selectors_<IT, K, INL>(r.lo, r.hi).x;  // selectors of the winning LS trial
     return r;
+}
+
+template <int IT, int K, bool ORDER = false>
+__device__ __noinline__ R refine_cf(R r, const M &m, unsigned orderings, bool exhaustive, int pp_sum, uint64_t *order_out = nullptr) {
+    return refine_cf_body<IT, K, ORDER, false>(r, m, orderings, exhaustive, pp_sum, order_out);
+}
+template <int IT, int K, bool INL>
+__device__ __forceinline__ R refine_cf_(R r, const M &m, unsigned orderings, bool exhaustive, int pp_sum) {
+    if constexpr (INL) return refine_cf_body<IT, K, false, true>(r, m, orderings, exhaustive, pp_sum, nullptr);
+    else return refine_cf<IT, K>(r, m, orderings, exhaustive, pp_sum);
 }
 
 // EndpointSearch (BC1Encoder.cpp:930-996): the reference's sequential loop
@@ -661,39 +715,40 @@ struct Deferred {
 // EncodeBlock from the 3-colour trials on (BC1Encoder.cpp:305-341): res is the
 // four-colour result after its cluster-fit passes, orig the endpoints before the
 // four-colour refinement. With `d`, a block that needs EndpointSearch stops before it
-// and is returned in *d instead.
-template <int IT>
+// and is returned in *d instead. INL inlines the phase bodies; without SEARCH the caller
+// guarantees p.search_rounds == 0 and no search code is compiled in.
+template <int IT, bool INL = false, bool SEARCH = true>
 __device__ __forceinline__ uint2 encode_tail(const qt_bc1_params &p, int color_mode, int pp_sum, const M &m, R res,
                                              const R &orig, Deferred *d) {
     const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
     const int ls_passes = p.two_ls_passes ? 2 : 1, cf_passes = p.two_cf_passes ? 2 : 1;
     if (res.err > 0 && (color_mode & CM_THREE)) {
         R t = orig;
-        const uint2 se = find_selectors<IT, K_T3>(t.lo, t.hi);
+        const uint2 se = find_selectors_<IT, K_T3, INL>(t.lo, t.hi);
         t.sel = se.x;
         t.err = se.y;
         t.mode = CM_THREE;
-        t = refine_ls<IT, K_T3>(t, m, ls_passes);
+        t = refine_ls_<IT, K_T3, INL>(t, m, ls_passes);
         if (t.err > 0 && use_likely)
-            for (int it = 0; it < cf_passes; it++) t = refine_cf<IT, K_T3>(t, m, p.orderings3, p.exhaustive, pp_sum);
+            for (int it = 0; it < cf_passes; it++) t = refine_cf_<IT, K_T3, INL>(t, m, p.orderings3, p.exhaustive, pp_sum);
         if (t.err < res.err) res = t;
     }
 
     if (res.err > 0 && color_mode == CM_TB && m.has_black && !((m.mx[0] | m.mx[1] | m.mx[2]) < 4)) {
-        const M mnb = metrics(true);
-        const int2 ep = find_endpoints(mnb, EP_PCA, true, (int)p.power_iterations);
+        const M mnb = metrics_<INL>(true);
+        const int2 ep = find_endpoints_<INL>(mnb, EP_PCA, true, (int)p.power_iterations);
         R t = rinit();
         t.lo = ep.x;
         t.hi = ep.y;
-        const uint2 se = find_selectors<IT, K_TB>(t.lo, t.hi);
+        const uint2 se = find_selectors_<IT, K_TB, INL>(t.lo, t.hi);
         t.sel = se.x;
         t.err = se.y;
         t.mode = CM_TB;
-        t = refine_ls<IT, K_TB>(t, mnb, ls_passes);
+        t = refine_ls_<IT, K_TB, INL>(t, mnb, ls_passes);
         if (t.err < res.err) res = t;
     }
 
-    if (res.err > 0 && p.search_rounds > 0) {
+    if (SEARCH && res.err > 0 && p.search_rounds > 0) {
         const int Md = res.mode == CM_THREE ? CM_THREE : (res.mode == CM_TB ? CM_TB : CM_FOUR);
         if (d) {
             d->need = true;
@@ -701,7 +756,8 @@ __device__ __forceinline__ uint2 encode_tail(const qt_bc1_params &p, int color_m
             d->r = res;
             return make_uint2(0u, 0u);
         }
-        res = search_any<IT>(kind_for(Md, Md == CM_FOUR ? p.error_mode : EM_FULL), res, p.search_rounds, pp_sum);
+        if constexpr (SEARCH)
+            res = search_any<IT>(kind_for(Md, Md == CM_FOUR ? p.error_mode : EM_FULL), res, p.search_rounds, pp_sum);
     }
     return write(res);
 }
@@ -710,14 +766,17 @@ __device__ __forceinline__ uint2 encode_tail(const qt_bc1_params &p, int color_m
 // needs EndpointSearch stops before it, and at settings with two four-colour cluster-fit
 // passes a block stops after the first when the second can change its result or when the
 // 3-colour trials follow; either is returned in *d instead.
-template <int IT>
+// Specialised form (k_bc1_fast): K4 >= 0 fixes the four-colour selector kind at compile time
+// (the caller guarantees kind_for(CM_FOUR, p.error_mode) == K4 and, without SEARCH,
+// p.search_rounds == 0); INL inlines every phase body; `d` must then be null.
+template <int IT, int K4 = -1, bool INL = false, bool SEARCH = true>
 __device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_mode, int pp_sum, Deferred *d = nullptr) {
     const uint32_t c0 = px(0);
     bool solid = true;
     for (int i = 1; i < 16; i++) solid &= px(i) == c0;
     if (solid) return write_block_solid<IT>(c0);
 
-    const M m = metrics(false);
+    const M m = metrics_<INL>(false);
     const bool use_likely = p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0;
     bool needs_err = use_likely;
     needs_err |= color_mode == CM_THREE;
@@ -731,22 +790,28 @@ __device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_
 
     R orig = rinit(), res = rinit();
     for (int round = 0; round < ep_passes; round++) {
-        const int2 ep = find_endpoints(m, round == 1 ? EP_BB : p.endpoint_mode, false, (int)p.power_iterations);
+        const int2 ep = find_endpoints_<INL>(m, round == 1 ? EP_BB : p.endpoint_mode, false, (int)p.power_iterations);
         R to = rinit();
         to.lo = ep.x;
         to.hi = ep.y;
         R tr = to;
-        const uint2 se = fs_any<IT>(k4, tr.lo, tr.hi);
+        uint2 se;
+        if constexpr (K4 >= 0) se = find_selectors_<IT, K4, INL>(tr.lo, tr.hi);
+        else se = fs_any<IT>(k4, tr.lo, tr.hi);
         tr.sel = se.x;
         tr.err = se.y;
         tr.mode = CM_FOUR;
-        tr = refine_ls_any<IT>(k4, tr, m, ls_passes);
+        if constexpr (K4 >= 0) tr = refine_ls_<IT, K4, INL>(tr, m, ls_passes);
+        else tr = refine_ls_any<IT>(k4, tr, m, ls_passes);
         if (!needs_err || tr.err < res.err) {
             res = tr;
             orig = to;
         }
     }
-    if (res.err > 0 && use_likely) {
+    if constexpr (K4 >= 0) {
+        if (res.err > 0 && use_likely)
+            for (int it = 0; it < cf_passes; it++) res = refine_cf_<IT, K4, INL>(res, m, p.orderings4, p.exhaustive, pp_sum);
+    } else if (res.err > 0 && use_likely) {
         const int kcf = kind_for(CM_FOUR, p.error_mode);
         if (d && cf_passes == 2) {
             const int start = cf_start_hash(true, res.sel);
@@ -766,7 +831,7 @@ __device__ __forceinline__ uint2 encode_block(const qt_bc1_params &p, int color_
                 res = refine_cf_any<IT>(kcf, res, m, p.orderings4, p.exhaustive, pp_sum);
         }
     }
-    return encode_tail<IT>(p, color_mode, pp_sum, m, res, orig, d);
+    return encode_tail<IT, INL, SEARCH>(p, color_mode, pp_sum, m, res, orig, d);
 }
 
 }  // namespace tpb
@@ -805,6 +870,49 @@ __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_thread(const uint8_t *
         if (bc3) {
 #pragma unroll
             for (int i = 0; i < 16; i++) v[i] = tpb::t_px[i][threadIdx.x];
+            const uint2 a = bc4_block_thread(v, 3);
+            reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
+        } else {
+            reinterpret_cast<uint2 *>(out)[b] = blk;
+        }
+    }
+}
+
+// The same for settings without EndpointSearch (levels 0-12), specialised: the four-colour
+// selector kind K4 fixed at compile time and every phase inlined, so a launch runs one
+// straight-line path with no calls. With `list`, the blocks are list[i] for i < *count;
+// otherwise [b_begin, nblocks).
+template <int IT, int K4>
+__global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_fast(const uint8_t *__restrict__ rgba, int w, int h, int bw,
+                                                                 long b_begin, long nblocks, qt_bc1_params p,
+                                                                 uint8_t *__restrict__ out, int bc3, int aligned,
+                                                                 const uint32_t *__restrict__ list,
+                                                                 const uint32_t *__restrict__ count) {
+    for (int i = threadIdx.x; i < 64; i += blockDim.x) {
+        if (i < 32) s_mid5[i] = c_mid5[i];
+        s_mid6[i] = c_mid6[i];
+    }
+    __syncthreads();
+    const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
+    const bool listed = list != nullptr;
+    const long end = listed ? (long)*count : nblocks;
+    for (long i = (listed ? 0 : b_begin) + (long)blockIdx.x * blockDim.x + threadIdx.x; i < end;
+         i += (long)gridDim.x * blockDim.x) {
+        const long b = listed ? (long)list[i] : i;
+        const int by = (int)(b / bw), bx = (int)(b - (long)by * bw);
+        uint32_t v[16];
+        load_block_thread(rgba, w, h, bx, by, aligned && (bx * 4 + 4 <= w) && (by * 4 + 4 <= h), v);
+        int pp = 0;
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            tpb::t_px[k][threadIdx.x] = v[k];
+            const uint32_t u = v[k] & 0x00FFFFFFu;
+            pp += (int)__dp4a(u, u, 0u);
+        }
+        const uint2 blk = tpb::encode_block<IT, K4, true, false>(p, color_mode, pp);
+        if (bc3) {
+#pragma unroll
+            for (int k = 0; k < 16; k++) v[k] = tpb::t_px[k][threadIdx.x];
             const uint2 a = bc4_block_thread(v, 3);
             reinterpret_cast<uint4 *>(out)[b] = make_uint4(a.x, a.y, blk.x, blk.y);
         } else {

@@ -89,6 +89,9 @@ int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int 
 // Persistent batch kernel: groups pull tiles from tiles[0 .. ctl[1]) through the
 // counter ctl[0] until the queue is empty. grid = CTAs to launch (0 = one wave).
 int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, void *stream);
+// the same with `threads` per CTA (32, 64 or 128; work is claimed per warp, so any of them
+// runs the same tiles); grid <= 0 fills the SMs to the kernel's occupancy at that size
+int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, int threads, void *stream);
 int batch_ctas_per_sm();
 int batch_sms();
 

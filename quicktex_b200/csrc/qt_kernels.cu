@@ -319,11 +319,28 @@ constexpr BC4Magic make_bc4_magic() {
 }
 __device__ const BC4Magic g_bc4_magic = make_bc4_magic();
 
+// Selector packing shared by the BC4 and BC5 encoders. A level q (0..9, see below) indexes
+// the Levels table with one PRMT: a selector nibble 0..7 copies byte q of {kBC4MapHi:kBC4MapLo},
+// and 8 or 9 copies the sign of byte 0 or 1 (map 1 and 7: sign 0), i.e. 0, which is map[7], the
+// selector of every level >= 7. So no clamp and no mask are needed: the other result bytes hold
+// map[0] = 1 (selector nibble 0), a known constant. Selector words are then accumulated with
+// IMAD, acc += word << 3j, and that constant's contribution is subtracted once at the end (the
+// arithmetic is exact modulo 2^32 and the 3-bit fields never overlap).
+constexpr uint32_t kPermOnes = 0x01010100u;  // PRMT result bytes 1..3 for a selector < 16
+template <int N>
+__host__ __device__ constexpr uint32_t perm_garbage(uint32_t word) {  // sum of word << 3j, j < N
+    uint32_t c = 0;
+    for (int j = 0; j < N; j++) c += word << (3 * j);
+    return c;
+}
+
 // BC4Encoder::EncodeBlock (BC4Encoder.cpp:30-71) on channel ch. The reference
 // counts the thresholds delta*(1+2c) - bias (c = 0..6) that 14*value reaches;
 // for min <= value <= max that count is exactly
-// min(7, floor((14*(value - min) + 4 + delta) / (2*delta))), taken here with one
-// multiply-high per texel (equal for every (min, max, value), checked exhaustively).
+// min(7, floor((14*(value - min) + 4 + delta) / (2*delta))), and the division is
+// a multiply-high by g_bc4_magic (exact for numerators below 4096; both facts
+// checked for every (min, max, value)). The level itself, floor(...), is at most 9
+// (delta >= 1), so the PRMT table lookup above takes it unclamped.
 __device__ __forceinline__ uint2 bc4_block_thread(const uint32_t px[16], int ch) {
     const uint32_t sel = 0x4440u | (uint32_t)ch;  // byte ch of the texel, zeros above
     uint32_t v[16];
@@ -338,20 +355,17 @@ __device__ __forceinline__ uint2 bc4_block_thread(const uint32_t px[16], int ch)
     const uint32_t delta = mx - mn;
     const uint32_t M = __ldg(&g_bc4_magic.m[delta]);
     const uint32_t K = 4u + delta - 14u * mn;  // 14*value + K == 14*(value - min) + 4 + delta (mod 2^32)
-    uint32_t lo = 0u, hi = 0u;                 // selector bits 0..31 and 32..47
+    uint32_t a0 = 0u, a1 = 0u;                 // texels 0..9 (30 bits), 10..15 (18 bits)
 #pragma unroll
     for (int i = 0; i < 16; i++) {
-        const uint32_t lvl = min(__umulhi(14u * v[i] + K, M), 7u);
-        const uint32_t s = __byte_perm(kBC4MapLo, kBC4MapHi, lvl) & 7u;
-        if (i < 10) {
-            lo |= s << (3 * i);
-        } else if (i == 10) {
-            lo |= s << 30;
-            hi |= s >> 2;
-        } else {
-            hi |= s << (3 * i - 32);
-        }
+        const uint32_t q = __umulhi(14u * v[i] + K, M);
+        const uint32_t word = __byte_perm(kBC4MapLo, kBC4MapHi, q);  // selector in byte 0
+        if (i < 10) a0 += word << (3 * i);
+        else a1 += word << (3 * (i - 10));
     }
+    a0 -= perm_garbage<10>(kPermOnes);
+    a1 -= perm_garbage<6>(kPermOnes);
+    const uint32_t lo = a0 | (a1 << 30), hi = a1 >> 2;  // selector bits 0..31 and 32..47
     return make_uint2(mx | (mn << 8) | (lo << 16), (lo >> 16) | (hi << 16));
 }
 
@@ -371,7 +385,10 @@ __device__ __forceinline__ uint32_t max_u16x2(uint32_t a, uint32_t b) {
 // min/max per texel covers both channels, and one IMAD forms both numerators
 // 14*value + K: a negative low-half K borrows one from the high half, which its
 // high constant pre-compensates, so each half holds its channel's exact value.
-// Per channel the rest is bc4_block_thread's arithmetic.
+// Both levels then index the Levels table in one PRMT (selector nibbles 0 and 2),
+// which puts channel c0's selector in byte 0 and c1's in byte 2 of one word; five
+// texels' words accumulate into one register (two 15-bit fields, 3 bits per
+// texel), as in bc4_block_thread.
 __device__ __forceinline__ uint4 bc5_block_thread(const uint32_t px[16], int c0, int c1) {
     const uint32_t sel = 0x4040u | (uint32_t)c0 | ((uint32_t)c1 << 8);  // byte c0 -> bits 0..7, byte c1 -> bits 16..23
     uint32_t v[16];
@@ -386,25 +403,24 @@ __device__ __forceinline__ uint4 bc5_block_thread(const uint32_t px[16], int c0,
     const uint32_t M0 = __ldg(&g_bc4_magic.m[d0]), M1 = __ldg(&g_bc4_magic.m[d1]);  // m[0] = 0: solid, fixed below
     const int K0 = 4 + (int)d0 - 14 * (int)mn0, K1 = 4 + (int)d1 - 14 * (int)mn1;
     const uint32_t Kp = ((uint32_t)K0 & 0xFFFFu) + ((uint32_t)(K1 - (K0 < 0 ? 1 : 0)) << 16);
-    uint32_t lo0 = 0u, hi0 = 0u, lo1 = 0u, hi1 = 0u;
+    uint32_t g[4] = {0u, 0u, 0u, 0u};  // texels 0-4, 5-9, 10-14, 15: c0 fields in bits 0..14, c1 in 16..30
 #pragma unroll
     for (int i = 0; i < 16; i++) {
         const uint32_t num = 14u * v[i] + Kp;
-        const uint32_t l0 = min(__umulhi(num & 0xFFFFu, M0), 7u), l1 = min(__umulhi(num >> 16, M1), 7u);
-        const uint32_t s0 = __byte_perm(kBC4MapLo, kBC4MapHi, l0) & 7u, s1 = __byte_perm(kBC4MapLo, kBC4MapHi, l1) & 7u;
-        if (i < 10) {
-            lo0 |= s0 << (3 * i);
-            lo1 |= s1 << (3 * i);
-        } else if (i == 10) {
-            lo0 |= s0 << 30;
-            hi0 |= s0 >> 2;
-            lo1 |= s1 << 30;
-            hi1 |= s1 >> 2;
-        } else {
-            hi0 |= s0 << (3 * i - 32);
-            hi1 |= s1 << (3 * i - 32);
-        }
+        const uint32_t q0 = __umulhi(num & 0xFFFFu, M0), q1 = __umulhi(num >> 16, M1);  // levels 0..9
+        const uint32_t word = __byte_perm(kBC4MapLo, kBC4MapHi, q0 + (q1 << 8));  // selectors in bytes 0, 2
+        g[i / 5] += word << (3 * (i % 5));
     }
+    constexpr uint32_t kOnes2 = 0x01000100u;  // PRMT result bytes 1 and 3 (selector nibbles 1, 3 = 0)
+    g[0] -= perm_garbage<5>(kOnes2);
+    g[1] -= perm_garbage<5>(kOnes2);
+    g[2] -= perm_garbage<5>(kOnes2);
+    g[3] -= perm_garbage<1>(kOnes2);
+    // channel fields: 15 + 15 + 15 + 3 bits -> selector bits 0..31 (lo) and 32..47 (hi)
+    const uint32_t f00 = g[0] & 0xFFFFu, f01 = g[1] & 0xFFFFu, f02 = g[2] & 0xFFFFu, f03 = g[3] & 0xFFFFu;
+    const uint32_t f10 = g[0] >> 16, f11 = g[1] >> 16, f12 = g[2] >> 16, f13 = g[3] >> 16;
+    const uint32_t lo0 = f00 | (f01 << 15) | (f02 << 30), hi0 = (f02 >> 2) | (f03 << 13);
+    const uint32_t lo1 = f10 | (f11 << 15) | (f12 << 30), hi1 = (f12 >> 2) | (f13 << 13);
     const uint32_t mx0 = mn0 + d0, mx1 = mn1 + d1;
     uint4 r;
     r.x = d0 ? (mx0 | (mn0 << 8) | (lo0 << 16)) : (mn0 | (mn0 << 8));  // BC4Block(min) when solid
@@ -728,6 +744,32 @@ static bool cf2_pass(const qt_bc1_params &p) {
     return p.two_cf_passes && (p.exhaustive || p.orderings3 > 0 || p.orderings4 > 0);
 }
 
+// The specialised encoder (k_bc1_fast) for a setting without EndpointSearch: its four-colour
+// selector kind is the error mode (every setting has cluster-fit orderings, so it needs block
+// errors: BC1Encoder.cpp:267-276). With list/count the blocks are the listed ones.
+template <int IT>
+static void launch_fast_it(int g, cudaStream_t s, const uint8_t *rgba, int w, int h, int bw, long b0, long b1,
+                           const qt_bc1_params &p, uint8_t *out, bool bc3, int aligned, const uint32_t *list,
+                           const uint32_t *count) {
+    switch (p.error_mode) {
+        case EM_NONE: k_bc1_fast<IT, K_F4_NONE><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        case EM_FASTER: k_bc1_fast<IT, K_F4_FASTER><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        case EM_CHECK2: k_bc1_fast<IT, K_F4_CHECK2><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        default: k_bc1_fast<IT, K_F4_FULL><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+    }
+}
+
+static void launch_fast(int g, cudaStream_t s, const uint8_t *rgba, int w, int h, int bw, long b0, long b1,
+                        const qt_bc1_params &p, uint8_t *out, bool bc3, int aligned, const uint32_t *list,
+                        const uint32_t *count) {
+    switch (p.interpolator) {
+        case IT_IDEAL: launch_fast_it<IT_IDEAL>(g, s, rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        case IT_ROUND: launch_fast_it<IT_ROUND>(g, s, rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        case IT_NVIDIA: launch_fast_it<IT_NVIDIA>(g, s, rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        default: launch_fast_it<IT_AMD>(g, s, rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+    }
+}
+
 int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
                             long b_begin, long b_end, void *stream) {
     const int bw = (w + 3) / 4;
@@ -737,6 +779,10 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
     {
         const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
         const int g = grid_for(n, tpb::kThreads);
+        if ((n < kSplitMinBlocks || n > 0xFFFFFFFFL) && p.search_rounds == 0) {
+            launch_fast(g, s, rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned, nullptr, nullptr);
+            return (int)cudaGetLastError();
+        }
         if (n < kSplitMinBlocks || n > 0xFFFFFFFFL) {
             switch (p.interpolator) {
                 case IT_IDEAL: k_bc1_thread<IT_IDEAL, false><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned, nullptr, nullptr); break;
@@ -805,6 +851,16 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
 #undef QT_DEFER
             }
             e = cudaGetLastError();
+        } else if (e == cudaSuccess && p.search_rounds == 0) {
+            const int gs = grid_for(n, 256);
+            switch (p.interpolator) {
+                case IT_IDEAL: k_bc1_split<IT_IDEAL><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count); break;
+                case IT_ROUND: k_bc1_split<IT_ROUND><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count); break;
+                case IT_NVIDIA: k_bc1_split<IT_NVIDIA><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count); break;
+                default: k_bc1_split<IT_AMD><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count); break;
+            }
+            launch_fast(g, s, rgba, w, h, bw, 0, 0, p, out, bc3, aligned, list, count);
+            e = cudaGetLastError();
         } else if (e == cudaSuccess) {
             const int gs = grid_for(n, 256);
             switch (p.interpolator) {
@@ -845,16 +901,24 @@ int launch_bc1_encode(const uint8_t *rgba, int w, int h, const qt_bc1_params &p,
 
 int batch_sms() { return num_sms(); }
 
-int batch_ctas_per_sm() {
+static int batch_ctas_per_sm_at(int threads) {
     int n = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch, tpb::kThreads, 0) != cudaSuccess || n <= 0) n = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch, threads, 0) != cudaSuccess || n <= 0) n = 1;
     return n;
 }
 
-int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, void *stream) {
-    if (grid <= 0) grid = num_sms() * batch_ctas_per_sm();
-    k_batch<<<grid, tpb::kThreads, 0, (cudaStream_t)stream>>>(items, tiles, ctl);
+int batch_ctas_per_sm() { return batch_ctas_per_sm_at(tpb::kThreads); }
+
+int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, int threads, void *stream) {
+    // the kernel's shared-memory columns hold tpb::kThreads threads; smaller CTAs use a prefix
+    if (threads != 32 && threads != 64 && threads != tpb::kThreads) return (int)cudaErrorInvalidValue;
+    if (grid <= 0) grid = num_sms() * batch_ctas_per_sm_at(threads);
+    k_batch<<<grid, threads, 0, (cudaStream_t)stream>>>(items, tiles, ctl);
     return (int)cudaGetLastError();
+}
+
+int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, void *stream) {
+    return launch_batch(items, tiles, ctl, grid, tpb::kThreads, stream);
 }
 
 // Grid of one thread per block when it fits (uint32_t indices), else a

@@ -354,6 +354,13 @@ int qt_server_set_grid(qt_server *s, int ctas_per_sm) {
     return QT_OK;
 }
 
+int qt_server_set_threads(qt_server *s, int threads_per_cta) {
+    if (!s) return qtk::set_error(QT_ERR_ARG, "NULL argument");
+    for (Slot &sl : s->slots)
+        if (int rc = qt_batch_set_threads(sl.batch, threads_per_cta)) return rc;
+    return QT_OK;
+}
+
 int qt_server_submit(qt_server *s, const qt_batch_item *items, const uint64_t *tags, size_t n) {
     if (!s || (n && (!items || !tags))) return qtk::set_error(QT_ERR_ARG, "NULL argument");
     for (size_t i = 0; i < n; i++) {

@@ -59,12 +59,13 @@ def _lib():
         L.qt_server_destroy.argtypes = [vp]
         L.qt_server_set_rules.argtypes = [vp, ctypes.POINTER(TileRule), sz]
         L.qt_server_set_grid.argtypes = [vp, ctypes.c_int]
+        L.qt_server_set_threads.argtypes = [vp, ctypes.c_int]
         L.qt_server_submit.argtypes = [vp, ctypes.POINTER(BatchItem), vp, sz]
         L.qt_server_poll.argtypes = [vp, vp, vp, vp, sz, ctypes.c_int64, ctypes.POINTER(sz)]
         L.qt_server_get_stats.argtypes = [vp, ctypes.POINTER(_Stats)]
         L.qt_server_clock.argtypes = []
         L.qt_server_clock.restype = ctypes.c_double
-        for n in ("qt_server_create", "qt_server_destroy", "qt_server_set_rules", "qt_server_set_grid",
+        for n in ("qt_server_create", "qt_server_destroy", "qt_server_set_rules", "qt_server_set_grid", "qt_server_set_threads",
                   "qt_server_submit", "qt_server_poll", "qt_server_get_stats"):
             getattr(L, n).restype = ctypes.c_int
         _sigs_done = True
@@ -157,6 +158,8 @@ class Server:
             for i, r in enumerate(rules):
                 arr[i] = TileRule(r["op"], r["format"], r.get("level", -1), r["tile_blocks"], r["cost_per_block"])
             capi.check(L.qt_server_set_rules(h, arr, len(rules)))
+            if tuning.get("threads_per_cta"):
+                capi.check(L.qt_server_set_threads(h, int(tuning["threads_per_cta"])))
             if tuning.get("ctas_per_sm"):
                 capi.check(L.qt_server_set_grid(h, int(tuning["ctas_per_sm"])))
         # completion times come on CLOCK_MONOTONIC; latencies are measured against time.perf_counter
