@@ -347,6 +347,29 @@ def run_ours(args, world, rank, local):
         e2e_s = reduce_max((time.perf_counter() - t0) / args.steps, world)
         e2e_value = world * blocks_step / e2e_s / 1e6
 
+    # the same through the drop-in Python API: BC1Encoder(level, mode, interpolator).encode(RawTexture),
+    # whose texels live in the RawTexture's own pageable host memory (one step)
+    e2e_dropin = None
+    if not args.no_e2e and world == 1:
+        import quicktex_b200 as qt
+        from quicktex_b200.s3tc.bc1 import BC1Encoder
+        from quicktex_b200.s3tc.interpolator import Interpolator, InterpolatorAMD, InterpolatorNvidia, InterpolatorRound
+
+        tex = qt.RawTexture.frombytes(img.tobytes(), W, H)
+        interps = [Interpolator, InterpolatorRound, InterpolatorNvidia, InterpolatorAMD]
+        mode_enum = {0x04: BC1Encoder.ColorMode.FourColor, 0x03: BC1Encoder.ColorMode.ThreeColor,
+                     0x13: BC1Encoder.ColorMode.ThreeColorBlack}
+        encoders = [BC1Encoder(L, mode_enum[m], interps[it]()) for L, _mn, m, _in, it in SETTINGS]
+        for e in encoders[:3]:
+            e.encode(tex)
+        t0 = time.perf_counter()
+        for e in encoders:
+            e.encode(tex)
+        e2e_dropin = {"value": blocks_step / (time.perf_counter() - t0) / 1e6, "unit": "Mblocks/s",
+                      "path": "BC1Encoder(level, color_mode, interpolator).encode(RawTexture) for the 36 settings: "
+                              "texels in pageable host memory, blocks returned in a new BC1Texture"}
+        del tex
+
     # roofline: algorithmic lane-ops (10 per candidate evaluation) / kernel time
     peaks, peaks_kind = load_peaks()
     with open(os.path.join(ROOT, "tests", "golden", "ce_counts.json")) as f:
@@ -387,6 +410,7 @@ def run_ours(args, world, rank, local):
         "by_level_mblocks_s": {k: v[1] / (v[0] / 1e3) / 1e6 for k, v in by_level.items()},
         "e2e": {"value": e2e_value, "unit": "Mblocks/s", "h2d_bytes_per_step": W * H * 4 * len(SETTINGS),
                 "d2h_bytes_per_step": NB * 8 * len(SETTINGS)},
+        "e2e_dropin": e2e_dropin,
         # per encode call, as the library reports it: the encoder, the split pass (>= 16384 blocks)
         # and, for settings with EndpointSearch on large textures, the search pass
         "gpu_launches": args.steps * sum(capi.bc1_encode_kernels(W, H, p) for p in params),
