@@ -320,13 +320,20 @@ constexpr BC4Magic make_bc4_magic() {
 __device__ const BC4Magic g_bc4_magic = make_bc4_magic();
 
 // Selector packing shared by the BC4 and BC5 encoders. A level q (0..9, see below) indexes
-// the Levels table with one PRMT: a selector nibble 0..7 copies byte q of {kBC4MapHi:kBC4MapLo},
-// and 8 or 9 copies the sign of byte 0 or 1 (map 1 and 7: sign 0), i.e. 0, which is map[7], the
-// selector of every level >= 7. So no clamp and no mask are needed: the other result bytes hold
-// map[0] = 1 (selector nibble 0), a known constant. Selector words are then accumulated with
-// IMAD, acc += word << 3j, and that constant's contribution is subtracted once at the end (the
-// arithmetic is exact modulo 2^32 and the 3-bit fields never overlap).
-constexpr uint32_t kPermOnes = 0x01010100u;  // PRMT result bytes 1..3 for a selector < 16
+// the Levels table with one PTX prmt.b32: a selector nibble 0..7 copies byte q of
+// {kBC4MapHi:kBC4MapLo}, and 8 or 9 copies the sign of byte 0 or 1 (map 1 and 7: sign 0), i.e. 0,
+// which is map[7], the selector of every level >= 7. So no clamp and no mask are needed: the
+// other result bytes hold map[0] = 1 (selector nibble 0), a known constant. Selector words are then
+// accumulated with IMAD, acc += word << 3j, and that constant's contribution is subtracted once at
+// the end (the arithmetic is exact modulo 2^32 and the 3-bit fields never overlap).
+// (CUDA's __byte_perm takes only the low 3 bits of each nibble, so it would map 8 and 9 to
+// map[0] and map[1]; the lookup needs the PTX instruction's sign-replicate mode.)
+__device__ __forceinline__ uint32_t prmt_levels(uint32_t selector) {
+    uint32_t d;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(d) : "r"(kBC4MapLo), "r"(kBC4MapHi), "r"(selector));
+    return d;
+}
+constexpr uint32_t kPermOnes = 0x01010100u;  // prmt result bytes 1..3 for a selector < 16
 template <int N>
 __host__ __device__ constexpr uint32_t perm_garbage(uint32_t word) {  // sum of word << 3j, j < N
     uint32_t c = 0;
@@ -340,7 +347,7 @@ __host__ __device__ constexpr uint32_t perm_garbage(uint32_t word) {  // sum of 
 // min(7, floor((14*(value - min) + 4 + delta) / (2*delta))), and the division is
 // a multiply-high by g_bc4_magic (exact for numerators below 4096; both facts
 // checked for every (min, max, value)). The level itself, floor(...), is at most 9
-// (delta >= 1), so the PRMT table lookup above takes it unclamped.
+// (delta >= 1), so the prmt table lookup above takes it unclamped.
 __device__ __forceinline__ uint2 bc4_block_thread(const uint32_t px[16], int ch) {
     const uint32_t sel = 0x4440u | (uint32_t)ch;  // byte ch of the texel, zeros above
     uint32_t v[16];
@@ -359,7 +366,7 @@ __device__ __forceinline__ uint2 bc4_block_thread(const uint32_t px[16], int ch)
 #pragma unroll
     for (int i = 0; i < 16; i++) {
         const uint32_t q = __umulhi(14u * v[i] + K, M);
-        const uint32_t word = __byte_perm(kBC4MapLo, kBC4MapHi, q);  // selector in byte 0
+        const uint32_t word = prmt_levels(q);  // selector in byte 0
         if (i < 10) a0 += word << (3 * i);
         else a1 += word << (3 * (i - 10));
     }
@@ -385,7 +392,7 @@ __device__ __forceinline__ uint32_t max_u16x2(uint32_t a, uint32_t b) {
 // min/max per texel covers both channels, and one IMAD forms both numerators
 // 14*value + K: a negative low-half K borrows one from the high half, which its
 // high constant pre-compensates, so each half holds its channel's exact value.
-// Both levels then index the Levels table in one PRMT (selector nibbles 0 and 2),
+// Both levels then index the Levels table in one prmt (selector nibbles 0 and 2),
 // which puts channel c0's selector in byte 0 and c1's in byte 2 of one word; five
 // texels' words accumulate into one register (two 15-bit fields, 3 bits per
 // texel), as in bc4_block_thread.
@@ -408,10 +415,10 @@ __device__ __forceinline__ uint4 bc5_block_thread(const uint32_t px[16], int c0,
     for (int i = 0; i < 16; i++) {
         const uint32_t num = 14u * v[i] + Kp;
         const uint32_t q0 = __umulhi(num & 0xFFFFu, M0), q1 = __umulhi(num >> 16, M1);  // levels 0..9
-        const uint32_t word = __byte_perm(kBC4MapLo, kBC4MapHi, q0 + (q1 << 8));  // selectors in bytes 0, 2
+        const uint32_t word = prmt_levels(q0 + (q1 << 8));  // selectors in bytes 0, 2
         g[i / 5] += word << (3 * (i % 5));
     }
-    constexpr uint32_t kOnes2 = 0x01000100u;  // PRMT result bytes 1 and 3 (selector nibbles 1, 3 = 0)
+    constexpr uint32_t kOnes2 = 0x01000100u;  // prmt result bytes 1 and 3 (selector nibbles 1, 3 = 0)
     g[0] -= perm_garbage<5>(kOnes2);
     g[1] -= perm_garbage<5>(kOnes2);
     g[2] -= perm_garbage<5>(kOnes2);

@@ -3,8 +3,9 @@
 bc4_block_thread / bc5_block_thread (quicktex_b200/csrc/qt_kernels.cu) find each
 texel's level as floor((14*(v - min) + 4 + delta) / (2*delta)) with a
 multiply-high by a magic number, look the selector up in the Levels table
-{1,7,6,5,4,3,2,0} (BC4Encoder.cpp:45-64) with one PRMT and no clamp (levels 8
-and 9 hit PRMT's sign-replicate mode, which yields 0 = map[7]), and accumulate
+{1,7,6,5,4,3,2,0} (BC4Encoder.cpp:45-64) with one PTX prmt.b32 and no clamp
+(levels 8 and 9 hit prmt's sign-replicate mode, which yields 0 = map[7]; CUDA's
+__byte_perm masks selectors to 3 bits and has no such mode), and accumulate
 the PRMT words with integer adds, subtracting the table's constant filler bytes
 once at the end. Here that arithmetic is emulated bit for bit and compared with
 the reference's own rule: the count of thresholds delta*(2c+1) - (4 - 14*min)
@@ -38,7 +39,8 @@ def umulhi(a, b):
 
 
 def prmt(x: int, y: int, s):
-    """PTX prmt.b32 (default mode) with constant x, y and selector array s."""
+    """PTX prmt.b32 (default mode: 4-bit selectors, bit 3 replicates the selected byte's sign)
+    with constant x, y and selector array s."""
     src = np.array([(x >> (8 * i)) & 0xFF for i in range(4)] + [(y >> (8 * i)) & 0xFF for i in range(4)], np.int64)
     out = np.zeros_like(s)
     for i in range(4):
