@@ -9,14 +9,19 @@
 // of the cluster-fit orderings are computed here with the reference's
 // operation order (OrderTable.h:65-83) and must match it bit for bit.
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstdarg>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <deque>
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -264,6 +269,189 @@ int finish_launch(int rc, const char *what) {
     return rc ? cuda_err((cudaError_t)rc, what) : QT_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Pageable host buffers. A copy from or to pageable memory goes through the CUDA
+// driver's own small pinned buffer, filled by one CPU thread, and cudaMemcpyAsync
+// returns only when it is done (about a quarter of the pinned-memory rate). The
+// drop-in API hands over RawTexture / BlockTexture storage, a pageable std::vector,
+// so the host-buffer entry points stage pageable buffers themselves: a ring of
+// pinned chunks per host thread and device, filled and drained by a small pool of
+// copy threads. The CPU copy of one chunk then overlaps the DMA of the others.
+// ---------------------------------------------------------------------------
+class CopyPool {
+   public:
+    static CopyPool &get() {
+        static CopyPool *p = new CopyPool();  // never destroyed: its threads live until exit
+        return *p;
+    }
+    // memcpy split over the pool's threads and the caller; returns when all of it is done
+    void copy(void *dst, const void *src, size_t n) {
+        const size_t kPiece = size_t(1) << 20;
+        const size_t pieces = std::min<size_t>(workers_ + 1, std::max<size_t>(1, n / kPiece));
+        if (pieces <= 1) {
+            std::memcpy(dst, src, n);
+            return;
+        }
+        const size_t step = (n / pieces + 63) & ~size_t(63);
+        std::atomic<size_t> left(pieces - 1);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            for (size_t k = 1; k < pieces; k++) {
+                const size_t off = k * step;
+                tasks_.push_back({static_cast<uint8_t *>(dst) + off, static_cast<const uint8_t *>(src) + off,
+                                  off < n ? std::min(step, n - off) : 0, &left});
+            }
+        }
+        cv_.notify_all();
+        std::memcpy(dst, src, std::min(step, n));
+        while (left.load(std::memory_order_acquire) != 0) std::this_thread::yield();
+    }
+
+   private:
+    struct Task {
+        uint8_t *dst;
+        const uint8_t *src;
+        size_t n;
+        std::atomic<size_t> *left;
+    };
+    CopyPool() {
+        const unsigned hw = std::thread::hardware_concurrency();
+        workers_ = std::min<unsigned>(7, hw > 2 ? hw / 2 - 1 : 1);
+        for (unsigned i = 0; i < workers_; i++) std::thread([this] { run(); }).detach();
+    }
+    void run() {
+        for (;;) {
+            Task t;
+            {
+                std::unique_lock<std::mutex> lk(mu_);
+                cv_.wait(lk, [this] { return !tasks_.empty(); });
+                t = tasks_.front();
+                tasks_.pop_front();
+            }
+            if (t.n) std::memcpy(t.dst, t.src, t.n);
+            t.left->fetch_sub(1, std::memory_order_release);
+        }
+    }
+    unsigned workers_ = 1;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<Task> tasks_;
+};
+
+bool is_pageable(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return true;
+    }
+    return a.type == cudaMemoryTypeUnregistered;
+}
+
+// Ring of pinned chunks of one host thread on one device. A chunk is reused only after the
+// async copy through it finished (its event); a chunk that received device data is copied to
+// its host destination then, or by flush().
+struct Stage {
+    static constexpr size_t kChunk = size_t(8) << 20;
+    static constexpr int kChunks = 4;
+    uint8_t *buf = nullptr;
+    cudaEvent_t ev[kChunks] = {};
+    bool busy[kChunks] = {};
+    uint8_t *pend_dst[kChunks] = {};
+    size_t pend_len[kChunks] = {};
+    int next = 0;
+
+    int init() {
+        if (buf) return QT_OK;
+        cudaError_t e = cudaHostAlloc((void **)&buf, kChunk * kChunks, cudaHostAllocDefault);
+        for (int j = 0; j < kChunks && e == cudaSuccess; j++) e = cudaEventCreateWithFlags(&ev[j], cudaEventDisableTiming);
+        if (e != cudaSuccess) {
+            buf = nullptr;
+            return cuda_err(e, "pinned staging buffer");
+        }
+        return QT_OK;
+    }
+    uint8_t *chunk(int j) { return buf + (size_t)j * kChunk; }
+    int retire(int j) {
+        if (!busy[j]) return QT_OK;
+        const cudaError_t e = cudaEventSynchronize(ev[j]);
+        busy[j] = false;
+        if (e != cudaSuccess) return cuda_err(e, "staged copy");
+        if (pend_len[j]) CopyPool::get().copy(pend_dst[j], chunk(j), pend_len[j]);
+        pend_len[j] = 0;
+        return QT_OK;
+    }
+    int take(int *j) {
+        *j = next;
+        next = (next + 1) % kChunks;
+        return retire(*j);
+    }
+    int upload(void *dev, const uint8_t *host, size_t n, cudaStream_t s) {
+        for (size_t off = 0; off < n; off += kChunk) {
+            const size_t len = std::min(kChunk, n - off);
+            int j, rc;
+            if ((rc = take(&j))) return rc;
+            CopyPool::get().copy(chunk(j), host + off, len);
+            cudaError_t e = cudaMemcpyAsync(static_cast<uint8_t *>(dev) + off, chunk(j), len, cudaMemcpyHostToDevice, s);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[j], s);
+            if (e != cudaSuccess) return cuda_err(e, "host-to-device copy");
+            busy[j] = true;
+        }
+        return QT_OK;
+    }
+    int download(uint8_t *host, const void *dev, size_t n, cudaStream_t s) {
+        for (size_t off = 0; off < n; off += kChunk) {
+            const size_t len = std::min(kChunk, n - off);
+            int j, rc;
+            if ((rc = take(&j))) return rc;
+            cudaError_t e = cudaMemcpyAsync(chunk(j), static_cast<const uint8_t *>(dev) + off, len, cudaMemcpyDeviceToHost, s);
+            if (e == cudaSuccess) e = cudaEventRecord(ev[j], s);
+            if (e != cudaSuccess) return cuda_err(e, "device-to-host copy");
+            busy[j] = true;
+            pend_dst[j] = host + off;
+            pend_len[j] = len;
+        }
+        return QT_OK;
+    }
+    int flush() {  // every chunk's copy done and delivered, oldest first
+        int rc = QT_OK;
+        for (int k = 0; k < kChunks; k++) {
+            const int r = retire((next + k) % kChunks);
+            if (!rc) rc = r;
+        }
+        return rc;
+    }
+};
+
+Stage &thread_stage(int dev) {
+    thread_local Stage stages[kMaxDevices];
+    return stages[dev];
+}
+
+// Host<->device copies of the host-buffer entry points: pinned (or otherwise registered)
+// host memory is copied directly, pageable memory through the thread's stage.
+struct HostXfer {
+    Stage *st = nullptr;  // set when either side is pageable
+    bool in_pageable = false, out_pageable = false;
+    int begin(int dev, const void *host_in, const void *host_out) {
+        in_pageable = is_pageable(host_in);
+        out_pageable = is_pageable(host_out);
+        if (!in_pageable && !out_pageable) return QT_OK;
+        st = &thread_stage(dev);
+        return st->init();
+    }
+    int in(void *dev, const uint8_t *host, size_t n, cudaStream_t s) {
+        if (in_pageable) return st->upload(dev, host, n, s);
+        const cudaError_t e = cudaMemcpyAsync(dev, host, n, cudaMemcpyHostToDevice, s);
+        return e == cudaSuccess ? QT_OK : cuda_err(e, "host-to-device copy");
+    }
+    int out(uint8_t *host, const void *dev, size_t n, cudaStream_t s) {
+        if (out_pageable) return st->download(host, dev, n, s);
+        const cudaError_t e = cudaMemcpyAsync(host, dev, n, cudaMemcpyDeviceToHost, s);
+        return e == cudaSuccess ? QT_OK : cuda_err(e, "device-to-host copy");
+    }
+    int finish() { return st ? st->flush() : QT_OK; }
+};
+
 // host path: H2D, kernel, D2H on this thread's stream; returns when done
 template <typename Launch>
 int run_host(const void *src, size_t src_bytes, void *dst, size_t dst_bytes, bool dst_needs_zero, Launch &&launch,
@@ -274,14 +462,17 @@ int run_host(const void *src, size_t src_bytes, void *dst, size_t dst_bytes, boo
     DevBuf din, dout;
     if ((rc = acquire(din, dev, src_bytes)) || (rc = acquire(dout, dev, dst_bytes))) return rc;
     cudaStream_t s = thread_stream(dev);
-    cudaError_t e = cudaMemcpyAsync(din.ptr, src, src_bytes, cudaMemcpyHostToDevice, s);
-    if (e != cudaSuccess) return cuda_err(e, "host-to-device copy");
-    if (dst_needs_zero && (e = cudaMemsetAsync(dout.ptr, 0, dst_bytes, s)) != cudaSuccess) return cuda_err(e, "memset");
-    rc = launch(din.ptr, dout.ptr, (void *)s);
-    if (rc) return cuda_err((cudaError_t)rc, what);
-    e = cudaMemcpyAsync(dst, dout.ptr, dst_bytes, cudaMemcpyDeviceToHost, s);
-    if (e != cudaSuccess) return cuda_err(e, "device-to-host copy");
+    HostXfer x;
+    if ((rc = x.begin(dev, src, dst))) return rc;
+    rc = x.in(din.ptr, static_cast<const uint8_t *>(src), src_bytes, s);
+    cudaError_t e = cudaSuccess;
+    if (!rc && dst_needs_zero && (e = cudaMemsetAsync(dout.ptr, 0, dst_bytes, s)) != cudaSuccess) rc = cuda_err(e, "memset");
+    if (!rc && (rc = launch(din.ptr, dout.ptr, (void *)s))) rc = cuda_err((cudaError_t)rc, what);
+    if (!rc) rc = x.out(static_cast<uint8_t *>(dst), dout.ptr, dst_bytes, s);
+    const int frc = x.finish();
     e = cudaStreamSynchronize(s);
+    if (rc) return rc;
+    if (frc) return frc;
     if (e != cudaSuccess) return cuda_err(e, what);
     return QT_OK;
 }
@@ -339,6 +530,8 @@ int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h,
     cudaEvent_t first_up = thread_event(dev);
     uint8_t *di = static_cast<uint8_t *>(din.ptr), *dout_p = static_cast<uint8_t *>(dout.ptr);
     cudaError_t e = cudaSuccess;
+    HostXfer x;
+    if ((rc = x.begin(dev, src, dst))) return rc;
     // uploads and kernels
     for (int k = 0; k < nbands && e == cudaSuccess && rc == QT_OK; k++) {
         const int r0 = cut[k], r1 = cut[k + 1];
@@ -351,8 +544,9 @@ int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h,
             off = (size_t)r0 * block_row;
             len = (size_t)(r1 - r0) * block_row;
         }
-        e = cudaMemcpyAsync(di + off, src + off, len, cudaMemcpyHostToDevice, s);
-        if (e == cudaSuccess && k == 0) e = cudaEventRecord(first_up, s);
+        rc = x.in(di + off, src + off, len, s);
+        if (rc) break;
+        if (k == 0) e = cudaEventRecord(first_up, s);
         if (e == cudaSuccess && encode && ragged && k == nbands - 1 && (k & 1)) e = cudaStreamWaitEvent(s, first_up, 0);
         if (e == cudaSuccess) {
             const int lrc = launch(din.ptr, dout.ptr, (long)r0 * bw, (long)r1 * bw, (void *)s);
@@ -370,10 +564,12 @@ int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h,
             off = (size_t)(4 * r0) * texel_row;
             len = (size_t)(std::min(h, 4 * r1) - 4 * r0) * texel_row;
         }
-        e = cudaMemcpyAsync(dst + off, dout_p + off, len, cudaMemcpyDeviceToHost, st[k & 1]);
+        rc = x.out(dst + off, dout_p + off, len, st[k & 1]);
     }
+    const int frc = x.finish();
     const cudaError_t e0 = cudaStreamSynchronize(st[0]), e1 = cudaStreamSynchronize(st[1]);
     if (rc) return rc;
+    if (frc) return frc;
     if (e != cudaSuccess) return cuda_err(e, what);
     if (e0 != cudaSuccess) return cuda_err(e0, what);
     if (e1 != cudaSuccess) return cuda_err(e1, what);
