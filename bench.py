@@ -80,6 +80,23 @@ CONFIG = {
 # kernels = 92,676,096 B for 262,144 blocks). Each pass re-reads the block's texels.
 BC1_DRAM_BYTES_PER_BLOCK = (16792832 + 18021376 + 2560 + 20707584 + 21565952 + 15585792) / 262144
 
+# Warp instructions executed per block by one encode call of each setting: smsp__inst_executed.sum
+# over the call's kernels divided by the texture's blocks, from the ncu launch list of the bench's
+# own per-setting pass at 2048x2048 (a crop of the same texture, the same kernels: split + fast
+# encoder, or the five-kernel level-18 pipeline), summarised in
+# profiles/bench_2048sq_inst_per_block.md.
+WARP_INST_PER_BLOCK: dict = {
+    "L0_four_ideal": 133.6, "L0_four_round": 134.3, "L0_four_nvidia": 134.2, "L0_four_amd": 133.6,
+    "L0_three_ideal": 212.5, "L0_three_round": 213.3, "L0_three_nvidia": 212.1, "L0_three_amd": 212.6,
+    "L0_three_black_ideal": 212.6, "L0_three_black_round": 213.3, "L0_three_black_nvidia": 212.2, "L0_three_black_amd": 212.6,
+    "L10_four_ideal": 462.9, "L10_four_round": 467.0, "L10_four_nvidia": 477.5, "L10_four_amd": 461.6,
+    "L10_three_ideal": 629.3, "L10_three_round": 633.3, "L10_three_nvidia": 647.5, "L10_three_amd": 628.0,
+    "L10_three_black_ideal": 629.3, "L10_three_black_round": 633.4, "L10_three_black_nvidia": 647.5, "L10_three_black_amd": 628.0,
+    "L18_four_ideal": 3304.3, "L18_four_round": 3348.1, "L18_four_nvidia": 3757.7, "L18_four_amd": 3309.0,
+    "L18_three_ideal": 4033.7, "L18_three_round": 4078.9, "L18_three_nvidia": 4613.3, "L18_three_amd": 4039.3,
+    "L18_three_black_ideal": 4033.8, "L18_three_black_round": 4080.0, "L18_three_black_nvidia": 4617.5, "L18_three_black_amd": 4039.8,
+}
+
 
 def measure_hbm_paths(dev, stream, side: int = 16384, reps: int = 5):
     """The bandwidth-bound kernels on side^2 textures (16384^2 = 1 GiB of texels, far larger
@@ -271,6 +288,36 @@ def run_reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def roofline_line(issue, achieved_exec, achieved_ref, peak_tops, sms, peaks_kind) -> dict:
+    """The sweep's roofline object. Bound: CUDA-core instruction issue (the BC1 encoder is neither
+    HBM- nor tensor-bound: even level 0 moves 72 B per ~4.6k thread instructions). Primary figure:
+    warp instructions issued per second (per-block counts from ncu x blocks / CUDA-event time)
+    over SMs x 4 schedulers x clock, when the counts are present. Beside it, the algorithmic work
+    model: 10 lane-ops per oracle-counted candidate evaluation over SMs x 128 lanes x clock (a
+    work count, not an issue fraction: the kernels spend ~3 instructions per candidate evaluation,
+    so it can pass 1.0 at level 18)."""
+    work = {
+        "achieved": achieved_exec, "peak": peak_tops, "unit": "Tlane-op/s", "frac": achieved_exec / peak_tops,
+        "work": "10 lane-ops x oracle-counted candidate evaluations per block, less those in second "
+                "cluster-fit passes that repeat the first pass's trials (skipped here with identical output)",
+        "achieved_reference_work": achieved_ref, "frac_reference_work": achieved_ref / peak_tops,
+        "peak_source": f"{sms} SMs x 128 lanes x sm_max_mhz ({peaks_kind})",
+    }
+    line = {"bound": "issue", "traffic": BC1_DRAM_BYTES_PER_BLOCK * NB,
+            "traffic_source": "ncu dram bytes of the five kernels of one 2048^2 level-18 call, per block, "
+                              "times this texture's blocks",
+            "kernel": "BC1 encode call: qtk::k_bc1_split, then qtk::k_bc1_fast for settings without "
+                      "EndpointSearch, or qtk::k_bc1_defer + qtk::k_bc1_cf2 + qtk::k_bc1_search + qtk::k_bc1_finish",
+            "work_model": work}
+    if issue:
+        line.update({k: issue[k] for k in ("achieved", "peak", "unit", "frac", "by_level_frac", "source")})
+        line["peak_source"] = f"{sms} SMs x 4 schedulers x sm_max_mhz ({peaks_kind})"
+    else:
+        line.update({"achieved": achieved_exec, "peak": peak_tops, "unit": "Tlane-op/s",
+                     "frac": achieved_exec / peak_tops, "source": "work model (instruction counts not measured)"})
+    return line
+
+
 def run_ours(args, world, rank, local):
     import torch
 
@@ -383,6 +430,22 @@ def run_ours(args, world, rank, local):
     peak_tops = sms * 128 * peaks.get("sm_max_mhz", 1965.0) * 1e6 / 1e12
     achieved = ops / (sum(per) / 1e3) / 1e12
     achieved_exec = ops_exec / (sum(per) / 1e3) / 1e12
+    # the counter-based issue roofline: warp instructions issued per second over the SMs'
+    # 4 schedulers x clock (one warp instruction per scheduler per cycle)
+    issue = None
+    if all(f"L{L}_{mn}_{iname}" in WARP_INST_PER_BLOCK for L, mn, _m, iname, _it in SETTINGS):
+        peak_wi = sms * 4 * peaks.get("sm_max_mhz", 1965.0) * 1e6
+        cls = {}
+        for (L, mn, _m, iname, _it), t in zip(SETTINGS, per):
+            c = cls.setdefault(f"L{L}", [0.0, 0.0])
+            c[0] += WARP_INST_PER_BLOCK[f"L{L}_{mn}_{iname}"] * NB
+            c[1] += t / 1e3
+        tot_i, tot_t = sum(c[0] for c in cls.values()), sum(c[1] for c in cls.values())
+        issue = {"achieved": tot_i / tot_t / 1e9, "peak": peak_wi / 1e9, "unit": "Gwarp-inst/s",
+                 "frac": tot_i / tot_t / peak_wi,
+                 "by_level_frac": {k: v[0] / v[1] / peak_wi for k, v in cls.items()},
+                 "source": "warp instructions per block per setting (ncu smsp__inst_executed.sum at 2048^2) x this "
+                           "texture's blocks / CUDA-event kernel time; peak = SMs x 4 schedulers x sm_max_mhz"}
     by_level = {}
     for (L, _mn, _m, _in, _it), t in zip(SETTINGS, per):
         by_level.setdefault(f"L{L}", [0.0, 0])
@@ -392,21 +455,7 @@ def run_ours(args, world, rank, local):
         "metric": METRIC, "value": value, "unit": "Mblocks/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "u8", "data": "synthetic (seeded PCG64 block mix; no public corpus exists)", "config": CONFIG,
-        "roofline": {
-            "bound": "fp32_issue", "achieved": achieved_exec, "peak": peak_tops, "unit": "Tlane-op/s",
-            "frac": achieved_exec / peak_tops, "traffic": BC1_DRAM_BYTES_PER_BLOCK * NB,
-            "traffic_source": "ncu dram bytes of the five kernels of one 2048^2 level-18 call, per block, "
-                              "times this texture's blocks",
-            "kernel": "BC1 encode call: qtk::k_bc1_split, then qtk::k_bc1_thread, or qtk::k_bc1_defer (+ "
-                      "qtk::k_bc1_cf2) + qtk::k_bc1_search + qtk::k_bc1_finish for settings with EndpointSearch "
-                      "(all settings)",
-            "work": "10 lane-ops x oracle-counted candidate evaluations per block, less those in second "
-                    "cluster-fit passes that repeat the first pass's trials (skipped here with identical output)",
-            "achieved_reference_work": achieved, "frac_reference_work": achieved / peak_tops,
-            "reference_work": "10 lane-ops x all of the reference's candidate evaluations per block, the skipped "
-                              "repeated passes included",
-            "peak_source": f"{sms} SMs x 128 lanes x sm_max_mhz ({peaks_kind})",
-        },
+        "roofline": roofline_line(issue, achieved_exec, achieved, peak_tops, sms, peaks_kind),
         "by_level_mblocks_s": {k: v[1] / (v[0] / 1e3) / 1e6 for k, v in by_level.items()},
         "e2e": {"value": e2e_value, "unit": "Mblocks/s", "h2d_bytes_per_step": W * H * 4 * len(SETTINGS),
                 "d2h_bytes_per_step": NB * 8 * len(SETTINGS)},
