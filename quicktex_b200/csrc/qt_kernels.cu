@@ -438,9 +438,11 @@ __device__ __forceinline__ uint4 bc5_block_thread(const uint32_t px[16], int c0,
 }
 
 // One thread per block. Idx is uint32_t whenever the block count and the grid fit
-// 31 bits (the common case: no 64-bit division per block), else uint64_t.
+// 31 bits (the common case: no 64-bit division per block), else uint64_t. BC5 is held to
+// 40 registers (6 CTAs of 256 threads per SM instead of 5 at its natural 44): its loads
+// need the extra warps in flight (measured 0.83 -> 0.88 of HBM at 16384^2, bit-identical).
 template <bool BC5, typename Idx>
-__global__ void __launch_bounds__(256) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, Idx bw, Idx b_begin,
+__global__ void __launch_bounds__(256, BC5 ? 6 : 4) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, Idx bw, Idx b_begin,
                                                     Idx nblocks, int c0, int c1, int aligned, uint8_t *__restrict__ out) {
     for (Idx b = b_begin + (Idx)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (Idx)gridDim.x * blockDim.x) {
         const int by = (int)(b / bw), bx = (int)(b - (Idx)by * bw);
