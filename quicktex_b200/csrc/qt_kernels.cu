@@ -73,8 +73,6 @@ constexpr int EM_NONE = 0, EM_FASTER = 1, EM_CHECK2 = 2, EM_FULL = 3;
 constexpr int EP_LS = 0, EP_BB = 1, EP_BBINT = 2, EP_PCA = 3;
 constexpr int IT_IDEAL = 0, IT_ROUND = 1, IT_NVIDIA = 2, IT_AMD = 3;
 
-// BC4 selector for each threshold count (BC4Encoder.cpp:46 Levels {1,7,6,5,4,3,2,0}), 3 bits each
-constexpr uint32_t kBC4Levels = 1u | (7u << 3) | (6u << 6) | (5u << 9) | (4u << 12) | (3u << 15) | (2u << 18) | (0u << 21);
 
 // ---------------------------------------------------------------------------
 // scalar helpers (util.h:110-154, Color.cpp)
@@ -441,8 +439,10 @@ __device__ __forceinline__ uint4 bc5_block_thread(const uint32_t px[16], int c0,
 // 31 bits (the common case: no 64-bit division per block), else uint64_t. BC5 is held to
 // 40 registers (6 CTAs of 256 threads per SM instead of 5 at its natural 44): its loads
 // need the extra warps in flight (measured 0.83 -> 0.88 of HBM at 16384^2, bit-identical).
+// BC4 gives no minimum (0), where the compiler also settles at 40 registers; an explicit
+// minimum of 1 to 4 CTAs lets it take 52-56 and costs BC4 a tenth of its bandwidth.
 template <bool BC5, typename Idx>
-__global__ void __launch_bounds__(256, BC5 ? 6 : 4) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, Idx bw, Idx b_begin,
+__global__ void __launch_bounds__(256, BC5 ? 6 : 0) k_bc4_encode(const uint8_t *__restrict__ rgba, int w, int h, Idx bw, Idx b_begin,
                                                     Idx nblocks, int c0, int c1, int aligned, uint8_t *__restrict__ out) {
     for (Idx b = b_begin + (Idx)blockIdx.x * blockDim.x + threadIdx.x; b < nblocks; b += (Idx)gridDim.x * blockDim.x) {
         const int by = (int)(b / bw), bx = (int)(b - (Idx)by * bw);
