@@ -286,7 +286,7 @@ class CopyPool {
     }
     // memcpy split over the pool's threads and the caller; returns when all of it is done
     void copy(void *dst, const void *src, size_t n) {
-        const size_t kPiece = size_t(1) << 20;
+        const size_t kPiece = size_t(2) << 20;
         const size_t pieces = std::min<size_t>(workers_ + 1, std::max<size_t>(1, n / kPiece));
         if (pieces <= 1) {
             std::memcpy(dst, src, n);
@@ -301,6 +301,7 @@ class CopyPool {
                 tasks_.push_back({static_cast<uint8_t *>(dst) + off, static_cast<const uint8_t *>(src) + off,
                                   off < n ? std::min(step, n - off) : 0, &left});
             }
+            pending_.store(tasks_.size(), std::memory_order_release);
         }
         cv_.notify_all();
         std::memcpy(dst, src, std::min(step, n));
@@ -314,19 +315,26 @@ class CopyPool {
         size_t n;
         std::atomic<size_t> *left;
     };
+    // Host memcpy scales to ~12 threads on the 16-core GPU hosts measured (14 GB/s with one,
+    // 48 with 8, 60 with 12); the pool takes three quarters of the cores, the caller one more.
     CopyPool() {
         const unsigned hw = std::thread::hardware_concurrency();
-        workers_ = std::min<unsigned>(7, hw > 2 ? hw / 2 - 1 : 1);
+        workers_ = std::max(1u, std::min(11u, hw * 3 / 4 > 1 ? hw * 3 / 4 - 1 : 1u));
         for (unsigned i = 0; i < workers_; i++) std::thread([this] { run(); }).detach();
     }
     void run() {
         for (;;) {
+            // copies come in bursts (one per staging chunk, a fraction of a millisecond apart):
+            // poll a little before sleeping, so the next chunk's pieces start without a wake-up
+            for (int spin = 0; spin < 2000 && pending_.load(std::memory_order_acquire) == 0; spin++)
+                std::this_thread::yield();
             Task t;
             {
                 std::unique_lock<std::mutex> lk(mu_);
                 cv_.wait(lk, [this] { return !tasks_.empty(); });
                 t = tasks_.front();
                 tasks_.pop_front();
+                pending_.store(tasks_.size(), std::memory_order_release);
             }
             if (t.n) std::memcpy(t.dst, t.src, t.n);
             t.left->fetch_sub(1, std::memory_order_release);
@@ -336,6 +344,7 @@ class CopyPool {
     std::mutex mu_;
     std::condition_variable cv_;
     std::deque<Task> tasks_;
+    std::atomic<size_t> pending_{0};
 };
 
 bool is_pageable(const void *p) {
@@ -351,7 +360,7 @@ bool is_pageable(const void *p) {
 // async copy through it finished (its event); a chunk that received device data is copied to
 // its host destination then, or by flush().
 struct Stage {
-    static constexpr size_t kChunk = size_t(8) << 20;
+    static constexpr size_t kChunk = size_t(16) << 20;
     static constexpr int kChunks = 4;
     uint8_t *buf = nullptr;
     cudaEvent_t ev[kChunks] = {};
