@@ -286,7 +286,7 @@ class CopyPool {
     }
     // memcpy split over the pool's threads and the caller; returns when all of it is done
     void copy(void *dst, const void *src, size_t n) {
-        const size_t kPiece = size_t(2) << 20;
+        const size_t kPiece = size_t(512) << 10;  // a band's chunk (~8 MB) still spreads over 12 threads
         const size_t pieces = std::min<size_t>(workers_ + 1, std::max<size_t>(1, n / kPiece));
         if (pieces <= 1) {
             std::memcpy(dst, src, n);
