@@ -147,35 +147,54 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clock/throttle sampling during the timed region."""
+    """nvidia-smi clock/throttle sampling during the timed region. The sampler starts before the
+    region and the region begins only after its first sample has arrived (nvidia-smi takes a
+    while to start); only samples that arrive inside the region are summarised."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_ms: int = 100):
         self.index = index
+        self.period_ms = period_ms
         self.proc = None
+        self.samples = []  # (arrival time, line)
+
+    def _reader(self):
+        for line in self.proc.stdout:
+            if line.strip():
+                self.samples.append((time.perf_counter(), line))
 
     def __enter__(self):
+        import threading
+
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", str(self.period_ms)],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
+        if self.proc:
+            self.thread = threading.Thread(target=self._reader, daemon=True)
+            self.thread.start()
+            t0 = time.perf_counter()
+            while not self.samples and time.perf_counter() - t0 < 5.0:
+                time.sleep(0.01)
+        self.t_start = time.perf_counter()
         return self
 
     def __exit__(self, *a):
-        self.lines = []
+        self.t_end = time.perf_counter() + self.period_ms / 1e3  # the sample taken as the region ends
         if self.proc:
+            time.sleep(self.period_ms / 1e3 * 1.5)
             self.proc.terminate()
             try:
-                out, _ = self.proc.communicate(timeout=5)
+                self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
-                out, _ = self.proc.communicate()
-            self.lines = [l for l in out.splitlines() if l.strip()]
+            self.thread.join(timeout=5)
+        self.lines = [l for t, l in self.samples if self.t_start <= t <= self.t_end]
 
     def summary(self):
         sm, mx, reasons = [], None, set()
