@@ -20,8 +20,6 @@
 #include <new>
 #include <stdexcept>
 #include <string>
-#include <utility>
-#include <vector>
 #include <tuple>
 #include <vector>
 
@@ -101,16 +99,6 @@ void check(int rc) {
 // ---------------------------------------------------------------------------
 // textures (quicktex/Texture.h)
 // ---------------------------------------------------------------------------
-// Allocator whose construct() without arguments leaves a byte uninitialised, so that a
-// texture the GPU fills completely (an encode or decode result) skips the zero fill.
-template <typename T> struct DefaultInitAlloc : std::allocator<T> {
-    template <typename U> struct rebind { using other = DefaultInitAlloc<U>; };
-    using std::allocator<T>::allocator;
-    template <typename U> void construct(U *p) noexcept { ::new (static_cast<void *>(p)) U; }
-    template <typename U, typename... A> void construct(U *p, A &&...a) { ::new (static_cast<void *>(p)) U(std::forward<A>(a)...); }
-};
-struct Uninit {};  // constructor tag: storage left unset, every byte written by the caller
-
 class Texture {
    public:
     virtual ~Texture() = default;
@@ -127,9 +115,8 @@ class Texture {
         if (h <= 0) throw std::invalid_argument("Texture height must be greater than 0");
         data_.assign(nbytes, 0);
     }
-    Texture(int w, int h, size_t nbytes, Uninit) : w_(w), h_(h) { data_.resize(nbytes); }
     int w_, h_;
-    std::vector<uint8_t, DefaultInitAlloc<uint8_t>> data_;
+    std::vector<uint8_t> data_;
 };
 
 inline size_t checked_area(int w, int h) { return (w > 0 && h > 0) ? (size_t)w * (size_t)h : 0; }
@@ -139,8 +126,6 @@ class RawTexture : public Texture {
     RawTexture(int w, int h) : Texture(w, h, checked_area(w, h) * 4) {
         for (size_t i = 3; i < data_.size(); i += 4) data_[i] = 255;  // Color() = (0, 0, 0, 255)
     }
-    // a decode result: every texel is written by the decoder (valid w, h checked by the caller)
-    RawTexture(int w, int h, Uninit u) : Texture(w, h, checked_area(w, h) * 4, u) {}
     Color GetPixel(int x, int y) const {
         const uint8_t *p = data_.data() + ((size_t)y * w_ + x) * 4;
         return Color{p[0], p[1], p[2], p[3]};
@@ -272,11 +257,6 @@ template <typename B> class BlockTexture : public Texture {
         bw_ = (w + 3) / 4;
         bh_ = (h + 3) / 4;
     }
-    // an encode result: every block is written by the encoder (valid w, h checked by the caller)
-    BlockTexture(int w, int h, Uninit u) : Texture(w, h, (size_t)((w + 3) / 4) * (size_t)((h + 3) / 4) * sizeof(B), u) {
-        bw_ = (w + 3) / 4;
-        bh_ = (h + 3) / 4;
-    }
     int BlocksX() const { return bw_; }
     int BlocksY() const { return bh_; }
     std::tuple<int, int> BlocksXY() const { return {bw_, bh_}; }
@@ -349,7 +329,7 @@ class BC1Encoder {
     }
 
     BC1Texture Encode(const RawTexture &tex) const {
-        BC1Texture out(tex.Width(), tex.Height(), Uninit{});
+        BC1Texture out(tex.Width(), tex.Height());
         const qt_bc1_params p = params();
         int rc;
         {
@@ -395,7 +375,7 @@ class BC1Decoder {
     }
     explicit BC1Decoder(bool write_alpha = false) : BC1Decoder(write_alpha, std::make_shared<Interpolator>()) {}
     RawTexture Decode(const BC1Texture &tex) const {
-        RawTexture out(tex.Width(), tex.Height(), Uninit{});
+        RawTexture out(tex.Width(), tex.Height());
         const int it = interp_->Type(), wa = write_alpha;
         int rc;
         {
@@ -418,7 +398,7 @@ class BC4Encoder {
         if (channel >= 4) throw std::invalid_argument("Channel out of range");
     }
     BC4Texture Encode(const RawTexture &tex) const {
-        BC4Texture out(tex.Width(), tex.Height(), Uninit{});
+        BC4Texture out(tex.Width(), tex.Height());
         int rc;
         {
             py::gil_scoped_release nogil;
@@ -439,7 +419,7 @@ class BC4Decoder {
         if (channel >= 4) throw std::invalid_argument("Channel out of range");
     }
     RawTexture Decode(const BC4Texture &tex) const {
-        RawTexture out(tex.Width(), tex.Height(), Uninit{});
+        RawTexture out(tex.Width(), tex.Height());
         int rc;
         {
             py::gil_scoped_release nogil;
@@ -460,7 +440,7 @@ class BC3Encoder {
         : bc1_(std::make_shared<BC1Encoder>(level, ColorMode::FourColor, std::move(interp))), bc4_(std::make_shared<BC4Encoder>(3)) {}
     explicit BC3Encoder(unsigned level = 5) : BC3Encoder(level, std::make_shared<Interpolator>()) {}
     BC3Texture Encode(const RawTexture &tex) const {
-        BC3Texture out(tex.Width(), tex.Height(), Uninit{});
+        BC3Texture out(tex.Width(), tex.Height());
         const qt_bc1_params p = bc1_->params();
         int rc;
         {
@@ -484,7 +464,7 @@ class BC3Decoder {
         : bc1_(std::make_shared<BC1Decoder>(false, std::move(interp))), bc4_(std::make_shared<BC4Decoder>(3)) {}
     BC3Decoder() : BC3Decoder(std::make_shared<Interpolator>()) {}
     RawTexture Decode(const BC3Texture &tex) const {
-        RawTexture out(tex.Width(), tex.Height(), Uninit{});
+        RawTexture out(tex.Width(), tex.Height());
         const int it = bc1_->GetInterpolator()->Type();
         int rc;
         {
@@ -506,7 +486,7 @@ class BC5Encoder {
    public:
     BC5Encoder(uint8_t c0 = 0, uint8_t c1 = 1) : e0_(std::make_shared<BC4Encoder>(c0)), e1_(std::make_shared<BC4Encoder>(c1)) {}
     BC5Texture Encode(const RawTexture &tex) const {
-        BC5Texture out(tex.Width(), tex.Height(), Uninit{});
+        BC5Texture out(tex.Width(), tex.Height());
         const int c0 = e0_->GetChannel(), c1 = e1_->GetChannel();
         int rc;
         {
@@ -527,7 +507,7 @@ class BC5Decoder {
    public:
     BC5Decoder(uint8_t c0 = 0, uint8_t c1 = 1) : d0_(std::make_shared<BC4Decoder>(c0)), d1_(std::make_shared<BC4Decoder>(c1)) {}
     RawTexture Decode(const BC5Texture &tex) const {
-        RawTexture out(tex.Width(), tex.Height(), Uninit{});
+        RawTexture out(tex.Width(), tex.Height());
         const int c0 = d0_->GetChannel(), c1 = d1_->GetChannel();
         int rc;
         {

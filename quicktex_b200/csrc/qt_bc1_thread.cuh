@@ -609,7 +609,8 @@ __device__ __forceinline__ R refine_cf_body(R r, const M &m, unsigned orderings,
                 qb += t_sb[l3][tid];
             }
             const float fr = (float)(qrg & 0xFFFF), fg = (float)(qrg >> 16), fb = (float)qb;
-            const float q0r = t16r * denom - fr, q0g = t16g * denom - fg, q0b = t16b * denom - fb;
+            // integers below 2^24 (sums of at most 3 x 16 x 255): exact whether fused or not, so one FMA
+            const float q0r = __fmaf_rn(t16r, denom, -fr), q0g = __fmaf_rn(t16g, denom, -fg), q0b = __fmaf_rn(t16b, denom, -fb);
             t.lo = precise_round565_cf(__fadd_rn(__fmul_rn(f.x, q0r), __fmul_rn(f.y, fr)),
                                     __fadd_rn(__fmul_rn(f.x, q0g), __fmul_rn(f.y, fg)),
                                     __fadd_rn(__fmul_rn(f.x, q0b), __fmul_rn(f.y, fb)), s_mid5, s_mid6);
