@@ -369,6 +369,19 @@ struct Stage {
     size_t pend_len[kChunks] = {};
     int next = 0;
 
+    Stage() = default;
+    Stage(const Stage &) = delete;
+    Stage &operator=(const Stage &) = delete;
+    ~Stage() {  // at thread exit: the ring's pinned memory and events go back (errors ignored:
+                // at process exit the runtime may already be gone)
+        if (!buf) return;
+        flush();
+        for (int j = 0; j < kChunks; j++)
+            if (ev[j]) cudaEventDestroy(ev[j]);
+        cudaFreeHost(buf);
+        cudaGetLastError();
+    }
+
     int init() {
         if (buf) return QT_OK;
         cudaError_t e = cudaHostAlloc((void **)&buf, kChunk * kChunks, cudaHostAllocDefault);
