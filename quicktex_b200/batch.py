@@ -268,6 +268,61 @@ class Arena:
         return [ho[o:o + j.out_bytes].tobytes() for j, o in zip(self.jobs, self.out_off)]
 
 
+class PipelinedRun:
+    """An arena's whole round trip (upload, persistent launch, download) cut into ``chunks``
+    consecutive groups of textures of about equal block counts, each with its own queue. Chunk
+    k's upload runs on a copy stream, its launch on a compute stream after that upload, its
+    download on a second copy stream after that launch: the uploads of later chunks and the
+    downloads of earlier ones overlap the launches. ``run()`` returns with every output in the
+    arena's pinned host buffer."""
+
+    def __init__(self, arena: "Arena", chunks: int = 4, device: int = 0, tuning: Optional[dict] = None):
+        import torch
+
+        self.arena = arena
+        n = len(arena.jobs)
+        total = sum(j.nblocks for j in arena.jobs)
+        cuts, acc = [0], 0
+        for k, j in enumerate(arena.jobs):
+            acc += j.nblocks
+            if len(cuts) < chunks and acc >= total * len(cuts) / chunks and k + 1 < n:
+                cuts.append(k + 1)
+        cuts.append(n)
+        self.groups = [(a, b) for a, b in zip(cuts, cuts[1:]) if b > a]
+        items = arena.items()
+        self.items = [items[a:b] for a, b in self.groups]
+        ends_in = arena.in_off[1:] + [arena.in_bytes]
+        ends_out = arena.out_off[1:] + [arena.out_bytes]
+        self.ranges = [(arena.in_off[a], ends_in[b - 1], arena.out_off[a], ends_out[b - 1]) for a, b in self.groups]
+        self.batches = [Batch(device, tuning=tuning) for _ in self.groups]
+        dev = torch.device("cuda", device)
+        self.up, self.comp, self.down = (torch.cuda.Stream(dev) for _ in range(3))
+        self.ev_up = [torch.cuda.Event() for _ in self.groups]
+        self.ev_run = [torch.cuda.Event() for _ in self.groups]
+
+    def run(self) -> None:
+        import torch
+
+        a = self.arena
+        for (i0, i1, _, _), ev in zip(self.ranges, self.ev_up):
+            with torch.cuda.stream(self.up):
+                a.d_in[i0:i1].copy_(a.h_in[i0:i1], non_blocking=True)
+            ev.record(self.up)
+        for b, items, eu, er in zip(self.batches, self.items, self.ev_up, self.ev_run):
+            self.comp.wait_event(eu)
+            b.run(items, self.comp.cuda_stream)
+            er.record(self.comp)
+        for (_, _, o0, o1), er in zip(self.ranges, self.ev_run):
+            self.down.wait_event(er)
+            with torch.cuda.stream(self.down):
+                a.h_out[o0:o1].copy_(a.d_out[o0:o1], non_blocking=True)
+        self.down.synchronize()
+
+    def close(self) -> None:
+        for b in self.batches:
+            b.close()
+
+
 def run_plain_native(items: Sequence[BatchItem], stream: int = 0) -> None:
     """The same work with one single-texture device entry point call per texture,
     issued by the library's own C++ loop (``qt_batch_run_plain``): the launch model

@@ -161,3 +161,21 @@ def test_copy_async_round_trip():
     copy_async(np.array([[h_out.data_ptr(), d.data_ptr(), o]], np.uint64), s.cuda_stream)
     s.synchronize()
     assert np.array_equal(h_out.numpy()[:o], h_in.numpy()[:o])
+
+
+def test_pipelined_round_trip_matches_one_launch():
+    """PipelinedRun (chunks with their own queues, copies overlapping launches) gives every
+    texture's bytes of a single persistent launch, on two runs in a row."""
+    from quicktex_b200.batch import PipelinedRun
+
+    jobs, refs = make_jobs(7, 90)
+    ref_out = run_jobs(jobs)
+    arena = Arena(jobs)
+    pipe = PipelinedRun(arena, chunks=3)
+    try:
+        for _ in range(2):
+            arena.h_out.fill_(0xA5)
+            pipe.run()
+            assert arena.outputs() == ref_out
+    finally:
+        pipe.close()
