@@ -2,8 +2,9 @@
 //
 // Owns the constant tables (built once per process, uploaded once per
 // device), a pooled device allocator for the host-buffer entry points, the
-// thread-local error message, and argument checking with the reference's
-// error semantics.
+// pinned staging of pageable host buffers (a ring per host thread and device,
+// a shared pool of copy threads), the thread-local error message, and argument
+// checking with the reference's error semantics.
 //
 // Compiled as plain C++ on x86-64 with -ffp-contract=off: the factor matrices
 // of the cluster-fit orderings are computed here with the reference's
