@@ -3,12 +3,12 @@
 // One thread encodes one 4x4 block, following BC1Encoder::EncodeBlock
 // (BC1Encoder.cpp:261-342) step by step, with no cross-lane work: no
 // replicated scalar code, no reductions, 32 blocks in flight per warp. The
-// block's texels, cluster-fit sort keys and prefix sums live in shared
-// memory in a transposed layout ([item][thread]), so every per-texel access of
-// a warp is one conflict-free shared load and the loops stay rolled (a small
-// instruction footprint). Float arithmetic uses the same round-to-nearest
-// intrinsics and operation order as the group kernel; every texel sum is an
-// exact integer.
+// block's texels and cluster-fit prefix sums live in shared memory in a
+// transposed layout ([item][thread]), so every per-texel access of a warp is
+// one conflict-free shared load and the loops stay rolled (a small instruction
+// footprint); the sort keys live in registers. Float arithmetic uses explicit
+// round-to-nearest intrinsics in the reference's operation order; every texel
+// sum is an exact integer.
 
 namespace tpb {
 
@@ -97,7 +97,7 @@ __device__ __forceinline__ int check2_threshold(float f, float quarter_den, floa
     return est + (int)!(__fadd_rn(__fmul_rn(__int2float_rn(est), f), 0.5f) >= s);
 }
 
-// FindSelectors<M>(error_mode), BC1Encoder.cpp:679-779; K is one of the group kernel's kinds
+// FindSelectors<M>(error_mode), BC1Encoder.cpp:679-779; K is one of the selector kinds (K_*)
 template <int IT, int K> __device__ __forceinline__ uint2 find_selectors_body(int lo, int hi) {
     const Pal P = make_pal<IT>(lo, hi, kind_three(K));
     // palette colours (internal order) as packed RGB words and their |c|^2: the error of texel p
@@ -691,15 +691,7 @@ template <int IT> __device__ __forceinline__ R search_any(int K, R r, unsigned r
     }
 }
 
-__device__ __forceinline__ uint2 write(const R &r) {
-    Res g;
-    g.lo = r.lo;
-    g.hi = r.hi;
-    g.sel = r.sel;
-    g.mode = r.mode;
-    g.err = r.err;
-    return write_block(g);
-}
+__device__ __forceinline__ uint2 write(const R &r) { return write_block(r.lo, r.hi, r.sel, r.mode); }
 
 // A block whose remaining work runs later in a pass of its own: its result so far.
 // need: EndpointSearch, in k_bc1_search; queue is the search queue of its colour mode

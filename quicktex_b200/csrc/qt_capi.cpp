@@ -258,7 +258,6 @@ int check_channel(int c) {
 int check_interp(int t) {
     return (t < 0 || t > 3) ? set_err(QT_ERR_ARG, "Invalid interpolator type") : QT_OK;
 }
-size_t nblocks(int w, int h) { return (size_t)((w + 3) / 4) * (size_t)((h + 3) / 4); }
 
 int check_ptr(const void *p, size_t align, const char *what) {
     if (!p) return set_err(QT_ERR_ARG, "%s is NULL", what);

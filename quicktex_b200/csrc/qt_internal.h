@@ -86,7 +86,7 @@ int launch_decode_range(int fmt, const uint8_t *blocks, int w, int h, int interp
 int launch_decode(int fmt, const uint8_t *blocks, int w, int h, int interp, int write_alpha, int c0, int c1,
                   uint8_t *rgba, void *stream);
 
-// Persistent batch kernel: groups pull tiles from tiles[0 .. ctl[1]) through the
+// Persistent batch kernel: warps pull tiles from tiles[0 .. ctl[1]) through the
 // counter ctl[0] until the queue is empty. grid = CTAs to launch (0 = one wave).
 int launch_batch(const BatchItemDev *items, const TileDev *tiles, uint32_t *ctl, int grid, void *stream);
 // the same with `threads` per CTA (32, 64 or 128; work is claimed per warp, so any of them

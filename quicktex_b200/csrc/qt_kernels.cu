@@ -94,12 +94,6 @@ __device__ __forceinline__ int epr(int e) { return e >> 11; }
 __device__ __forceinline__ int epg(int e) { return (e >> 5) & 63; }
 __device__ __forceinline__ int epb(int e) { return e & 31; }
 __device__ __forceinline__ int eppack(int r, int g, int b) { return (r << 11) | (g << 5) | b; }
-__device__ __forceinline__ int sel4(int a0, int a1, int a2, int a3, int s) {
-    return s == 0 ? a0 : (s == 1 ? a1 : (s == 2 ? a2 : a3));
-}
-__device__ __forceinline__ float sel4f(float a0, float a1, float a2, float a3, int s) {
-    return s == 0 ? a0 : (s == 1 ? a1 : (s == 2 ? a2 : a3));
-}
 __device__ __forceinline__ unsigned sq3(int a, int b, int c) { return (unsigned)(a * a + b * b + c * c); }
 
 // Color::PreciseRound565 (Color.cpp:66-86)
@@ -190,13 +184,6 @@ template <int IT> __device__ __forceinline__ Pal make_pal(int lo, int hi, bool t
 __shared__ float s_mid5[32], s_mid6[64];
 __shared__ uint16_t s_vox[16];
 
-struct Res {  // EncodeResults (BC1Encoder.h:147-153); endpoints packed 5:6:5
-    int lo, hi;
-    uint32_t sel;  // 16 x 2-bit internal selectors, texel i at bits 2i
-    int mode;
-    uint32_t err;
-};
-
 // Selector-search kinds: the (colour mode, error mode) pairs FindSelectors is
 // ever called with. Three-colour searches are always ErrorMode::Full
 // (BC1Encoder.cpp:313-333, 978-984).
@@ -243,10 +230,12 @@ template <int IT> __device__ __forceinline__ uint2 write_block_solid(uint32_t c)
     return make_uint2((uint32_t)mx | ((uint32_t)mn << 16), mask * 0x01010101u);
 }
 
-__device__ __forceinline__ uint2 write_block(const Res &r) {
-    int ep1 = r.lo, ep0 = r.hi;
+// WriteBlock of an EncodeResults (BC1Encoder.h:147-153): endpoints packed 5:6:5, sel the 16
+// 2-bit internal selectors (texel i at bits 2i), mode its colour mode
+__device__ __forceinline__ uint2 write_block(int lo, int hi, uint32_t sel_in, int mode) {
+    int ep1 = lo, ep0 = hi;
     uint32_t lut;  // 4 x 2-bit entries
-    if (r.mode & CM_FOUR) {
+    if (mode & CM_FOUR) {
         lut = 1 | (3 << 2) | (2 << 4) | (0 << 6);
         if (ep1 > ep0) {
             const int t = ep1; ep1 = ep0; ep0 = t;
@@ -264,7 +253,7 @@ __device__ __forceinline__ uint2 write_block(const Res &r) {
     }
     uint32_t sel = 0;
 #pragma unroll
-    for (int i = 0; i < 16; i++) sel |= ((lut >> (2 * ((r.sel >> (2 * i)) & 3))) & 3) << (2 * i);
+    for (int i = 0; i < 16; i++) sel |= ((lut >> (2 * ((sel_in >> (2 * i)) & 3))) & 3) << (2 * i);
     return make_uint2((uint32_t)ep0 | ((uint32_t)ep1 << 16), sel);
 }
 
