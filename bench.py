@@ -86,15 +86,15 @@ BC1_DRAM_BYTES_PER_BLOCK = (16792832 + 18021376 + 2560 + 20707584 + 21565952 + 1
 # encoder, or the five-kernel level-18 pipeline), summarised in
 # profiles/bench_2048sq_inst_per_block.md.
 WARP_INST_PER_BLOCK: dict = {
-    "L0_four_ideal": 133.6, "L0_four_round": 134.3, "L0_four_nvidia": 134.2, "L0_four_amd": 133.6,
-    "L0_three_ideal": 212.5, "L0_three_round": 213.3, "L0_three_nvidia": 212.1, "L0_three_amd": 212.6,
-    "L0_three_black_ideal": 212.6, "L0_three_black_round": 213.3, "L0_three_black_nvidia": 212.2, "L0_three_black_amd": 212.6,
-    "L10_four_ideal": 462.9, "L10_four_round": 467.0, "L10_four_nvidia": 477.5, "L10_four_amd": 461.6,
-    "L10_three_ideal": 629.3, "L10_three_round": 633.3, "L10_three_nvidia": 647.5, "L10_three_amd": 628.0,
-    "L10_three_black_ideal": 629.3, "L10_three_black_round": 633.4, "L10_three_black_nvidia": 647.5, "L10_three_black_amd": 628.0,
-    "L18_four_ideal": 3304.3, "L18_four_round": 3348.1, "L18_four_nvidia": 3757.7, "L18_four_amd": 3309.0,
-    "L18_three_ideal": 4033.7, "L18_three_round": 4078.9, "L18_three_nvidia": 4613.3, "L18_three_amd": 4039.3,
-    "L18_three_black_ideal": 4033.8, "L18_three_black_round": 4080.0, "L18_three_black_nvidia": 4617.5, "L18_three_black_amd": 4039.8,
+    "L0_four_ideal": 131.7, "L0_four_round": 132.4, "L0_four_nvidia": 132.4, "L0_four_amd": 131.7,
+    "L0_three_ideal": 210.9, "L0_three_round": 211.6, "L0_three_nvidia": 210.5, "L0_three_amd": 210.9,
+    "L0_three_black_ideal": 212.0, "L0_three_black_round": 212.7, "L0_three_black_nvidia": 211.5, "L0_three_black_amd": 211.9,
+    "L10_four_ideal": 458.9, "L10_four_round": 463.0, "L10_four_nvidia": 473.6, "L10_four_amd": 457.5,
+    "L10_three_ideal": 624.4, "L10_three_round": 628.5, "L10_three_nvidia": 643.0, "L10_three_amd": 623.1,
+    "L10_three_black_ideal": 625.7, "L10_three_black_round": 629.8, "L10_three_black_nvidia": 643.2, "L10_three_black_amd": 624.4,
+    "L18_four_ideal": 3280.6, "L18_four_round": 3324.4, "L18_four_nvidia": 3739.8, "L18_four_amd": 3283.1,
+    "L18_three_ideal": 4002.9, "L18_three_round": 4048.4, "L18_three_nvidia": 4588.1, "L18_three_amd": 4009.1,
+    "L18_three_black_ideal": 4003.7, "L18_three_black_round": 4048.1, "L18_three_black_nvidia": 4593.6, "L18_three_black_amd": 4009.2,
 }
 
 

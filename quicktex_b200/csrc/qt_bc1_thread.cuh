@@ -872,12 +872,13 @@ __global__ void __launch_bounds__(tpb::kThreads, 4) k_bc1_thread(const uint8_t *
 }
 
 // The same for settings without EndpointSearch (levels 0-12), specialised: the four-colour
-// selector kind K4 fixed at compile time and every phase inlined, so a launch runs one
-// straight-line path with no calls. With `list`, the blocks are list[i] for i < *count;
-// otherwise [b_begin, nblocks). The Faster-selector instance (levels 5-8) is held to 80
-// registers for 6 CTAs per SM (measured +2-4% at level 5); the others keep 96 registers
-// (5 CTAs), which level 10's three-colour trials need (-4% at 80).
-template <int IT, int K4>
+// selector kind K4 and the colour mode CM (CM_FOUR for BC3) fixed at compile time and every
+// phase inlined, so a launch runs one straight-line path with no calls and no code for the
+// other colour modes' trials. With `list`, the blocks are list[i] for i < *count; otherwise
+// [b_begin, nblocks). The Faster-selector instance (levels 5-8) is held to 80 registers for 6
+// CTAs per SM (measured +2-4% at level 5); the others keep 90-96 registers (5 CTAs), which
+// level 10's three-colour trials need (-4% at 80).
+template <int IT, int K4, int CM>
 __global__ void __launch_bounds__(tpb::kThreads, K4 == K_F4_FASTER ? 6 : 4) k_bc1_fast(const uint8_t *__restrict__ rgba, int w, int h, int bw,
                                                                  long b_begin, long nblocks, qt_bc1_params p,
                                                                  uint8_t *__restrict__ out, int bc3, int aligned,
@@ -888,7 +889,7 @@ __global__ void __launch_bounds__(tpb::kThreads, K4 == K_F4_FASTER ? 6 : 4) k_bc
         s_mid6[i] = c_mid6[i];
     }
     __syncthreads();
-    const int color_mode = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
+    constexpr int color_mode = CM;
     const bool listed = list != nullptr;
     const long end = listed ? (long)*count : nblocks;
     for (long i = (listed ? 0 : b_begin) + (long)blockIdx.x * blockDim.x + threadIdx.x; i < end;

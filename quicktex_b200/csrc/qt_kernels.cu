@@ -789,16 +789,30 @@ static bool cf2_pass(const qt_bc1_params &p) {
 
 // The specialised encoder (k_bc1_fast) for a setting without EndpointSearch: its four-colour
 // selector kind is the error mode (every setting has cluster-fit orderings, so it needs block
-// errors: BC1Encoder.cpp:267-276). With list/count the blocks are the listed ones.
+// errors: BC1Encoder.cpp:267-276); its colour mode is the setting's, four-colour for BC3. With
+// list/count the blocks are the listed ones.
+template <int IT, int K4>
+static void launch_fast_k(int g, cudaStream_t s, const uint8_t *rgba, int w, int h, int bw, long b0, long b1,
+                          const qt_bc1_params &p, uint8_t *out, bool bc3, int aligned, const uint32_t *list,
+                          const uint32_t *count) {
+    const int cm = bc3 ? CM_FOUR : p.color_mode;  // BC3Encoder.h:39-40
+    if (cm == CM_FOUR)
+        k_bc1_fast<IT, K4, CM_FOUR><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count);
+    else if (cm == CM_THREE)
+        k_bc1_fast<IT, K4, CM_THREE><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count);
+    else
+        k_bc1_fast<IT, K4, CM_TB><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count);
+}
+
 template <int IT>
 static void launch_fast_it(int g, cudaStream_t s, const uint8_t *rgba, int w, int h, int bw, long b0, long b1,
                            const qt_bc1_params &p, uint8_t *out, bool bc3, int aligned, const uint32_t *list,
                            const uint32_t *count) {
     switch (p.error_mode) {
-        case EM_NONE: k_bc1_fast<IT, K_F4_NONE><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
-        case EM_FASTER: k_bc1_fast<IT, K_F4_FASTER><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
-        case EM_CHECK2: k_bc1_fast<IT, K_F4_CHECK2><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
-        default: k_bc1_fast<IT, K_F4_FULL><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        case EM_NONE: launch_fast_k<IT, K_F4_NONE>(g, s, rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        case EM_FASTER: launch_fast_k<IT, K_F4_FASTER>(g, s, rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        case EM_CHECK2: launch_fast_k<IT, K_F4_CHECK2>(g, s, rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
+        default: launch_fast_k<IT, K_F4_FULL>(g, s, rgba, w, h, bw, b0, b1, p, out, bc3, aligned, list, count); break;
     }
 }
 
