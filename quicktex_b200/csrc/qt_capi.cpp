@@ -292,7 +292,7 @@ class CopyPool {
             std::memcpy(dst, src, n);
             return;
         }
-        const size_t step = (n / pieces + 63) & ~size_t(63);
+        const size_t step = ((n + pieces - 1) / pieces + 63) & ~size_t(63);  // pieces * step >= n
         std::atomic<size_t> left(pieces - 1);
         {
             std::lock_guard<std::mutex> lk(mu_);

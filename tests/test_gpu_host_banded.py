@@ -108,3 +108,29 @@ def test_banded_search_encode_equals_device(w, h):
         d_out = torch.empty(nb * bsz, dtype=torch.uint8, device="cuda")
         capi.check(dev_fn(capi._vp(d_in.data_ptr()), capi._vp(d_out.data_ptr())))
         assert np.array_equal(out_h, d_out.cpu().numpy()), (name, w, h)
+
+
+@pytest.mark.parametrize("pieces", range(2, 13))
+def test_staged_copy_of_uneven_length(pieces):
+    """A pageable buffer is copied into the pinned staging chunk by up to 12 threads in
+    64-byte-aligned pieces. Lengths of pieces x 512 KiB + 4 bytes split unevenly (the
+    even share is itself a multiple of 64): the last 4 bytes (the texture's last texel
+    on upload, the decoded texture's last texel on download) must arrive too."""
+    import torch
+
+    L = capi.lib()
+    w, h = 1, pieces * 131072 + 1  # w * h * 4 = pieces * 524288 + 4 bytes
+    img = np.random.default_rng(pieces).integers(0, 256, (h, w, 4), dtype=np.uint8)
+    nb = (h + 3) // 4
+    s = capi._vp(torch.cuda.current_stream().cuda_stream)
+    p0 = capi.params_for_level(0)
+    out_h = np.empty(nb * 8, np.uint8)
+    capi.check(L.qt_bc1_encode_host(capi._vp(img.ctypes.data), w, h, ctypes.byref(p0), capi._vp(out_h.ctypes.data)))
+    d_in, d_out = _dev(img), torch.empty(nb * 8, dtype=torch.uint8, device="cuda")
+    capi.check(L.qt_bc1_encode_device(capi._vp(d_in.data_ptr()), w, h, ctypes.byref(p0), capi._vp(d_out.data_ptr()), s))
+    assert np.array_equal(out_h, d_out.cpu().numpy())
+    rgba_h = np.full(w * h * 4, 0xA5, np.uint8)
+    capi.check(L.qt_bc1_decode_host(capi._vp(out_h.ctypes.data), w, h, 0, 1, capi._vp(rgba_h.ctypes.data)))
+    d_rgba = torch.full((w * h * 4,), 0xA5, dtype=torch.uint8, device="cuda")
+    capi.check(L.qt_bc1_decode_device(capi._vp(d_out.data_ptr()), w, h, 0, 1, capi._vp(d_rgba.data_ptr()), s))
+    assert np.array_equal(rgba_h, d_rgba.cpu().numpy())
