@@ -505,10 +505,10 @@ cudaStream_t thread_stream2(int dev) {
     if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
     return streams[dev];
 }
-cudaEvent_t thread_event(int dev) {
-    thread_local cudaEvent_t events[kMaxDevices] = {};
-    if (!events[dev]) cudaEventCreateWithFlags(&events[dev], cudaEventDisableTiming);
-    return events[dev];
+cudaEvent_t thread_event(int dev, int which = 0) {  // which < 3
+    thread_local cudaEvent_t events[kMaxDevices][3] = {};
+    if (!events[dev][which]) cudaEventCreateWithFlags(&events[dev][which], cudaEventDisableTiming);
+    return events[dev][which];
 }
 
 // Host path, pipelined: the texture is cut into bands of block rows (about 8 MB of
@@ -527,16 +527,14 @@ int run_host_banded(const uint8_t *src, uint8_t *dst, bool encode, int w, int h,
     const size_t texel_row = (size_t)w * 4, block_row = (size_t)bw * block_bytes;
     const size_t texel_bytes = texel_row * (size_t)h, blocks_bytes = block_row * (size_t)bh;
     const size_t per_brow = 4 * texel_row + block_row;
-    // ~8 MB of texels per band, and at least min_band_blocks blocks (a launch that large
-    // runs the BC1 EndpointSearch as its own refill pass). Settings that pass min_band_blocks
-    // are compute-heavy: their kernels outlast the copies, so after a first band that starts
-    // the pipeline each band is twice the last, which keeps the uploads ahead of the kernels
-    // with few bands (each band's multi-pass launch ends with a tail of idle lanes).
+    // ~8 MB of texels per band, and at least min_band_blocks blocks: a BC1/BC3 setting with
+    // EndpointSearch passes defer_min_blocks(), so a texture too small for the deferred path
+    // (run_host_bc1_parts takes the larger ones) is not cut into bands that each pay the
+    // search's serial latency.
     const size_t by_bytes = std::max<size_t>(1, (size_t(8) << 20) / per_brow);
     const int rows_first = (int)std::max<size_t>(by_bytes, (size_t)((min_band_blocks + bw - 1) / bw));
     std::vector<int> cut(1, 0);  // band k covers block rows [cut[k], cut[k + 1])
-    for (long rows = rows_first; cut.back() < bh; rows = min_band_blocks > 0 ? 2 * rows : rows)
-        cut.push_back((int)std::min<long>(bh, (long)cut.back() + rows));
+    while (cut.back() < bh) cut.push_back((int)std::min<long>(bh, (long)cut.back() + rows_first));
     const int nbands = (int)cut.size() - 1;
     const bool ragged = (h & 3) != 0;
     const size_t in_bytes = encode ? texel_bytes : blocks_bytes, out_bytes = encode ? blocks_bytes : texel_bytes;
@@ -787,12 +785,76 @@ int qt_bc5_encode_device(const uint8_t *rgba, int w, int h, int c0, int c1, uint
     return finish_launch(qtk::launch_bc4_encode(rgba, w, h, c0, c1, true, blocks, stream), "bc5 encode");
 }
 
+// Host path of a BC1/BC3 encode on the deferred path (EndpointSearch, defer_min_blocks() or more
+// blocks): the texels go up in row bands, ~8 MB first and each band twice the last, on two
+// streams in turn; each band's split pass and encoder start when its upload is done and append
+// to queues shared by the whole texture; the passes over those queues (second cluster-fit pass,
+// search, finish) run once after the last band, and the blocks come back in one download.
+// Encoding the bands as independent textures instead would end every band's search pass with
+// its own tail of idle lanes. A bottom block row that wraps (h % 4 != 0) reads texel rows 0-3,
+// so its band waits for band 0's upload.
+int run_host_bc1_parts(const uint8_t *src, uint8_t *dst, int w, int h, size_t block_bytes, const qt_bc1_params &p,
+                       bool bc3, const char *what) {
+    const int bw = (w + 3) / 4, bh = (h + 3) / 4;
+    const size_t texel_row = (size_t)w * 4, block_row = (size_t)bw * block_bytes;
+    const size_t in_bytes = texel_row * (size_t)h, out_bytes = block_row * (size_t)bh;
+    const int rows_first = (int)std::max<size_t>(1, (size_t(8) << 20) / (4 * texel_row + block_row));
+    std::vector<int> cut(1, 0);  // band k covers block rows [cut[k], cut[k + 1])
+    for (long rows = rows_first; cut.back() < bh; rows *= 2)
+        cut.push_back((int)std::min<long>(bh, (long)cut.back() + rows));
+    const int nbands = (int)cut.size() - 1;  // <= 12 for any texture of <= 2^32 texels
+    int dev = 0;
+    int rc = ensure_device(&dev);
+    if (rc) return rc;
+    DevBuf din, dout;
+    if ((rc = acquire(din, dev, in_bytes)) || (rc = acquire(dout, dev, out_bytes))) return rc;
+    cudaStream_t st[2] = {thread_stream(dev), thread_stream2(dev)};
+    cudaEvent_t ev_first = thread_event(dev, 0), ev_ready = thread_event(dev, 1), ev_join = thread_event(dev, 2);
+    uint8_t *di = static_cast<uint8_t *>(din.ptr), *dout_p = static_cast<uint8_t *>(dout.ptr);
+    HostXfer x;
+    if ((rc = x.begin(dev, src, dst))) return rc;
+    qtk::Bc1Parts ps;
+    cudaError_t e = cudaSuccess;
+    if (const int brc = qtk::bc1_parts_begin(ps, (long)bw * bh, p, st[0])) rc = cuda_err((cudaError_t)brc, what);
+    if (!rc && (e = cudaEventRecord(ev_ready, st[0])) == cudaSuccess) e = cudaStreamWaitEvent(st[1], ev_ready, 0);
+    for (int k = 0; k < nbands && e == cudaSuccess && rc == QT_OK; k++) {
+        const int r0 = cut[k], r1 = cut[k + 1];
+        cudaStream_t s = st[k & 1];
+        const size_t off = (size_t)(4 * r0) * texel_row, len = (size_t)(std::min(h, 4 * r1) - 4 * r0) * texel_row;
+        if ((rc = x.in(di + off, src + off, len, s))) break;
+        if (k == 0) e = cudaEventRecord(ev_first, s);
+        if (e == cudaSuccess && (h & 3) && k == nbands - 1 && (k & 1)) e = cudaStreamWaitEvent(s, ev_first, 0);
+        if (e == cudaSuccess) {
+            const int lrc = qtk::bc1_parts_add(ps, di, w, h, p, dout_p, bc3, (long)r0 * bw, (long)r1 * bw, s);
+            if (lrc) rc = cuda_err((cudaError_t)lrc, what);
+        }
+    }
+    if (!rc && e == cudaSuccess && (e = cudaEventRecord(ev_join, st[1])) == cudaSuccess)
+        e = cudaStreamWaitEvent(st[0], ev_join, 0);
+    if (!rc && e == cudaSuccess) {
+        const int lrc = qtk::bc1_parts_end(ps, di, w, h, p, dout_p, bc3, st[0]);
+        if (lrc) rc = cuda_err((cudaError_t)lrc, what);
+    }
+    if (!rc && e == cudaSuccess) rc = x.out(dst, dout_p, out_bytes, st[0]);
+    const int frc = x.finish();
+    const cudaError_t e0 = cudaStreamSynchronize(st[0]), e1 = cudaStreamSynchronize(st[1]);
+    qtk::bc1_parts_free(ps, st[0]);  // still held only after a failure
+    if (rc) return rc;
+    if (frc) return frc;
+    if (e != cudaSuccess) return cuda_err(e, what);
+    if (e0 != cudaSuccess) return cuda_err(e0, what);
+    if (e1 != cudaSuccess) return cuda_err(e1, what);
+    return QT_OK;
+}
+
 int qt_bc1_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p, uint8_t *blocks) {
     int rc;
     if ((rc = check_dims(w, h)) || (rc = check_params(p, false)) || (rc = check_ptr(rgba, 1, "rgba")) ||
         (rc = check_ptr(blocks, 1, "blocks")))
         return rc;
     const qt_bc1_params pp = *p;
+    if (qtk::bc1_parts_eligible((long)((w + 3) / 4) * ((h + 3) / 4), pp))
+        return run_host_bc1_parts(rgba, blocks, w, h, 8, pp, false, "bc1 encode");
     return run_host_banded(rgba, blocks, true, w, h, 8,
                            [&](void *in, void *out, long b0, long b1, void *s) {
                                return qtk::launch_bc1_encode_range((const uint8_t *)in, w, h, pp, (uint8_t *)out, false, b0, b1, s);
@@ -806,6 +868,8 @@ int qt_bc3_encode_host(const uint8_t *rgba, int w, int h, const qt_bc1_params *p
         (rc = check_ptr(blocks, 1, "blocks")))
         return rc;
     const qt_bc1_params pp = *p;
+    if (qtk::bc1_parts_eligible((long)((w + 3) / 4) * ((h + 3) / 4), pp))
+        return run_host_bc1_parts(rgba, blocks, w, h, 16, pp, true, "bc3 encode");
     return run_host_banded(rgba, blocks, true, w, h, 16,
                            [&](void *in, void *out, long b0, long b1, void *s) {
                                return qtk::launch_bc1_encode_range((const uint8_t *)in, w, h, pp, (uint8_t *)out, true, b0, b1, s);

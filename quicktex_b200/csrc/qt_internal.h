@@ -77,6 +77,28 @@ int launch_bc4_encode_range(const uint8_t *rgba, int w, int h, int c0, int c1, b
 // The fewest blocks for which a BC1/BC3 launch with EndpointSearch runs the search as its own
 // refill pass (two searches per resident lane of that pass).
 long defer_min_blocks();
+// BC1/BC3 encode of one texture whose texels arrive in parts (the row bands of a host upload),
+// on the deferred path: bc1_parts_begin allocates and clears the shared scratch on `stream`;
+// bc1_parts_add runs the split pass and the encoder over the blocks [b_begin, b_end) on its
+// stream once that part's texels are there (the stream ordered after begin's); bc1_parts_end,
+// on a stream ordered after every part, runs the second cluster-fit pass, EndpointSearch and the
+// finish pass over all parts' queues, then frees the scratch. The result equals one
+// launch_bc1_encode over the texture. Only where bc1_parts_eligible holds (settings with
+// EndpointSearch, defer_min_blocks() to 2^32 blocks), in at most 32 parts; bc1_parts_free
+// releases the scratch after a failure.
+struct Bc1Parts {
+    uint32_t *scratch = nullptr;
+    long n = 0;
+    bool cf2 = false;
+    int parts = 0;
+};
+bool bc1_parts_eligible(long nblocks, const qt_bc1_params &p);
+int bc1_parts_begin(Bc1Parts &ps, long nblocks, const qt_bc1_params &p, void *stream);
+int bc1_parts_add(Bc1Parts &ps, const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
+                  long b_begin, long b_end, void *stream);
+int bc1_parts_end(Bc1Parts &ps, const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
+                  void *stream);
+void bc1_parts_free(Bc1Parts &ps, void *stream);
 // kernels one launch_bc1_encode_range over n blocks issues (0 for none): the encoder, plus the
 // split pass from kSplitMinBlocks blocks, plus the search pass from defer_min_blocks() blocks
 int bc1_encode_kernels(long n, const qt_bc1_params &p);

@@ -26,6 +26,7 @@
 #include <climits>
 #include <cstdint>
 #include <cstdlib>
+#include <type_traits>
 
 #include "qt_internal.h"
 
@@ -827,6 +828,140 @@ static void launch_fast(int g, cudaStream_t s, const uint8_t *rgba, int w, int h
     }
 }
 
+template <typename F>
+static void by_interp(int interpolator, F &&f) {
+    switch (interpolator) {
+        case IT_IDEAL: f(std::integral_constant<int, IT_IDEAL>()); break;
+        case IT_ROUND: f(std::integral_constant<int, IT_ROUND>()); break;
+        case IT_NVIDIA: f(std::integral_constant<int, IT_NVIDIA>()); break;
+        default: f(std::integral_constant<int, IT_AMD>()); break;
+    }
+}
+
+// Scratch of the deferred path over n blocks, in 32-bit words: a 64-word header (word 0 the
+// list count, 1-3 the search queues' counts, 4-6 their heads, 8-9 the second-pass queue's
+// counts, 16 the finish queue's count, 32-63 the list counts of a texture encoded in parts),
+// the list of non-solid blocks, the three search queues (5 arrays each), the finish queue (3
+// arrays) and, with the second cluster-fit pass, its queue (6 arrays).
+constexpr int kPartCount0 = 32, kMaxParts = 32;
+static size_t defer_words(long n, bool cf2) { return 64 + 19 * (size_t)n + (cf2 ? 6 * (size_t)n : 0); }
+
+struct DeferQueues {
+    SearchQueues q;
+    FinishQueue fq;
+    Cf2Queue c;
+};
+
+static DeferQueues defer_layout(uint32_t *scratch, long n, bool cf2) {
+    DeferQueues d{};
+    uint32_t *qb = scratch + 64 + n;
+    d.q.count = scratch + 1;
+    d.q.head = scratch + 4;
+    d.q.cap = n;
+    d.q.b = qb;
+    d.q.lohi = qb + 3 * (size_t)n;
+    d.q.err = qb + 6 * (size_t)n;
+    d.q.sel = qb + 9 * (size_t)n;
+    d.q.mode = qb + 12 * (size_t)n;
+    d.fq.count = scratch + 16;  // searches that moved the endpoints
+    d.fq.b = qb + 15 * (size_t)n;
+    d.fq.lohi = d.fq.b + (size_t)n;
+    d.fq.mode = d.fq.b + 2 * (size_t)n;
+    if (cf2) {
+        uint32_t *cb = qb + 18 * (size_t)n;
+        d.c.count = scratch + 8;
+        d.c.b = cb;
+        d.c.lohi = cb + (size_t)n;
+        d.c.err = cb + 2 * (size_t)n;
+        d.c.sel = cb + 3 * (size_t)n;
+        d.c.mode = cb + 4 * (size_t)n;
+        d.c.orig = cb + 5 * (size_t)n;
+        d.c.cap = n;
+    }
+    return d;
+}
+
+// The deferred path's first passes over the blocks [b0, b1): the split pass lists the
+// non-solid blocks in list/count, the encoder runs each to its first cluster-fit pass and
+// queues what remains (second pass, 3-colour trials, EndpointSearch) in d.
+template <int I>
+static void defer_front(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3, int aligned,
+                        const DeferQueues &d, uint32_t *list, uint32_t *count, long b0, long b1, cudaStream_t s) {
+    const int bw = (w + 3) / 4;
+    const long n = b1 - b0;
+    k_bc1_split<I><<<grid_for(n, 256), 256, 0, s>>>(rgba, w, h, bw, b0, b1, out, bc3, aligned, list, count);
+    k_bc1_defer<I><<<grid_for(n, tpb::kThreads), tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, list,
+                                                                          count, d.q, d.c);
+}
+
+// ... and its passes over the queues: second cluster-fit pass and 3-colour trials (cf2),
+// EndpointSearch with lane refill, and the selectors of the searches that moved.
+template <int I>
+static void defer_back(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3, int aligned,
+                       const DeferQueues &d, bool cf2, cudaStream_t s) {
+    const int bw = (w + 3) / 4;
+    const int gsearch = num_sms() * 4;
+    if (cf2) k_bc1_cf2<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, d.c, d.q);
+    k_bc1_search<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, d.q, d.fq);
+    k_bc1_finish<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, d.fq);
+}
+
+static int texel_aligned(const uint8_t *rgba, int w) {
+    return ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
+}
+
+bool bc1_parts_eligible(long nblocks, const qt_bc1_params &p) {
+    return p.search_rounds > 0 && nblocks >= defer_min_blocks() && nblocks <= 0xFFFFFFFFL;
+}
+
+int bc1_parts_begin(Bc1Parts &ps, long nblocks, const qt_bc1_params &p, void *stream) {
+    cudaStream_t s = (cudaStream_t)stream;
+    ps = Bc1Parts{};
+    if (!bc1_parts_eligible(nblocks, p)) return (int)cudaErrorInvalidValue;
+    ps.n = nblocks;
+    ps.cf2 = cf2_pass(p);
+    cudaError_t e = scratch_alloc((void **)&ps.scratch, defer_words(nblocks, ps.cf2) * sizeof(uint32_t), s);
+    if (e != cudaSuccess) {
+        ps.scratch = nullptr;
+        return (int)e;
+    }
+    e = cudaMemsetAsync(ps.scratch, 0, 64 * sizeof(uint32_t), s);
+    return (int)e;
+}
+
+int bc1_parts_add(Bc1Parts &ps, const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
+                  long b_begin, long b_end, void *stream) {
+    if (!ps.scratch || ps.parts >= kMaxParts || b_begin < 0 || b_end > ps.n || b_end <= b_begin)
+        return (int)cudaErrorInvalidValue;
+    // part k lists its non-solid blocks in its own slice of the list (at most b_end - b_begin
+    // of them) and counts them in header word 32 + k; the queues are shared
+    uint32_t *list = ps.scratch + 64 + b_begin, *count = ps.scratch + kPartCount0 + ps.parts++;
+    const DeferQueues d = defer_layout(ps.scratch, ps.n, ps.cf2);
+    cudaStream_t s = (cudaStream_t)stream;
+    by_interp(p.interpolator, [&](auto I) {
+        defer_front<decltype(I)::value>(rgba, w, h, p, out, bc3, texel_aligned(rgba, w), d, list, count, b_begin, b_end, s);
+    });
+    return (int)cudaGetLastError();
+}
+
+int bc1_parts_end(Bc1Parts &ps, const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
+                  void *stream) {
+    if (!ps.scratch) return (int)cudaErrorInvalidValue;
+    const DeferQueues d = defer_layout(ps.scratch, ps.n, ps.cf2);
+    cudaStream_t s = (cudaStream_t)stream;
+    by_interp(p.interpolator, [&](auto I) {
+        defer_back<decltype(I)::value>(rgba, w, h, p, out, bc3, texel_aligned(rgba, w), d, ps.cf2, s);
+    });
+    const cudaError_t e = cudaGetLastError();
+    bc1_parts_free(ps, stream);
+    return (int)e;
+}
+
+void bc1_parts_free(Bc1Parts &ps, void *stream) {
+    if (ps.scratch) scratch_free(ps.scratch, (cudaStream_t)stream);
+    ps.scratch = nullptr;
+}
+
 int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_params &p, uint8_t *out, bool bc3,
                             long b_begin, long b_end, void *stream) {
     const int bw = (w + 3) / 4;
@@ -834,7 +969,7 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
     if (n <= 0) return 0;
     cudaStream_t s = (cudaStream_t)stream;
     {
-        const int aligned = ((w & 3) == 0) && ((reinterpret_cast<uintptr_t>(rgba) & 15) == 0);
+        const int aligned = texel_aligned(rgba, w);
         const int g = grid_for(n, tpb::kThreads);
         if ((n < kSplitMinBlocks || n > 0xFFFFFFFFL) && p.search_rounds == 0) {
             launch_fast(g, s, rgba, w, h, bw, b_begin, b_end, p, out, bc3, aligned, nullptr, nullptr);
@@ -858,55 +993,18 @@ int launch_bc1_encode_range(const uint8_t *rgba, int w, int h, const qt_bc1_para
         // and the second four-colour cluster-fit pass, when there is one, runs in its own pass
         // for the blocks where it can change the result
         const bool cf2 = defer && cf2_pass(p);
-        const size_t words = 64 + (size_t)n + (defer ? 18 * (size_t)n : 0) + (cf2 ? 6 * (size_t)n : 0);
+        const size_t words = defer ? defer_words(n, cf2) : 64 + (size_t)n;
         uint32_t *scratch = nullptr;
         cudaError_t e = scratch_alloc((void **)&scratch, words * sizeof(uint32_t), s);
         if (e != cudaSuccess) return (int)e;
         uint32_t *count = scratch, *list = scratch + 64;
         e = cudaMemsetAsync(scratch, 0, 64 * sizeof(uint32_t), s);  // list count, queue counts and heads
         if (e == cudaSuccess && defer) {
-            SearchQueues q;
-            q.count = scratch + 1;
-            q.head = scratch + 4;
-            q.cap = n;
-            uint32_t *qb = list + n;
-            q.b = qb;
-            q.lohi = qb + 3 * (size_t)n;
-            q.err = qb + 6 * (size_t)n;
-            q.sel = qb + 9 * (size_t)n;
-            q.mode = qb + 12 * (size_t)n;
-            FinishQueue fq;  // searches that moved the endpoints
-            fq.count = scratch + 16;
-            fq.b = qb + 15 * (size_t)n;
-            fq.lohi = fq.b + (size_t)n;
-            fq.mode = fq.b + 2 * (size_t)n;
-            Cf2Queue c{};
-            if (cf2) {
-                uint32_t *cb = qb + 18 * (size_t)n;
-                c.count = scratch + 8;
-                c.b = cb;
-                c.lohi = cb + (size_t)n;
-                c.err = cb + 2 * (size_t)n;
-                c.sel = cb + 3 * (size_t)n;
-                c.mode = cb + 4 * (size_t)n;
-                c.orig = cb + 5 * (size_t)n;
-                c.cap = n;
-            }
-            const int gs = grid_for(n, 256);
-            const int gsearch = num_sms() * 4;
-            switch (p.interpolator) {
-#define QT_DEFER(I)                                                                                                        \
-    k_bc1_split<I><<<gs, 256, 0, s>>>(rgba, w, h, bw, b_begin, b_end, out, bc3, aligned, list, count);                      \
-    k_bc1_defer<I><<<g, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, list, count, q, c);                    \
-    if (cf2) k_bc1_cf2<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, c, q);                    \
-    k_bc1_search<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, q, fq);                       \
-    k_bc1_finish<I><<<gsearch, tpb::kThreads, 0, s>>>(rgba, w, h, bw, p, out, bc3, aligned, fq);
-                case IT_IDEAL: QT_DEFER(IT_IDEAL) break;
-                case IT_ROUND: QT_DEFER(IT_ROUND) break;
-                case IT_NVIDIA: QT_DEFER(IT_NVIDIA) break;
-                default: QT_DEFER(IT_AMD) break;
-#undef QT_DEFER
-            }
+            const DeferQueues d = defer_layout(scratch, n, cf2);
+            by_interp(p.interpolator, [&](auto I) {
+                defer_front<decltype(I)::value>(rgba, w, h, p, out, bc3, aligned, d, list, count, b_begin, b_end, s);
+                defer_back<decltype(I)::value>(rgba, w, h, p, out, bc3, aligned, d, cf2, s);
+            });
             e = cudaGetLastError();
         } else if (e == cudaSuccess && p.search_rounds == 0) {
             const int gs = grid_for(n, 256);

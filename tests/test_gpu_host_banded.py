@@ -34,7 +34,15 @@ def test_banded_encode_equals_device(w, h):
     s = torch.cuda.current_stream()
     p0 = capi.params_for_level(0)
     p3 = capi.params_for_level(3)
+    # EndpointSearch settings on >= ~151k blocks take the parted host path: bands encoded to
+    # their first cluster-fit pass as they arrive, then one pass over the shared queues
+    p13 = capi.params_for_level(13, 0x03, 2)
+    p18 = capi.params_for_level(18, 0x13, 0)
     cases = [
+        ("bc1 L13", 8, lambda src, dst: L.qt_bc1_encode_host(src, w, h, ctypes.byref(p13), dst),
+         lambda src, dst: L.qt_bc1_encode_device(src, w, h, ctypes.byref(p13), dst, capi._vp(s.cuda_stream))),
+        ("bc3 L18", 16, lambda src, dst: L.qt_bc3_encode_host(src, w, h, ctypes.byref(p18), dst),
+         lambda src, dst: L.qt_bc3_encode_device(src, w, h, ctypes.byref(p18), dst, capi._vp(s.cuda_stream))),
         ("bc1", 8, lambda src, dst: L.qt_bc1_encode_host(src, w, h, ctypes.byref(p0), dst),
          lambda src, dst: L.qt_bc1_encode_device(src, w, h, ctypes.byref(p0), dst, capi._vp(s.cuda_stream))),
         ("bc3", 16, lambda src, dst: L.qt_bc3_encode_host(src, w, h, ctypes.byref(p3), dst),
@@ -134,3 +142,31 @@ def test_staged_copy_of_uneven_length(pieces):
     d_rgba = torch.full((w * h * 4,), 0xA5, dtype=torch.uint8, device="cuda")
     capi.check(L.qt_bc1_decode_device(capi._vp(d_out.data_ptr()), w, h, 0, 1, capi._vp(d_rgba.data_ptr()), s))
     assert np.array_equal(rgba_h, d_rgba.cpu().numpy())
+
+
+@pytest.mark.parametrize("pinned", [False, True])
+def test_parted_search_encode_equals_device(pinned):
+    """The parted host path (EndpointSearch settings on >= ~151k blocks) with pinned and
+    with pageable host buffers, on a ragged texture whose last band waits for band 0."""
+    import torch
+
+    L = capi.lib()
+    w, h = 2051, 2047
+    img = np.ascontiguousarray(syn.block_mix(w, h, workload=7))
+    nb = ((w + 3) // 4) * ((h + 3) // 4)
+    s = capi._vp(torch.cuda.current_stream().cuda_stream)
+    d_in = _dev(img)
+    for level, mode, interp in ((18, 0x04, 0), (16, 0x03, 3)):
+        p = capi.params_for_level(level, mode, interp)
+        if pinned:
+            h_in = torch.from_numpy(img.reshape(-1)).pin_memory()
+            h_out = torch.zeros(nb * 8, dtype=torch.uint8).pin_memory()
+            src, dst = capi._vp(h_in.data_ptr()), capi._vp(h_out.data_ptr())
+        else:
+            out_np = np.zeros(nb * 8, np.uint8)
+            src, dst = capi._vp(img.ctypes.data), capi._vp(out_np.ctypes.data)
+        capi.check(L.qt_bc1_encode_host(src, w, h, ctypes.byref(p), dst))
+        got = h_out.numpy() if pinned else out_np
+        d_out = torch.empty(nb * 8, dtype=torch.uint8, device="cuda")
+        capi.check(L.qt_bc1_encode_device(capi._vp(d_in.data_ptr()), w, h, ctypes.byref(p), capi._vp(d_out.data_ptr()), s))
+        assert np.array_equal(got, d_out.cpu().numpy()), (level, mode, interp, pinned)
