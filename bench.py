@@ -416,7 +416,7 @@ def run_ours(args, world, rank, local):
         e2e_value = world * blocks_step / e2e_s / 1e6
 
     # the same through the drop-in Python API: BC1Encoder(level, mode, interpolator).encode(RawTexture),
-    # whose texels live in the RawTexture's own pageable host memory (one step)
+    # whose texels live in the RawTexture's own storage (pinned blocks from the library's cache)
     e2e_dropin = None
     if not args.no_e2e and world == 1:
         import quicktex_b200 as qt
@@ -439,7 +439,8 @@ def run_ours(args, world, rank, local):
         e2e_dropin = {"value": blocks_step / float(np.median(passes)) / 1e6, "unit": "Mblocks/s",
                       "passes_mblocks_s": [blocks_step / t / 1e6 for t in passes],
                       "path": "BC1Encoder(level, color_mode, interpolator).encode(RawTexture) for the 36 settings: "
-                              "texels in pageable host memory, blocks returned in a new BC1Texture; median of 3 passes"}
+                              "texels in the RawTexture's storage (pinned, from qt_host_alloc), blocks returned in a new "
+                              "BC1Texture; median of 3 passes"}
         del tex
 
     # roofline: algorithmic lane-ops (10 per candidate evaluation) / kernel time
@@ -595,7 +596,7 @@ def measure_config1(dev, stream, flush, reps: int = 20):
     """512x512 gradient + noise (10% solid blocks), BC1 level 5 four-colour Ideal encode, then
     decode. Device-resident through the C-ABI (CUDA events, L2 flushed before each run), and end
     to end through the drop-in Python API (BC1Encoder(5).encode(RawTexture) and
-    BC1Decoder().decode, whose texels live in pageable host memory), beside the reference's CPU
+    BC1Decoder().decode, whose texels live in the textures' own pinned storage), beside the reference's CPU
     figures. Outputs are checked against the reference's committed digests."""
     import torch
 
@@ -640,7 +641,7 @@ def measure_config1(dev, stream, flush, reps: int = 20):
                    "l2": "flushed before each run"},
         "e2e_dropin": {"encode_mblocks_s": nb / e_enc / 1e3, "decode_mblocks_s": nb / e_dec / 1e3,
                        "encode_decode_mblocks_s": nb / e_both / 1e3,
-                       "path": "BC1Encoder(5).encode(RawTexture) / BC1Decoder().decode: pageable host memory, "
+                       "path": "BC1Encoder(5).encode(RawTexture) / BC1Decoder().decode: the textures' own (pinned) storage, "
                                "copies and kernel launches inside the timed call"},
         "roofline": {"bound": "hbm", "encode_gb_s": nb * 72 / enc_ms / 1e6, "decode_gb_s": nb * 72 / dec_ms / 1e6,
                      "peak_gb_s": hbm, "encode_frac": nb * 72 / enc_ms / 1e6 / hbm,
@@ -656,7 +657,7 @@ def measure_config3(dev, stream, reps: int = 5):
     cutouts, ramps, noise), BC4 on channels 0, 1 and 3 of it, and BC5 (channels 0, 1) of the
     normal map of a sum of 8 Gaussian bumps; each decoded back. Device-resident (256 MiB inputs,
     larger than L2), CUDA events; BC3 and BC5 encode also end to end through the drop-in Python
-    API from pageable memory. Outputs checked against the reference's committed digests."""
+    API from the textures' own (pinned) storage. Outputs checked against the reference's committed digests."""
     import torch
 
     import quicktex_b200 as qt
@@ -720,7 +721,7 @@ def measure_config3(dev, stream, reps: int = 5):
         "blocks": nb, "device": res, "peak_gb_s": hbm, "peak_source": kind,
         "algorithmic_bytes_per_block": {"bc3": 80, "bc5": 80, "bc4": 72},
         "e2e_dropin": {"bc3_L5_encode_mblocks_s": nb / e3 / 1e3, "bc5_encode_mblocks_s": nb / e5 / 1e3,
-                       "path": "BC3Encoder(5) / BC5Encoder(0, 1).encode(RawTexture): pageable host memory, "
+                       "path": "BC3Encoder(5) / BC5Encoder(0, 1).encode(RawTexture): the textures' own (pinned) storage, "
                                "copies and kernels inside the timed call"},
         "cpu": {"bc3_L5_encode": cpu3, "bc4_encode": cpu4, "bc5_encode": cpu5},
         "bit_exact_vs_reference": exact,

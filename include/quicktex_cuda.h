@@ -113,6 +113,18 @@ int qt_bc3_encode_host(const uint8_t *rgba, int width, int height, const qt_bc1_
 int qt_bc3_encode_device(const uint8_t *rgba, int width, int height, const qt_bc1_params *params, uint8_t *blocks,
                          void *stream);
 
+/* No reference counterpart: host memory for texture storage from the library's cache of
+ * pinned (page-locked) blocks. The *_host entry points copy pinned buffers with the copy
+ * engines directly; pageable buffers go through a pinned staging ring first, which costs
+ * about as much again on a large texture. A block is page-locked once, when first
+ * allocated, and a freed block stays cached for the next allocation of its size class
+ * (sizes round up by at most 12.5%; up to 2 GiB stay cached). Blocks under 256 KiB, and
+ * all blocks where no pinned memory can be had (no usable GPU, or the system's limit), are
+ * ordinary memory, which the entry points stage as usual. Thread-safe. qt_host_free ignores NULL and pointers it did
+ * not hand out. The drop-in texture classes keep their texels here. */
+int qt_host_alloc(size_t bytes, void **ptr);
+void qt_host_free(void *ptr);
+
 /* No reference counterpart: the number of kernels one qt_bc1_encode_device or
  * qt_bc3_encode_device call on a width x height texture launches on the current
  * device with these params (1 = the encoder; 2 = a split pass that writes the solid

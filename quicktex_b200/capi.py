@@ -32,7 +32,7 @@ EXPORTS = (
     "qt_server_create", "qt_server_destroy", "qt_server_set_rules", "qt_server_set_grid", "qt_server_set_threads",
     "qt_server_submit",
     "qt_server_poll", "qt_server_get_stats", "qt_server_clock",
-    "qt_resize_bilinear_device", "qt_flip_swizzle_device", "qt_bc1_encode_kernels",
+    "qt_resize_bilinear_device", "qt_flip_swizzle_device", "qt_bc1_encode_kernels", "qt_host_alloc", "qt_host_free",
 )
 
 
@@ -98,6 +98,10 @@ def lib() -> ctypes.CDLL:
             f.restype = _i
         L.qt_last_error.restype = ctypes.c_char_p
         L.qt_version.restype = ctypes.c_char_p
+        L.qt_host_alloc.argtypes = [ctypes.c_size_t, ctypes.POINTER(_vp)]
+        L.qt_host_alloc.restype = _i
+        L.qt_host_free.argtypes = [_vp]
+        L.qt_host_free.restype = None
         _lib = L
     return _lib
 

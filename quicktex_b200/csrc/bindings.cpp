@@ -99,6 +99,43 @@ void check(int rc) {
 // ---------------------------------------------------------------------------
 // textures (quicktex/Texture.h)
 // ---------------------------------------------------------------------------
+// Texel or block storage in the library's cache of pinned host blocks (qt_host_alloc): the
+// host-buffer entry points copy it with the copy engines directly, where the reference's
+// pageable std::vector would be staged through a pinned ring first (about as much time again
+// as the copy itself on a large texture).
+class HostBytes {
+   public:
+    HostBytes() = default;
+    explicit HostBytes(size_t n) : n_(n) {
+        void *p = nullptr;
+        if (qt_host_alloc(n, &p) != QT_OK) throw std::bad_alloc();
+        p_ = static_cast<uint8_t *>(p);
+    }
+    HostBytes(const HostBytes &o) : HostBytes(o.n_) { std::memcpy(p_, o.p_, n_); }
+    HostBytes(HostBytes &&o) noexcept : p_(o.p_), n_(o.n_) {
+        o.p_ = nullptr;
+        o.n_ = 0;
+    }
+    HostBytes &operator=(HostBytes o) noexcept {
+        std::swap(p_, o.p_);
+        std::swap(n_, o.n_);
+        return *this;
+    }
+    ~HostBytes() { qt_host_free(p_); }
+    uint8_t *data() { return p_; }
+    const uint8_t *data() const { return p_; }
+    size_t size() const { return n_; }
+    uint8_t &operator[](size_t i) { return p_[i]; }
+
+   private:
+    uint8_t *p_ = nullptr;
+    size_t n_ = 0;
+};
+
+// Construction without the initial fill, for textures whose every byte is written next (an
+// encoder's result, a texture made from a bytes-like object).
+struct NoFill {};
+
 class Texture {
    public:
     virtual ~Texture() = default;
@@ -110,13 +147,14 @@ class Texture {
     const uint8_t *Data() const { return data_.data(); }
 
    protected:
-    Texture(int w, int h, size_t nbytes) : w_(w), h_(h) {
+    Texture(int w, int h, size_t nbytes, NoFill) : w_(w), h_(h) {
         if (w <= 0) throw std::invalid_argument("Texture width must be greater than 0");
         if (h <= 0) throw std::invalid_argument("Texture height must be greater than 0");
-        data_.assign(nbytes, 0);
+        data_ = HostBytes(nbytes);
     }
+    Texture(int w, int h, size_t nbytes) : Texture(w, h, nbytes, NoFill{}) { std::memset(data_.data(), 0, nbytes); }
     int w_, h_;
-    std::vector<uint8_t> data_;
+    HostBytes data_;
 };
 
 inline size_t checked_area(int w, int h) { return (w > 0 && h > 0) ? (size_t)w * (size_t)h : 0; }
@@ -126,6 +164,7 @@ class RawTexture : public Texture {
     RawTexture(int w, int h) : Texture(w, h, checked_area(w, h) * 4) {
         for (size_t i = 3; i < data_.size(); i += 4) data_[i] = 255;  // Color() = (0, 0, 0, 255)
     }
+    RawTexture(int w, int h, NoFill f) : Texture(w, h, checked_area(w, h) * 4, f) {}
     Color GetPixel(int x, int y) const {
         const uint8_t *p = data_.data() + ((size_t)y * w_ + x) * 4;
         return Color{p[0], p[1], p[2], p[3]};
@@ -257,6 +296,10 @@ template <typename B> class BlockTexture : public Texture {
         bw_ = (w + 3) / 4;
         bh_ = (h + 3) / 4;
     }
+    BlockTexture(int w, int h, NoFill f) : Texture(w, h, (size_t)((w + 3) / 4) * (size_t)((h + 3) / 4) * sizeof(B), f) {
+        bw_ = (w + 3) / 4;
+        bh_ = (h + 3) / 4;
+    }
     int BlocksX() const { return bw_; }
     int BlocksY() const { return bh_; }
     std::tuple<int, int> BlocksXY() const { return {bw_, bh_}; }
@@ -329,7 +372,7 @@ class BC1Encoder {
     }
 
     BC1Texture Encode(const RawTexture &tex) const {
-        BC1Texture out(tex.Width(), tex.Height());
+        BC1Texture out(tex.Width(), tex.Height(), NoFill{});  // every block is written
         const qt_bc1_params p = params();
         int rc;
         {
@@ -398,7 +441,7 @@ class BC4Encoder {
         if (channel >= 4) throw std::invalid_argument("Channel out of range");
     }
     BC4Texture Encode(const RawTexture &tex) const {
-        BC4Texture out(tex.Width(), tex.Height());
+        BC4Texture out(tex.Width(), tex.Height(), NoFill{});  // every block is written
         int rc;
         {
             py::gil_scoped_release nogil;
@@ -440,7 +483,7 @@ class BC3Encoder {
         : bc1_(std::make_shared<BC1Encoder>(level, ColorMode::FourColor, std::move(interp))), bc4_(std::make_shared<BC4Encoder>(3)) {}
     explicit BC3Encoder(unsigned level = 5) : BC3Encoder(level, std::make_shared<Interpolator>()) {}
     BC3Texture Encode(const RawTexture &tex) const {
-        BC3Texture out(tex.Width(), tex.Height());
+        BC3Texture out(tex.Width(), tex.Height(), NoFill{});  // every block is written
         const qt_bc1_params p = bc1_->params();
         int rc;
         {
@@ -486,7 +529,7 @@ class BC5Encoder {
    public:
     BC5Encoder(uint8_t c0 = 0, uint8_t c1 = 1) : e0_(std::make_shared<BC4Encoder>(c0)), e1_(std::make_shared<BC4Encoder>(c1)) {}
     BC5Texture Encode(const RawTexture &tex) const {
-        BC5Texture out(tex.Width(), tex.Height());
+        BC5Texture out(tex.Width(), tex.Height(), NoFill{});  // every block is written
         const int c0 = e0_->GetChannel(), c1 = e1_->GetChannel();
         int rc;
         {
@@ -538,7 +581,7 @@ py::buffer_info request_bytes(py::buffer buf, size_t need) {
 }
 
 template <typename T> T buffer_to_texture(py::buffer buf, int w, int h) {
-    T out(w, h);
+    T out(w, h, NoFill{});
     py::buffer_info info = request_bytes(buf, out.NBytes());
     std::memcpy(out.Data(), info.ptr, out.NBytes());
     return out;
@@ -593,6 +636,9 @@ template <typename B> py::class_<BlockTexture<B>, Texture> bind_block_texture(py
     py::class_<T, Texture> c(m, name);
     c.def(py::init<int, int>(), "width"_a, "height"_a);
     c.def_static("from_bytes", &buffer_to_texture<T>, "data"_a, "width"_a, "height"_a);
+    // no reference counterpart: a texture whose blocks the caller writes next (a device-to-host
+    // copy straight into its storage), without the zero fill
+    c.def_static("_uninitialized", [](int w, int h) { return T(w, h, NoFill{}); }, "width"_a, "height"_a);
     c.def_property_readonly("width_blocks", &T::BlocksX);
     c.def_property_readonly("height_blocks", &T::BlocksY);
     c.def_property_readonly("size_blocks", &T::BlocksXY);

@@ -3,7 +3,8 @@
 // Owns the constant tables (built once per process, uploaded once per
 // device), a pooled device allocator for the host-buffer entry points, the
 // pinned staging of pageable host buffers (a ring per host thread and device,
-// a shared pool of copy threads), the thread-local error message, and argument
+// a shared pool of copy threads), the cache of pinned host blocks behind
+// qt_host_alloc, the thread-local error message, and argument
 // checking with the reference's error semantics.
 //
 // Compiled as plain C++ on x86-64 with -ffp-contract=off: the factor matrices
@@ -449,6 +450,95 @@ Stage &thread_stage(int dev) {
     return stages[dev];
 }
 
+// Cache of pinned host blocks for texture storage (qt_host_alloc). A block is page-locked
+// once, when it is first allocated, and kept for reuse when freed: cudaFreeHost synchronises
+// the whole device, so it runs only when the cached total passes kMaxCached. Sizes round up
+// to an eighth of their power of two (at most 12.5% over). Blocks under 256 KiB, and all blocks
+// where no pinned memory can be had (no usable GPU, or the system's limit), come from ordinary
+// memory instead; the host-buffer entry points then stage them like any pageable buffer.
+class HostCache {
+   public:
+    static HostCache &get() {
+        static HostCache *c = new HostCache();  // never destroyed: blocks may outlive static teardown
+        return *c;
+    }
+    int alloc(size_t n, void **out) {
+        const size_t cls = host_class(n);
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            auto it = free_.find(cls);
+            if (it != free_.end()) {
+                *out = it->second;
+                free_.erase(it);
+                cached_ -= cls;
+                live_[*out] = {cls, true};
+                return QT_OK;
+            }
+        }
+        void *p = nullptr;
+        bool pinned = false;
+        if (cls >= kMinPinned && !no_pinned_.load(std::memory_order_relaxed)) {
+            const cudaError_t e = cudaHostAlloc(&p, cls, cudaHostAllocPortable);
+            if (e == cudaSuccess) {
+                pinned = true;
+            } else {
+                cudaGetLastError();
+                p = nullptr;
+                if (e != cudaErrorMemoryAllocation) no_pinned_.store(true, std::memory_order_relaxed);
+            }
+        }
+        if (!p && posix_memalign(&p, 4096, cls) != 0) return set_err(QT_ERR_OOM, "host allocation of %zu bytes failed", n);
+        std::lock_guard<std::mutex> lk(mu_);
+        live_[p] = {cls, pinned};
+        *out = p;
+        return QT_OK;
+    }
+    void release(void *p) {
+        if (!p) return;
+        void *drop = nullptr;
+        {
+            std::lock_guard<std::mutex> lk(mu_);
+            auto it = live_.find(p);
+            if (it == live_.end()) return;  // not ours
+            const Entry e = it->second;
+            live_.erase(it);
+            if (!e.pinned) {
+                std::free(p);
+                return;
+            }
+            if (cached_ + e.cls <= kMaxCached) {
+                free_.emplace(e.cls, p);
+                cached_ += e.cls;
+                return;
+            }
+            drop = p;
+        }
+        cudaFreeHost(drop);
+        cudaGetLastError();
+    }
+
+   private:
+    struct Entry {
+        size_t cls;
+        bool pinned;
+    };
+    static constexpr size_t kMaxCached = size_t(2) << 30;
+    // below this, ordinary memory: staging a small buffer costs less than pinning it
+    static constexpr size_t kMinPinned = size_t(256) << 10;
+    static size_t host_class(size_t n) {
+        if (n == 0) n = 1;
+        size_t c = 4096;
+        while (c < n) c <<= 1;
+        const size_t step = std::max<size_t>(4096, c / 8);
+        return (n + step - 1) / step * step;
+    }
+    std::mutex mu_;
+    std::multimap<size_t, void *> free_;
+    std::map<void *, Entry> live_;
+    size_t cached_ = 0;
+    std::atomic<bool> no_pinned_{false};
+};
+
 // Host<->device copies of the host-buffer entry points: pinned (or otherwise registered)
 // host memory is copied directly, pageable memory through the thread's stage.
 struct HostXfer {
@@ -746,6 +836,14 @@ int qt_init(int device) {
     cudaSetDevice(prev);
     return rc;
 }
+
+int qt_host_alloc(size_t bytes, void **ptr) {
+    if (!ptr) return set_err(QT_ERR_ARG, "ptr is NULL");
+    *ptr = nullptr;
+    return HostCache::get().alloc(bytes, ptr);
+}
+
+void qt_host_free(void *ptr) { HostCache::get().release(ptr); }
 
 // ---- encoders ----
 int qt_bc1_encode_device(const uint8_t *rgba, int w, int h, const qt_bc1_params *p, uint8_t *blocks, void *stream) {

@@ -287,7 +287,7 @@ def encode_many(requests: typing.Sequence[EncodeRequest], max_batch_bytes: int =
     import torch
 
     from . import RawTexture
-    from .batch import Batch, Job
+    from .batch import Batch, Job, copy_async
 
     prepared = [_prepare(r) for r in requests]
     out: typing.List[typing.Optional[DDSFile]] = [None] * len(requests)
@@ -336,16 +336,22 @@ def encode_many(requests: typing.Sequence[EncodeRequest], max_batch_bytes: int =
             kw = {k: v for k, v in item.items() if k != "fmt"}
             for (w, h), a, b in zip(sizes, lv_in, lv_out):
                 items.append(Job.encode(item["fmt"], np.zeros(0, np.uint8), w, h, **kw).item(lb + a, ob + b))
+        # the result textures first (their storage is pinned host memory), so every level's
+        # blocks are copied from the device straight into its texture
+        made, copies = [], []
+        for (i, sizes, fmt, _item, _img), lv_out in zip(pending, out_off):
+            texs = [fmt.texture._uninitialized(w, h) for w, h in sizes]
+            for t, o in zip(texs, lv_out):
+                copies.append((np.frombuffer(memoryview(t), np.uint8).ctypes.data, ob + o, t.nbytes))
+            made.append((i, texs, fmt))
         batch = Batch(dev.index)
         try:
             batch.run(items, sp)  # every level of every image in one persistent launch
-            host = d_out.cpu().numpy()
+            copy_async(np.array(copies, np.uint64).reshape(-1, 3), sp)
+            stream.synchronize()
         finally:
             batch.close()
-        for (i, sizes, fmt, _item, _img), lv_out in zip(pending, out_off):
-            bb = _BLOCK_BYTES[fmt.name]
-            texs = [fmt.texture.from_bytes(host[o: o + ((w + 3) // 4) * ((h + 3) // 4) * bb].tobytes(), w, h)
-                    for (w, h), o in zip(sizes, lv_out)]
+        for i, texs, fmt in made:
             out[i] = _dds_file(texs, requests[i].four_cc, fmt)
         pending.clear()
 
@@ -446,7 +452,10 @@ def decode_many(files: typing.Sequence[DDSFile], mip: int = 0, flip: bool = Fals
             for j, b in zip(jobs, out_off):
                 capi.check(capi.lib().qt_flip_swizzle_device(capi._vp(ob + b), j.width, j.height, capi._vp(fb + b),
                                                             1, -1, 0, capi._vp(sp)))
-        host = d_flip.cpu().numpy()
+        h_out = torch.empty(no, dtype=torch.uint8).pin_memory()  # a pinned download runs at the link's rate
+        h_out.copy_(d_flip, non_blocking=True)
+        stream.synchronize()
+        host = h_out.numpy()
     finally:
         batch.close()
     return [Image.frombuffer("RGBA", (j.width, j.height), host[b: b + j.out_bytes].tobytes(), "raw", "RGBA", 0, 1)

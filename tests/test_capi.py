@@ -118,3 +118,40 @@ def test_server_argument_errors():
     import time
 
     assert abs(L.qt_server_clock() - time.monotonic()) < 1.0
+
+
+def test_host_alloc_without_gpu_is_ordinary_memory():
+    """qt_host_alloc hands out writable blocks of every size even where no pinned memory can
+    be had (this machine has no GPU); qt_host_free takes them back and ignores NULL and
+    foreign pointers."""
+    L = capi.lib()
+    blocks = []
+    for n in (0, 1, 4095, 4096, 300 << 10, 5 << 20):
+        p = ctypes.c_void_p()
+        assert L.qt_host_alloc(n, ctypes.byref(p)) == 0
+        assert p.value
+        if n:
+            buf = (ctypes.c_uint8 * n).from_address(p.value)
+            ctypes.memset(p.value, 0x5A, n)
+            assert buf[0] == 0x5A and buf[n - 1] == 0x5A
+        blocks.append(p)
+    for p in blocks:
+        L.qt_host_free(p)
+    L.qt_host_free(None)
+    foreign = ctypes.create_string_buffer(16)
+    L.qt_host_free(ctypes.cast(foreign, ctypes.c_void_p))
+    assert L.qt_host_alloc(16, None) != 0
+
+
+def test_texture_storage_round_trips_on_cpu(qt):
+    """The drop-in textures keep their bytes in qt_host_alloc blocks: construction, the
+    reference's fills and bytes round trips hold without a GPU."""
+    t = qt.RawTexture(3, 2)
+    assert t.tobytes() == bytes([0, 0, 0, 255] * 6)
+    data = bytes(range(256)) * 4
+    r = qt.RawTexture.frombytes(data, 16, 16)
+    assert r.tobytes() == data and bytes(memoryview(r)) == data
+    from quicktex_b200.s3tc.bc1 import BC1Texture
+
+    b = BC1Texture(9, 5)
+    assert b.tobytes() == bytes(8 * 3 * 2)
