@@ -88,15 +88,15 @@ BC1_DRAM_BYTES_PER_BLOCK = (16792832 + 18021376 + 2560 + 20707584 + 21565952 + 1
 # encoder, or the five-kernel level-18 pipeline), summarised in
 # profiles/bench_2048sq_inst_per_block.md.
 WARP_INST_PER_BLOCK: dict = {
-    "L0_four_ideal": 131.7, "L0_four_round": 132.4, "L0_four_nvidia": 132.4, "L0_four_amd": 131.7,
-    "L0_three_ideal": 210.9, "L0_three_round": 211.6, "L0_three_nvidia": 210.5, "L0_three_amd": 210.9,
-    "L0_three_black_ideal": 212.0, "L0_three_black_round": 212.7, "L0_three_black_nvidia": 211.5, "L0_three_black_amd": 211.9,
-    "L10_four_ideal": 458.9, "L10_four_round": 463.0, "L10_four_nvidia": 473.6, "L10_four_amd": 457.5,
-    "L10_three_ideal": 624.4, "L10_three_round": 628.5, "L10_three_nvidia": 643.0, "L10_three_amd": 623.1,
-    "L10_three_black_ideal": 625.7, "L10_three_black_round": 629.8, "L10_three_black_nvidia": 643.2, "L10_three_black_amd": 624.4,
-    "L18_four_ideal": 3280.6, "L18_four_round": 3324.4, "L18_four_nvidia": 3739.8, "L18_four_amd": 3283.1,
-    "L18_three_ideal": 4002.9, "L18_three_round": 4048.4, "L18_three_nvidia": 4588.1, "L18_three_amd": 4009.1,
-    "L18_three_black_ideal": 4003.7, "L18_three_black_round": 4048.1, "L18_three_black_nvidia": 4593.6, "L18_three_black_amd": 4009.2,
+    "L0_four_ideal": 131.8, "L0_four_round": 132.6, "L0_four_nvidia": 132.5, "L0_four_amd": 131.8,
+    "L0_three_ideal": 211.0, "L0_three_round": 211.8, "L0_three_nvidia": 210.6, "L0_three_amd": 211.0,
+    "L0_three_black_ideal": 212.5, "L0_three_black_round": 213.2, "L0_three_black_nvidia": 212.2, "L0_three_black_amd": 212.4,
+    "L10_four_ideal": 459.6, "L10_four_round": 463.6, "L10_four_nvidia": 474.2, "L10_four_amd": 458.2,
+    "L10_three_ideal": 625.1, "L10_three_round": 629.2, "L10_three_nvidia": 643.7, "L10_three_amd": 623.8,
+    "L10_three_black_ideal": 627.0, "L10_three_black_round": 631.0, "L10_three_black_nvidia": 645.6, "L10_three_black_amd": 625.6,
+    "L18_four_ideal": 3279.9, "L18_four_round": 3324.2, "L18_four_nvidia": 3738.0, "L18_four_amd": 3285.1,
+    "L18_three_ideal": 4003.2, "L18_three_round": 4047.6, "L18_three_nvidia": 4591.9, "L18_three_amd": 4008.1,
+    "L18_three_black_ideal": 4002.1, "L18_three_black_round": 4047.4, "L18_three_black_nvidia": 4587.6, "L18_three_black_amd": 4007.8,
 }
 
 
