@@ -15,10 +15,13 @@ namespace tpb {
 constexpr int kThreads = 128;
 
 // -2 and -1 that the compiler cannot fold: d * kNeg2 + v stays one IMAD on the FMA pipe. The
-// Full error loops use it for half of their |c|^2 - 2 p.c terms, so that the integer ALU pipe
-// (min, add) and the FMA pipe (dp4a, IMAD) share the work; the Check2 loops, whose comparisons
-// and selects already fill the ALU pipe, for all four terms and for p.axis (measured L0 +2.5-4%,
-// L10 +2-4.5% over the plain expressions, which compile to ALU instructions).
+// Full trial-error loops use it for half of their |c|^2 - 2 p.c terms, so that the integer ALU
+// pipe (min, add) and the FMA pipe (dp4a, IMAD) share the work; the loops whose comparisons and
+// selects already fill the ALU pipe (Check2 and Faster, and FindSelectors in Full mode) for every
+// term and for p.axis. Measured over the plain expressions, which compile to ALU instructions:
+// Check2 L0 +2.5-4%, L10 +2-4.5%; Faster (which also selects among four errors instead of
+// among palette words) L5 +4.5-7%, L7 +12%, BC3 L5 +8%; FindSelectors' Full loop +1-2% at the
+// three-colour settings.
 __constant__ int kNeg2 = -2;
 __constant__ int kNeg1 = -1;
 
@@ -115,18 +118,20 @@ template <int IT, int K> __device__ __forceinline__ uint2 find_selectors_body(in
         const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
         const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
         const int t0 = d0 + d1, t1 = d1 + d2, t2 = d2 + d3;
+        const int h0 = t0 >> 1, h1 = (t1 - 1) >> 1, h2 = (t2 - 1) >> 1;  // floor division
 #pragma unroll 4
         for (int i = 0; i < 16; i++) {
             const uint32_t v = px(i);
             // 2 p.axis, with axis = palette entry 3 - entry 0 (the palette words' byte 3 is 0)
             const int p0 = (int)__dp4a(v, c0, 0u), p3 = (int)__dp4a(v, c3, 0u);
-            const int dot = 2 * (p3 - p0);
-            const int s = 3 - ((dot <= t0) + (dot < t1) + (dot < t2));
+            const int pd = p0 * kNeg1 + p3;  // p.axis; 2 p.axis <= t0 exactly when p.axis <= h0 ...
+            const int s = 3 - ((pd <= h0) + (pd <= h1) + (pd <= h2));
             if (K == K_F4_FASTER) {
                 const uint32_t u = v & 0x00FFFFFFu;
-                const uint32_t c = s == 0 ? c0 : s == 1 ? c1 : s == 2 ? c2 : c3;
-                const int vc = s == 0 ? v0 : s == 1 ? v1 : s == 2 ? v2 : v3;
-                tot += (uint32_t)((int)__dp4a(u, u, 0u) + vc - 2 * (int)__dp4a(u, c, 0u));
+                const int p1 = (int)__dp4a(v, c1, 0u), p2 = (int)__dp4a(v, c2, 0u);
+                const int q0 = p0 * kNeg2 + v0, q1 = p1 * kNeg2 + v1, q2 = p2 * kNeg2 + v2, q3 = p3 * kNeg2 + v3;
+                const int e = s == 0 ? q0 : s == 1 ? q1 : s == 2 ? q2 : q3;
+                tot += (uint32_t)((int)__dp4a(u, u, 0u) + e);
             }
             sel |= (uint32_t)s << (2 * i);
         }
@@ -165,13 +170,13 @@ template <int IT, int K> __device__ __forceinline__ uint2 find_selectors_body(in
             const uint32_t u = px(i) & 0x00FFFFFFu;
             const int pp = (int)__dp4a(u, u, 0u);
             // ties keep the lower index except selector 3 (:762)
-            int e = v0 - 2 * (int)__dp4a(u, c0, 0u), s = 0;
-            const int e1 = v1 - 2 * (int)__dp4a(u, c1, 0u);
+            int e = (int)__dp4a(u, c0, 0u) * kNeg2 + v0, s = 0;
+            const int e1 = (int)__dp4a(u, c1, 0u) * kNeg2 + v1;
             if (e1 < e) { e = e1; s = 1; }
-            const int e2 = v2 - 2 * (int)__dp4a(u, c2, 0u);
+            const int e2 = (int)__dp4a(u, c2, 0u) * kNeg2 + v2;
             if (e2 < e) { e = e2; s = 2; }
             if (K != K_T3) {
-                const int e3 = v3 - 2 * (int)__dp4a(u, c3, 0u);
+                const int e3 = (int)__dp4a(u, c3, 0u) * kNeg2 + v3;
                 if (e3 <= e) { e = e3; s = 3; }
             }
             tot += (uint32_t)(e + pp);
@@ -258,15 +263,16 @@ template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo,
             const int d0 = ar * P.r0 + ag * P.g0 + ab * P.b0, d1 = ar * P.r1 + ag * P.g1 + ab * P.b1;
             const int d2 = ar * P.r2 + ag * P.g2 + ab * P.b2, d3 = ar * P.r3 + ag * P.g3 + ab * P.b3;
             const int t0 = d0 + d1, t1 = d1 + d2, t2 = d2 + d3;
+            const int h0 = t0 >> 1, h1 = (t1 - 1) >> 1, h2 = (t2 - 1) >> 1;  // floor division
 #pragma unroll 4
             for (int i = 0; i < 16; i++) {
                 const uint32_t u = px(i);
-                const int e0 = (int)__dp4a(u, c0, 0u), e3 = (int)__dp4a(u, c3, 0u);
-                const int dot = 2 * (e3 - e0);  // 2 p.axis
-                const int s = 3 - ((dot <= t0) + (dot < t1) + (dot < t2));
-                const uint32_t c = s == 0 ? c0 : s == 1 ? c1 : s == 2 ? c2 : c3;
-                const int vc = s == 0 ? v0 : s == 1 ? v1 : s == 2 ? v2 : v3;
-                t += vc - 2 * (int)__dp4a(u, c, 0u);
+                const int p0 = (int)__dp4a(u, c0, 0u), p1 = (int)__dp4a(u, c1, 0u);
+                const int p2 = (int)__dp4a(u, c2, 0u), p3 = (int)__dp4a(u, c3, 0u);
+                const int pd = p0 * kNeg1 + p3;
+                const int s = 3 - ((pd <= h0) + (pd <= h1) + (pd <= h2));
+                const int q0 = p0 * kNeg2 + v0, q1 = p1 * kNeg2 + v1, q2 = p2 * kNeg2 + v2, q3 = p3 * kNeg2 + v3;
+                t += s == 0 ? q0 : s == 1 ? q1 : s == 2 ? q2 : q3;
             }
         }
         return (uint32_t)(pp_sum + t);
