@@ -463,6 +463,7 @@ class HostCache {
         return *c;
     }
     int alloc(size_t n, void **out) {
+        if (n > (size_t(1) << 48)) return set_err(QT_ERR_OOM, "host allocation of %zu bytes failed", n);
         const size_t cls = host_class(n);
         {
             std::lock_guard<std::mutex> lk(mu_);
@@ -904,7 +905,7 @@ int run_host_bc1_parts(const uint8_t *src, uint8_t *dst, int w, int h, size_t bl
     std::vector<int> cut(1, 0);  // band k covers block rows [cut[k], cut[k + 1])
     for (long rows = rows_first; cut.back() < bh; rows *= 2)
         cut.push_back((int)std::min<long>(bh, (long)cut.back() + rows));
-    const int nbands = (int)cut.size() - 1;  // <= 12 for any texture of <= 2^32 texels
+    const int nbands = (int)cut.size() - 1;  // <= 13 for any texture of <= 2^32 texels (bc1_parts_add takes 32)
     int dev = 0;
     int rc = ensure_device(&dev);
     if (rc) return rc;

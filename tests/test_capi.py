@@ -141,6 +141,8 @@ def test_host_alloc_without_gpu_is_ordinary_memory():
     foreign = ctypes.create_string_buffer(16)
     L.qt_host_free(ctypes.cast(foreign, ctypes.c_void_p))
     assert L.qt_host_alloc(16, None) != 0
+    p = ctypes.c_void_p()
+    assert L.qt_host_alloc(ctypes.c_size_t(-1).value, ctypes.byref(p)) == capi.QT_ERR_OOM and not p.value
 
 
 def test_texture_storage_round_trips_on_cpu(qt):
