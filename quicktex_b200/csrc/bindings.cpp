@@ -13,6 +13,7 @@
 #include <pybind11/pybind11.h>
 #include <pybind11/stl.h>
 
+#include <algorithm>
 #include <array>
 #include <cstdint>
 #include <cstring>
@@ -161,8 +162,9 @@ inline size_t checked_area(int w, int h) { return (w > 0 && h > 0) ? (size_t)w *
 
 class RawTexture : public Texture {
    public:
-    RawTexture(int w, int h) : Texture(w, h, checked_area(w, h) * 4) {
-        for (size_t i = 3; i < data_.size(); i += 4) data_[i] = 255;  // Color() = (0, 0, 0, 255)
+    RawTexture(int w, int h) : Texture(w, h, checked_area(w, h) * 4, NoFill{}) {
+        // Color() = (0, 0, 0, 255) in every texel, one 32-bit store each (the storage is page-aligned)
+        std::fill_n(reinterpret_cast<uint32_t *>(data_.data()), data_.size() / 4, 0xFF000000u);
     }
     RawTexture(int w, int h, NoFill f) : Texture(w, h, checked_area(w, h) * 4, f) {}
     Color GetPixel(int x, int y) const {
@@ -418,7 +420,7 @@ class BC1Decoder {
     }
     explicit BC1Decoder(bool write_alpha = false) : BC1Decoder(write_alpha, std::make_shared<Interpolator>()) {}
     RawTexture Decode(const BC1Texture &tex) const {
-        RawTexture out(tex.Width(), tex.Height());
+        RawTexture out(tex.Width(), tex.Height(), NoFill{});  // every texel is written, defaults included
         const int it = interp_->Type(), wa = write_alpha;
         int rc;
         {
@@ -462,7 +464,7 @@ class BC4Decoder {
         if (channel >= 4) throw std::invalid_argument("Channel out of range");
     }
     RawTexture Decode(const BC4Texture &tex) const {
-        RawTexture out(tex.Width(), tex.Height());
+        RawTexture out(tex.Width(), tex.Height(), NoFill{});  // every texel is written, defaults included
         int rc;
         {
             py::gil_scoped_release nogil;
@@ -507,7 +509,7 @@ class BC3Decoder {
         : bc1_(std::make_shared<BC1Decoder>(false, std::move(interp))), bc4_(std::make_shared<BC4Decoder>(3)) {}
     BC3Decoder() : BC3Decoder(std::make_shared<Interpolator>()) {}
     RawTexture Decode(const BC3Texture &tex) const {
-        RawTexture out(tex.Width(), tex.Height());
+        RawTexture out(tex.Width(), tex.Height(), NoFill{});  // every texel is written, defaults included
         const int it = bc1_->GetInterpolator()->Type();
         int rc;
         {
@@ -550,7 +552,7 @@ class BC5Decoder {
    public:
     BC5Decoder(uint8_t c0 = 0, uint8_t c1 = 1) : d0_(std::make_shared<BC4Decoder>(c0)), d1_(std::make_shared<BC4Decoder>(c1)) {}
     RawTexture Decode(const BC5Texture &tex) const {
-        RawTexture out(tex.Width(), tex.Height());
+        RawTexture out(tex.Width(), tex.Height(), NoFill{});  // every texel is written, defaults included
         const int c0 = d0_->GetChannel(), c1 = d1_->GetChannel();
         int rc;
         {
