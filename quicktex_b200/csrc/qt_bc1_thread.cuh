@@ -58,25 +58,32 @@ __device__ __forceinline__ bool black(uint32_t v) { return (cr(v) | cg(v) | cb(v
 
 __device__ __forceinline__ M metrics_body(bool ignore_black) {
     M m;
-    m.mn[0] = m.mn[1] = m.mn[2] = 255;
-    m.mx[0] = m.mx[1] = m.mx[2] = 0;
-    m.sum[0] = m.sum[1] = m.sum[2] = 0;
-    m.has_black = false;
-    m.grey = true;
     int total = 0;
+    // two channels per word (r | b << 16, g | a << 16): packed 16-bit min, max and sums (at most
+    // 16 x 255 per half); the alpha half is carried along and dropped
+    uint32_t mn_rb = 0x00FF00FFu, mn_ga = 0x00FF00FFu, mx_rb = 0u, mx_ga = 0u, s_rb = 0u, s_ga = 0u;
+    bool grey = true, has_black = false;
 #pragma unroll 4
     for (int i = 0; i < 16; i++) {
         const uint32_t v = px(i);
-        const bool b = black(v);
-        m.has_black |= b;
+        const bool b = (v & 0x00FCFCFCu) == 0u;  // (r | g | b) < 4
+        has_black |= b;
         if (ignore_black && b) continue;
-        const int r = cr(v), g = cg(v), bl = cb(v);
-        m.grey &= (r == g) && (r == bl);
-        m.mn[0] = min(m.mn[0], r); m.mn[1] = min(m.mn[1], g); m.mn[2] = min(m.mn[2], bl);
-        m.mx[0] = max(m.mx[0], r); m.mx[1] = max(m.mx[1], g); m.mx[2] = max(m.mx[2], bl);
-        m.sum[0] += r; m.sum[1] += g; m.sum[2] += bl;
+        const uint32_t rb = v & 0x00FF00FFu, ga = (v >> 8) & 0x00FF00FFu;
+        grey &= (v & 0x00FFFFFFu) == (v & 0xFFu) * 0x010101u;
+        asm("min.u16x2 %0, %0, %1;" : "+r"(mn_rb) : "r"(rb));
+        asm("min.u16x2 %0, %0, %1;" : "+r"(mn_ga) : "r"(ga));
+        asm("max.u16x2 %0, %0, %1;" : "+r"(mx_rb) : "r"(rb));
+        asm("max.u16x2 %0, %0, %1;" : "+r"(mx_ga) : "r"(ga));
+        s_rb += rb;
+        s_ga += ga;
         total++;
     }
+    m.has_black = has_black;
+    m.grey = grey;
+    m.mn[0] = (int)(mn_rb & 0xFFFFu); m.mn[1] = (int)(mn_ga & 0xFFFFu); m.mn[2] = (int)(mn_rb >> 16);
+    m.mx[0] = (int)(mx_rb & 0xFFFFu); m.mx[1] = (int)(mx_ga & 0xFFFFu); m.mx[2] = (int)(mx_rb >> 16);
+    m.sum[0] = (int)(s_rb & 0xFFFFu); m.sum[1] = (int)(s_ga & 0xFFFFu); m.sum[2] = (int)(s_rb >> 16);
 #pragma unroll
     for (int c = 0; c < 3; c++) m.av[c] = total > 0 ? (m.sum[c] + total / 2) / total : 0;
     return m;
@@ -452,13 +459,19 @@ template <bool INL> __device__ __forceinline__ int2 find_endpoints_(const M &m, 
 template <int IT, int K, bool INL> __device__ __forceinline__ R refine_ls_body(R r, const M &m, int passes) {
     for (int pass = 0; pass < passes; pass++) {
         R t = r;
-        int q0r = 0, q0g = 0, q0b = 0, n1 = 0, n2 = 0, n3 = 0;
+        // sum of selector x colour per channel, two channels per word (r | b << 16, g | a << 16:
+        // at most 16 x 3 x 255 = 12240 per half, no carry), and the selector histogram by popcount
+        uint32_t acc_rb = 0, acc_ga = 0;
+#pragma unroll
         for (int i = 0; i < 16; i++) {
-            const uint32_t v = px(i);
-            const int s = (t.sel >> (2 * i)) & 3;
-            q0r += cr(v) * s; q0g += cg(v) * s; q0b += cb(v) * s;
-            n1 += s == 1; n2 += s == 2; n3 += s == 3;
+            const uint32_t v = px(i), s = (t.sel >> (2 * i)) & 3u;
+            acc_rb = s * (v & 0x00FF00FFu) + acc_rb;
+            acc_ga = s * ((v >> 8) & 0x00FF00FFu) + acc_ga;
         }
+        const int q0r = (int)(acc_rb & 0xFFFFu), q0g = (int)(acc_ga & 0xFFFFu), q0b = (int)(acc_rb >> 16);
+        const uint32_t w = t.sel;
+        const int n1 = __popc(w & ~(w >> 1) & 0x55555555u), n2 = __popc(~w & (w >> 1) & 0x55555555u);
+        const int n3 = __popc(w & (w >> 1) & 0x55555555u);
         const int n0 = 16 - n1 - n2 - n3;
         float m0 = (float)(n1 + 4 * n2 + 9 * n3), m1 = (float)(2 * n1 + 2 * n2), m2 = m1, m3 = (float)(9 * n0 + 4 * n1 + n2);
         const float det = __fsub_rn(__fmul_rn(m0, m3), __fmul_rn(m1, m2));
