@@ -88,15 +88,15 @@ BC1_DRAM_BYTES_PER_BLOCK = (16792832 + 18021376 + 2560 + 20707584 + 21565952 + 1
 # encoder, or the five-kernel level-18 pipeline), summarised in
 # profiles/bench_2048sq_inst_per_block.md.
 WARP_INST_PER_BLOCK: dict = {
-    "L0_four_ideal": 131.8, "L0_four_round": 132.6, "L0_four_nvidia": 132.5, "L0_four_amd": 131.8,
-    "L0_three_ideal": 211.0, "L0_three_round": 211.8, "L0_three_nvidia": 210.6, "L0_three_amd": 211.0,
-    "L0_three_black_ideal": 212.5, "L0_three_black_round": 213.2, "L0_three_black_nvidia": 212.2, "L0_three_black_amd": 212.4,
-    "L10_four_ideal": 459.6, "L10_four_round": 463.6, "L10_four_nvidia": 474.2, "L10_four_amd": 458.2,
-    "L10_three_ideal": 625.1, "L10_three_round": 629.2, "L10_three_nvidia": 643.7, "L10_three_amd": 623.8,
-    "L10_three_black_ideal": 627.0, "L10_three_black_round": 631.0, "L10_three_black_nvidia": 645.6, "L10_three_black_amd": 625.6,
-    "L18_four_ideal": 3279.9, "L18_four_round": 3324.2, "L18_four_nvidia": 3738.0, "L18_four_amd": 3285.1,
-    "L18_three_ideal": 4003.2, "L18_three_round": 4047.6, "L18_three_nvidia": 4591.9, "L18_three_amd": 4008.1,
-    "L18_three_black_ideal": 4002.1, "L18_three_black_round": 4047.4, "L18_three_black_nvidia": 4587.6, "L18_three_black_amd": 4007.8,
+    "L0_four_ideal": 124.7, "L0_four_round": 125.4, "L0_four_nvidia": 125.4, "L0_four_amd": 124.7,
+    "L0_three_ideal": 198.8, "L0_three_round": 199.6, "L0_three_nvidia": 198.6, "L0_three_amd": 198.9,
+    "L0_three_black_ideal": 200.8, "L0_three_black_round": 201.5, "L0_three_black_nvidia": 200.5, "L0_three_black_amd": 200.8,
+    "L10_four_ideal": 447.4, "L10_four_round": 451.4, "L10_four_nvidia": 462.0, "L10_four_amd": 446.1,
+    "L10_three_ideal": 602.9, "L10_three_round": 607.0, "L10_three_nvidia": 621.3, "L10_three_amd": 601.7,
+    "L10_three_black_ideal": 605.0, "L10_three_black_round": 609.1, "L10_three_black_nvidia": 623.2, "L10_three_black_amd": 603.7,
+    "L18_four_ideal": 3257.4, "L18_four_round": 3300.9, "L18_four_nvidia": 3718.6, "L18_four_amd": 3260.3,
+    "L18_three_ideal": 3968.5, "L18_three_round": 4015.2, "L18_three_nvidia": 4556.1, "L18_three_amd": 3973.8,
+    "L18_three_black_ideal": 3968.4, "L18_three_black_round": 4014.6, "L18_three_black_nvidia": 4553.8, "L18_three_black_amd": 3975.1,
 }
 
 
