@@ -397,11 +397,35 @@ __device__ __forceinline__ int2 find_endpoints_body(const M &m, int mode, bool i
         }
     } else {  // PCA
         int s00 = 0, s01 = 0, s02 = 0, s11 = 0, s12 = 0, s22 = 0;
-        for (int i = 0; i < 16; i++) {
-            const uint32_t v = px(i);
-            if (ignore_black && black(v)) continue;
-            const int dr = cr(v) - m.av[0], dg = cg(v) - m.av[1], db = cb(v) - m.av[2];
-            s00 += dr * dr; s01 += dr * dg; s02 += dr * db; s11 += dg * dg; s12 += dg * db; s22 += db * db;
+        if (ignore_black) {
+            for (int i = 0; i < 16; i++) {
+                const uint32_t v = px(i);
+                if (black(v)) continue;
+                const int dr = cr(v) - m.av[0], dg = cg(v) - m.av[1], db = cb(v) - m.av[2];
+                s00 += dr * dr; s01 += dr * dg; s02 += dr * db; s11 += dg * dg; s12 += dg * db; s22 += db * db;
+            }
+        } else {
+            // the same sums over all 16 texels from raw moments, exactly in integers:
+            // sum (x - a)(y - b) = sum xy - b sum x - a sum y + 16 a b. The raw moments come four
+            // texels at a time: one word per channel of four texels' bytes, one dp4a per product.
+            uint32_t rr = 0, rg = 0, rb = 0, gg = 0, gb = 0, bb = 0;
+#pragma unroll
+            for (int i = 0; i < 16; i += 4) {
+                const uint32_t v0 = px(i), v1 = px(i + 1), v2 = px(i + 2), v3 = px(i + 3);
+                const uint32_t t01 = __byte_perm(v0, v1, 0x5140), t23 = __byte_perm(v2, v3, 0x5140);  // r r g g
+                const uint32_t u01 = __byte_perm(v0, v1, 0x7362), u23 = __byte_perm(v2, v3, 0x7362);  // b b a a
+                const uint32_t R = __byte_perm(t01, t23, 0x5410), G = __byte_perm(t01, t23, 0x7632);
+                const uint32_t B = __byte_perm(u01, u23, 0x5410);
+                rr = __dp4a(R, R, rr); rg = __dp4a(R, G, rg); rb = __dp4a(R, B, rb);
+                gg = __dp4a(G, G, gg); gb = __dp4a(G, B, gb); bb = __dp4a(B, B, bb);
+            }
+            const int a0 = m.av[0], a1 = m.av[1], a2 = m.av[2], S0 = m.sum[0], S1 = m.sum[1], S2 = m.sum[2];
+            s00 = (int)rr - 2 * a0 * S0 + 16 * a0 * a0;
+            s01 = (int)rg - a1 * S0 - a0 * S1 + 16 * a0 * a1;
+            s02 = (int)rb - a2 * S0 - a0 * S2 + 16 * a0 * a2;
+            s11 = (int)gg - 2 * a1 * S1 + 16 * a1 * a1;
+            s12 = (int)gb - a2 * S1 - a1 * S2 + 16 * a1 * a2;
+            s22 = (int)bb - 2 * a2 * S2 + 16 * a2 * a2;
         }
         const float k255 = 255.0f;
         const float c00 = __fdiv_rn((float)(1 + s00), k255), c01 = __fdiv_rn((float)s01, k255);
