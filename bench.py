@@ -88,15 +88,15 @@ BC1_DRAM_BYTES_PER_BLOCK = (16792832 + 18021376 + 2560 + 20707584 + 21565952 + 1
 # encoder, or the five-kernel level-18 pipeline), summarised in
 # profiles/bench_2048sq_inst_per_block.md.
 WARP_INST_PER_BLOCK: dict = {
-    "L0_four_ideal": 124.7, "L0_four_round": 125.4, "L0_four_nvidia": 125.4, "L0_four_amd": 124.7,
-    "L0_three_ideal": 198.8, "L0_three_round": 199.6, "L0_three_nvidia": 198.6, "L0_three_amd": 198.9,
-    "L0_three_black_ideal": 200.8, "L0_three_black_round": 201.5, "L0_three_black_nvidia": 200.5, "L0_three_black_amd": 200.8,
-    "L10_four_ideal": 447.4, "L10_four_round": 451.4, "L10_four_nvidia": 462.0, "L10_four_amd": 446.1,
-    "L10_three_ideal": 602.9, "L10_three_round": 607.0, "L10_three_nvidia": 621.3, "L10_three_amd": 601.7,
-    "L10_three_black_ideal": 605.0, "L10_three_black_round": 609.1, "L10_three_black_nvidia": 623.2, "L10_three_black_amd": 603.7,
-    "L18_four_ideal": 3257.4, "L18_four_round": 3300.9, "L18_four_nvidia": 3718.6, "L18_four_amd": 3260.3,
-    "L18_three_ideal": 3968.5, "L18_three_round": 4015.2, "L18_three_nvidia": 4556.1, "L18_three_amd": 3973.8,
-    "L18_three_black_ideal": 3968.4, "L18_three_black_round": 4014.6, "L18_three_black_nvidia": 4553.8, "L18_three_black_amd": 3975.1,
+    "L0_four_ideal": 122.5, "L0_four_round": 123.3, "L0_four_nvidia": 123.2, "L0_four_amd": 122.6,
+    "L0_three_ideal": 196.7, "L0_three_round": 197.4, "L0_three_nvidia": 196.3, "L0_three_amd": 196.7,
+    "L0_three_black_ideal": 198.2, "L0_three_black_round": 198.9, "L0_three_black_nvidia": 197.9, "L0_three_black_amd": 198.2,
+    "L10_four_ideal": 444.0, "L10_four_round": 448.1, "L10_four_nvidia": 458.7, "L10_four_amd": 442.7,
+    "L10_three_ideal": 599.6, "L10_three_round": 603.6, "L10_three_nvidia": 617.9, "L10_three_amd": 598.3,
+    "L10_three_black_ideal": 601.3, "L10_three_black_round": 605.4, "L10_three_black_nvidia": 620.1, "L10_three_black_amd": 600.1,
+    "L18_four_ideal": 3247.6, "L18_four_round": 3292.0, "L18_four_nvidia": 3705.9, "L18_four_amd": 3250.3,
+    "L18_three_ideal": 3957.6, "L18_three_round": 4003.8, "L18_three_nvidia": 4549.1, "L18_three_amd": 3964.5,
+    "L18_three_black_ideal": 3959.2, "L18_three_black_round": 4003.7, "L18_three_black_nvidia": 4548.3, "L18_three_black_amd": 3964.9,
 }
 
 

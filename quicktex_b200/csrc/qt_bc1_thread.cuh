@@ -56,6 +56,16 @@ __device__ __forceinline__ int cg(uint32_t v) { return (v >> 8) & 0xFF; }
 __device__ __forceinline__ int cb(uint32_t v) { return (v >> 16) & 0xFF; }
 __device__ __forceinline__ bool black(uint32_t v) { return (cr(v) | cg(v) | cb(v)) < 4; }
 
+// Texels i..i+3 as one word per channel (byte k = texel i + k), for dp4a over four texels
+__device__ __forceinline__ void channel_words(int i, uint32_t &R, uint32_t &G, uint32_t &B) {
+    const uint32_t v0 = px(i), v1 = px(i + 1), v2 = px(i + 2), v3 = px(i + 3);
+    const uint32_t t01 = __byte_perm(v0, v1, 0x5140), t23 = __byte_perm(v2, v3, 0x5140);  // r r g g
+    const uint32_t u01 = __byte_perm(v0, v1, 0x7362), u23 = __byte_perm(v2, v3, 0x7362);  // b b a a
+    R = __byte_perm(t01, t23, 0x5410);
+    G = __byte_perm(t01, t23, 0x7632);
+    B = __byte_perm(u01, u23, 0x5410);
+}
+
 __device__ __forceinline__ M metrics_body(bool ignore_black) {
     M m;
     int total = 0;
@@ -362,13 +372,18 @@ __device__ __forceinline__ int2 find_endpoints_body(const M &m, int mode, bool i
         lo = precise_round565(l[0], l[1], l[2], s_mid5, s_mid6);
         hi = precise_round565(h[0], h[1], h[2], s_mid5, s_mid6);
     } else if (mode == EP_BB || mode == EP_BBINT) {
-        int cxz = 0, cyz = 0;
-        for (int i = 0; i < 16; i++) {  // b * r - avg.r, as written (:572-573)
-            const uint32_t v = px(i);
-            const int b = cb(v) - m.av[2];
-            cxz += b * cr(v) - m.av[0];
-            cyz += b * cg(v) - m.av[1];
+        // sum over the 16 texels of (b - avg.b) * r - avg.r and (b - avg.b) * g - avg.g, as written
+        // (:572-573), from raw moments: sum br - avg.b sum r - 16 avg.r (exact in integers)
+        uint32_t rb = 0, gb = 0;
+#pragma unroll
+        for (int i = 0; i < 16; i += 4) {
+            uint32_t R, G, B;
+            channel_words(i, R, G, B);
+            rb = __dp4a(R, B, rb);
+            gb = __dp4a(G, B, gb);
         }
+        const int cxz = (int)rb - m.av[2] * m.sum[0] - 16 * m.av[0];
+        const int cyz = (int)gb - m.av[2] * m.sum[1] - 16 * m.av[1];
         if (mode == EP_BB) {
             const float bias = __fdiv_rn(8.0f, 255.0f);
             float l[3], h[3];
@@ -411,11 +426,8 @@ __device__ __forceinline__ int2 find_endpoints_body(const M &m, int mode, bool i
             uint32_t rr = 0, rg = 0, rb = 0, gg = 0, gb = 0, bb = 0;
 #pragma unroll
             for (int i = 0; i < 16; i += 4) {
-                const uint32_t v0 = px(i), v1 = px(i + 1), v2 = px(i + 2), v3 = px(i + 3);
-                const uint32_t t01 = __byte_perm(v0, v1, 0x5140), t23 = __byte_perm(v2, v3, 0x5140);  // r r g g
-                const uint32_t u01 = __byte_perm(v0, v1, 0x7362), u23 = __byte_perm(v2, v3, 0x7362);  // b b a a
-                const uint32_t R = __byte_perm(t01, t23, 0x5410), G = __byte_perm(t01, t23, 0x7632);
-                const uint32_t B = __byte_perm(u01, u23, 0x5410);
+                uint32_t R, G, B;
+                channel_words(i, R, G, B);
                 rr = __dp4a(R, R, rr); rg = __dp4a(R, G, rg); rb = __dp4a(R, B, rb);
                 gg = __dp4a(G, G, gg); gb = __dp4a(G, B, gb); bb = __dp4a(B, B, bb);
             }
