@@ -88,15 +88,15 @@ BC1_DRAM_BYTES_PER_BLOCK = (16792832 + 18021376 + 2560 + 20707584 + 21565952 + 1
 # encoder, or the five-kernel level-18 pipeline), summarised in
 # profiles/bench_2048sq_inst_per_block.md.
 WARP_INST_PER_BLOCK: dict = {
-    "L0_four_ideal": 122.5, "L0_four_round": 123.3, "L0_four_nvidia": 123.2, "L0_four_amd": 122.6,
-    "L0_three_ideal": 196.7, "L0_three_round": 197.4, "L0_three_nvidia": 196.3, "L0_three_amd": 196.7,
-    "L0_three_black_ideal": 198.2, "L0_three_black_round": 198.9, "L0_three_black_nvidia": 197.9, "L0_three_black_amd": 198.2,
-    "L10_four_ideal": 444.0, "L10_four_round": 448.1, "L10_four_nvidia": 458.7, "L10_four_amd": 442.7,
-    "L10_three_ideal": 599.6, "L10_three_round": 603.6, "L10_three_nvidia": 617.9, "L10_three_amd": 598.3,
-    "L10_three_black_ideal": 601.3, "L10_three_black_round": 605.4, "L10_three_black_nvidia": 620.1, "L10_three_black_amd": 600.1,
-    "L18_four_ideal": 3247.6, "L18_four_round": 3292.0, "L18_four_nvidia": 3705.9, "L18_four_amd": 3250.3,
-    "L18_three_ideal": 3957.6, "L18_three_round": 4003.8, "L18_three_nvidia": 4549.1, "L18_three_amd": 3964.5,
-    "L18_three_black_ideal": 3959.2, "L18_three_black_round": 4003.7, "L18_three_black_nvidia": 4548.3, "L18_three_black_amd": 3964.9,
+    "L0_four_ideal": 121.0, "L0_four_round": 121.7, "L0_four_nvidia": 122.8, "L0_four_amd": 120.8,
+    "L0_three_ideal": 188.3, "L0_three_round": 189.0, "L0_three_nvidia": 191.1, "L0_three_amd": 188.2,
+    "L0_three_black_ideal": 190.1, "L0_three_black_round": 190.8, "L0_three_black_nvidia": 192.8, "L0_three_black_amd": 189.9,
+    "L10_four_ideal": 443.9, "L10_four_round": 448.0, "L10_four_nvidia": 457.8, "L10_four_amd": 442.6,
+    "L10_three_ideal": 593.0, "L10_three_round": 597.1, "L10_three_nvidia": 612.6, "L10_three_amd": 591.7,
+    "L10_three_black_ideal": 594.8, "L10_three_black_round": 598.9, "L10_three_black_nvidia": 614.2, "L10_three_black_amd": 593.4,
+    "L18_four_ideal": 3221.0, "L18_four_round": 3266.3, "L18_four_nvidia": 3678.5, "L18_four_amd": 3225.4,
+    "L18_three_ideal": 3917.7, "L18_three_round": 3962.8, "L18_three_nvidia": 4511.4, "L18_three_amd": 3922.0,
+    "L18_three_black_ideal": 3917.9, "L18_three_black_round": 3963.0, "L18_three_black_nvidia": 4515.0, "L18_three_black_amd": 3924.5,
 }
 
 

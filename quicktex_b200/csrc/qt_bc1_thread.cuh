@@ -300,13 +300,17 @@ template <int IT, int K> __device__ __forceinline__ uint32_t block_error(int lo,
 // FindEndpointsSingleColor(result, pixels, color, is_3color) (BC1Encoder.cpp:458-471)
 template <int IT> __device__ __forceinline__ R single_color_body(int stale_lo, int stale_hi, int ar, int ag, int ab, bool is3) {
     const Pal P = make_pal<IT>(stale_lo, stale_hi, is3);  // colors[2] is internal index 1
-    uint32_t e = 0;
+    // sum over texels of |p - c|^2 in RGBA with c = (colors[2], 255), as
+    // sum |p|^2 - 2 sum p.c + 16 |c|^2 (exact in integers): two dp4a per texel
+    const uint32_t c = (uint32_t)P.r1 | ((uint32_t)P.g1 << 8) | ((uint32_t)P.b1 << 16) | 0xFF000000u;
+    uint32_t pp = 0, pc = 0;
 #pragma unroll 4
     for (int i = 0; i < 16; i++) {
         const uint32_t v = px(i);
-        const int dr = cr(v) - P.r1, dg = cg(v) - P.g1, db = cb(v) - P.b1, da = (int)(v >> 24) - 255;
-        e += (uint32_t)(dr * dr + dg * dg + db * db + da * da);
+        pp = __dp4a(v, v, pp);
+        pc = __dp4a(v, c, pc);
     }
+    const uint32_t e = pp - 2u * pc + 16u * __dp4a(c, c, 0u);
     const uint32_t mr = g_tab.match5[IT][ar], mg = g_tab.match6[IT][ag], mb = g_tab.match5[IT][ab];
     R r;
     r.lo = eppack((mr >> 8) & 0xFF, (mg >> 8) & 0xFF, (mb >> 8) & 0xFF);
